@@ -1,0 +1,216 @@
+/*
+ * collinea_sgm.h - C ABI of the B200 semi-global stereo matcher.
+ *
+ * This is the drop-in boundary for Collinea's GPU stereo backend.  In the reference the Java host
+ * calls OpenCL through Panama FFM downcalls (src/main/java/sgm/GpuSgm.java:30-54); a maintainer
+ * replaces those downcalls with downcalls into this library (libcollinea_sgm.so).  Every entry
+ * point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain C types only: pointers, sizes, int32/int64/double.  No CUDA or torch types.
+ *   - Every function returns CSGM_OK (0) or a negative CSGM_E_* code.  The message of the last
+ *     failure on the calling thread is returned by csgm_last_error().
+ *   - All host buffers are owned by the caller.  They may be pageable or pinned.  The library owns
+ *     every device allocation it makes, inside the session's memory budget.
+ *   - There is no CPU fallback: when the GPU path cannot run, the call fails.
+ *   - A session is bound to one CUDA device and one stream.  Calls on one session are serialised
+ *     by the session's own lock; different sessions may be used from different threads.
+ *
+ * Image and volume layouts
+ *   - Images are row-major uint8, index p = y * w + x.
+ *   - Census descriptors are word-major: desc[word * w * h + p], the layout the reference uploads
+ *     (src/main/java/sgm/GpuStereo.java:243-250).  Bit order follows CensusSgm.census
+ *     (src/main/java/sgm/CensusSgm.java:540-555): row-major over the window, centre skipped.
+ *   - Masks are uint8, non-zero = true.
+ */
+#ifndef COLLINEA_SGM_H
+#define COLLINEA_SGM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSGM_ABI_VERSION 1
+
+/* Status codes. */
+#define CSGM_OK 0
+#define CSGM_E_INVALID (-1)     /* bad argument: IllegalArgumentException in the reference */
+#define CSGM_E_CUDA (-2)        /* CUDA runtime failure: IllegalStateException("... failed") */
+#define CSGM_E_NOMEM (-3)       /* device allocation failed or the memory plan exceeds the budget */
+#define CSGM_E_NODEVICE (-4)    /* no CUDA device at the requested index */
+#define CSGM_E_TIMEOUT (-5)     /* a bounded device-side wait expired; the context stays usable */
+#define CSGM_E_BUSY (-6)        /* batch queue full or request not finished */
+#define CSGM_E_UNSUPPORTED (-7) /* parameter combination outside what the kernels implement */
+
+/* Matching-cost codes: StereoCost.code (src/main/java/sgm/StereoCost.java:7-15). */
+#define CSGM_COST_CENSUS 0
+#define CSGM_COST_AD_CENSUS 1
+#define CSGM_COST_CENSUS_GRADIENT 2
+#define CSGM_COST_ZNCC 3
+
+/*
+ * Matcher parameters.  Mirrors the scalar arguments of the reference `costs`/`paths` kernels
+ * (src/main/java/sgm/GpuStereo.java:384-403,600-614) plus the selection and LR settings.
+ * Penalties are the EFFECTIVE integer penalties, i.e. StereoCost.penalty(o.p1, o) and
+ * StereoCost.p2(o) (src/main/java/sgm/StereoCost.java:17-23); csgm_effective_penalties()
+ * computes them from Options-style values.
+ */
+typedef struct csgm_params {
+  int32_t disparities;         /* D = Options.disparities, 3..4096 */
+  int32_t min_disparity;       /* Options.minDisparity */
+  int32_t window_x;            /* census/texture/ZNCC window width  (Options.census) */
+  int32_t window_y;            /* census/texture/ZNCC window height (== window_x in the reference) */
+  int32_t cost_mode;           /* CSGM_COST_* */
+  int32_t census_weight_milli; /* (int) Math.round(Options.censusWeight * 1000) */
+  int32_t ad_truncation;       /* Options.adTruncation */
+  int32_t gradient_truncation; /* Options.gradientTruncation */
+  int32_t p1;                  /* effective P1 */
+  int32_t p2;                  /* effective P2 */
+  int32_t edge_scale;          /* Options.sgmEdgeScale, 0..255 (0 = constant P2) */
+  int32_t directions;          /* 4 or 8 (reference); 16 adds the (+-1,+-2),(+-2,+-1) paths */
+  int32_t aggregate_bytes;     /* 2 (uint16) or 4 (uint32): StereoCost.aggregateBytes */
+  int32_t flags;               /* reserved, must be 0 */
+  double uniqueness;           /* Options.uniqueness */
+  double lr_threshold;         /* Options.lrThreshold */
+} csgm_params;
+
+/* Rejection counters: CensusSgm.Stats (src/main/java/sgm/CensusSgm.java:683-737). */
+typedef struct csgm_stats {
+  int64_t lower_boundary_rejected;
+  int64_t full_interval_pixels;
+  int64_t boundary_rejected;
+  int64_t upper_boundary_rejected;
+  int64_t ambiguity_rejected;
+  int64_t selected;
+  int64_t lr_rejected;
+  int64_t post_median_lr_rejected;
+  int64_t photometric_rejected;
+  int64_t speckle_rejected;
+  int64_t valid;
+} csgm_stats;
+
+/* Device description: GpuSgm.Device (src/main/java/sgm/GpuSgm.java:11-18). */
+typedef struct csgm_device_info {
+  char name[256];
+  int64_t memory_bytes;
+  int32_t sm_count;
+  int32_t cc_major;
+  int32_t cc_minor;
+} csgm_device_info;
+
+/* Per-session device timing: GpuSgm.Compute.profile (src/main/java/sgm/GpuSgm.java:592-604). */
+typedef struct csgm_profile {
+  int64_t kernel_ns;   /* summed device time of the library's kernels (CUDA events) */
+  int64_t upload_ns;   /* host->device copy time */
+  int64_t download_ns; /* device->host copy time */
+  int64_t uploaded_bytes;
+  int64_t downloaded_bytes;
+  int64_t launches;    /* kernels launched by the library */
+  int64_t calls;       /* csgm_match/csgm_pair calls profiled */
+} csgm_profile;
+
+typedef struct csgm_session csgm_session;
+
+/* ---- library ---------------------------------------------------------------------------- */
+
+/* ABI version (CSGM_ABI_VERSION). */
+int csgm_version(void);
+
+/* Message of the last failure on this thread ("" if none).  Thread-local, like the exception
+ * text the reference attaches in GpuSgm.check (src/main/java/sgm/GpuSgm.java:56-58). */
+const char* csgm_last_error(void);
+
+/* Effective penalties from Options values: StereoCost.penalty / StereoCost.p2
+ * (src/main/java/sgm/StereoCost.java:17-23), with bits = window_x * window_y - 1. */
+int csgm_effective_penalties(double p1, double p2, int32_t window_x, int32_t window_y,
+                             int32_t* p1_eff, int32_t* p2_eff);
+
+/* Aggregate width: StereoCost.aggregateBound / aggregateBytes (src/main/java/sgm/StereoCost.java:31-41).
+ * mode: 0 auto, 16 force uint16 (fails with CSGM_E_INVALID if the bound does not fit), 32 force uint32. */
+int csgm_aggregate_bytes(int32_t directions, int32_t p2_eff, int32_t mode, int32_t* bytes,
+                         int64_t* bound);
+
+/* ---- devices and sessions ----------------------------------------------------------------- */
+
+/* Number of CUDA devices: GpuSgm.devices (src/main/java/sgm/GpuSgm.java:79-141). */
+int csgm_device_count(int32_t* count);
+
+/* Device description: GpuSgm.enumerateDevices (src/main/java/sgm/GpuSgm.java:120-136). */
+int csgm_device_info_get(int32_t device, csgm_device_info* info);
+
+/* Open a session on a device: GpuSgm.session + constructor (src/main/java/sgm/GpuSgm.java:163-221).
+ * CSGM_E_NODEVICE when the index does not exist (the reference's "No OpenCL GPU at index"). */
+int csgm_session_open(int32_t device, csgm_session** session);
+
+/* Close a session and free its device memory: GpuSgm.closeSession (src/main/java/sgm/GpuSgm.java:392-397). */
+void csgm_session_close(csgm_session* session);
+
+/* Device memory budget in bytes (0 = 70% of device memory): GpuSgm.budget
+ * (src/main/java/sgm/GpuSgm.java:629-633). */
+int csgm_session_set_budget(csgm_session* session, int64_t bytes);
+
+/* Device bytes csgm_pair needs for a w x h pair; CSGM_E_NOMEM if it exceeds the session budget.
+ * Replaces the resident branch of GpuStereo.plan (src/main/java/sgm/GpuStereo.java:33-54). */
+int csgm_plan(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
+              int64_t* device_bytes);
+
+/* Largest disparity count whose plan fits the budget (0 if none):
+ * GpuSgm.disparityLimit / GpuStereo.limit (src/main/java/sgm/GpuSgm.java:237-245,
+ * src/main/java/sgm/GpuStereo.java:86-94). */
+int csgm_disparity_limit(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
+                         int32_t* limit);
+
+/* Accumulated device timing since the last reset (reset != 0 clears it afterwards). */
+int csgm_profile_get(csgm_session* session, csgm_profile* out, int32_t reset);
+
+/* ---- the hot path ------------------------------------------------------------------------ */
+
+/*
+ * One view of the matcher: cost volume, path aggregation, WTA, uniqueness and parabolic subpixel.
+ * Exact drop-in for GpuSgm.match -> GpuStereo.execute (src/main/java/sgm/GpuSgm.java:267-303,
+ * src/main/java/sgm/GpuStereo.java:170-210), i.e. for the CPU loops CensusSgm.match
+ * (src/main/java/sgm/CensusSgm.java:375-516).
+ *   desc_a/desc_b : [words][w*h] census words of the matching/target view (words = ceil(bits/64))
+ *   gray_a/gray_b : matching/target images (edge-aware P2 and the AD/gradient/ZNCC costs)
+ *   tex_a/tex_b   : textured & valid masks
+ *   reverse       : 0 = left view (target x - d), 1 = right view (target x + d)
+ *   out_disp      : float[w*h], NaN where no disparity is selected
+ *   out_summary   : optional int32[6*w*h] winners record (best, value, second, before, after,
+ *                   full-interval flags), src/main/java/sgm/GpuStereo.java:758-769
+ *   reasons       : optional uint8[w*h]; pixels decided here get 0 (selected), 2 (boundary) or
+ *                   3 (ambiguous); others are left as the caller set them
+ *   boundary      : optional uint8[w*h] searchBoundary flags (4 full interval, |1 lower, |2 upper)
+ *   stats         : optional; the six selection counters are ADDED to it, as GpuSgm.match merges
+ *                   them (src/main/java/sgm/GpuSgm.java:289-294)
+ */
+int csgm_match(csgm_session* session, const csgm_params* params, const uint64_t* desc_a,
+               const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
+               const uint8_t* tex_a, const uint8_t* tex_b, int32_t w, int32_t h, int32_t reverse,
+               float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
+               csgm_stats* stats);
+
+/*
+ * A whole rectified pair on the GPU: census + texture masks of both images (masks ANDed with the
+ * optional validity masks), left and right views, and the left-right check.  Replaces
+ * CensusSgm.computeRecorded up to the LR check (src/main/java/sgm/CensusSgm.java:56-201).
+ *   left/right      : uint8[w*h] rectified images
+ *   valid_l/valid_r : optional uint8[w*h] validity masks (both or neither)
+ *   lr_checked      : float[w*h] left disparities that pass the LR check, NaN elsewhere
+ *   disp_l/disp_r   : optional float[w*h] raw left/right view disparities (dl, dr)
+ *   reasons         : optional uint8[w*h]; set to 1 everywhere, then 0/2/3 by the left view and 4
+ *                     by the LR check (src/main/java/sgm/CensusSgm.java:104-106,190,198)
+ *   boundary        : optional uint8[w*h] searchBoundary flags of the left view
+ *   stats           : optional; overwritten with the left view's counters plus lr_rejected
+ */
+int csgm_pair(csgm_session* session, const csgm_params* params, const uint8_t* left,
+              const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r, int32_t w,
+              int32_t h, float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+              uint8_t* boundary, csgm_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COLLINEA_SGM_H */
