@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 stereo matcher: SGM Gcells/s (pixels x disparities per pair).
+
+One step = one rectified pair through the whole hot path (census + texture of both images, the
+left and right views with 8-path aggregation, WTA + uniqueness + parabolic subpixel, the LR check)
+on the 1600x1067 D=128 Census 9x7 workload (synthetic pair, seeded).  Per GPU the work is fixed
+(weak scaling: every rank matches its own pair; no collective on the data path).
+
+  value  device time of K steps, CUDA events on the library's stream, inputs resident in HBM
+         (csgm_pair_device); L2 flushed (256 MiB memset) before every step, outside the timing.
+  e2e    the same metric through csgm_pair with pinned host buffers: every step uploads the two
+         images and downloads the LR-checked disparities and counters (wall clock).
+  --impl reference  the reference's CPU matcher (the oracle restatement) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SGM Gcells/s (px×disp) bit-exact; batched pairs/s & p50/p99 vs per-pair GPU"
+WORKLOADS = {
+    "cfg0": dict(spec="cfg0", census=(9, 7), D=64, cost="census", p1=10, p2=120),
+    "cfg1": dict(spec="cfg1", census=(9, 7), D=128, cost="census", p1=10, p2=120),
+    "cfg1-gradient": dict(spec="cfg1", census=(9, 7), D=128, cost="census-gradient", p1=10,
+                          p2=120),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfg1")
+    ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_params(name: str):
+    from pose_b200.options import Options
+    from pose_b200.stereo_cost import params_from_options
+
+    wl = WORKLOADS[name]
+    o = Options()
+    o.census, o.censusHeight = wl["census"]
+    o.disparities, o.matchingCost, o.directions = wl["D"], wl["cost"], 8
+    prm = params_from_options(o)
+    prm.p1, prm.p2 = wl["p1"], wl["p2"]  # the workload's effective penalties
+    return prm
+
+
+def workload_desc(name: str, prm) -> str:
+    wl = WORKLOADS[name]
+    from pose_b200.synthetic import spec_for
+
+    s = spec_for(wl["spec"])
+    return (f"{s.width}x{s.height} D{prm.disparities} {wl['cost']} {prm.window_x}x{prm.window_y} "
+            f"{prm.directions}-path P1={prm.p1} P2={prm.p2} uint{8 * prm.aggregate_bytes} "
+            "aggregate, WTA+subpixel, LR check; both views per pair")
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", self.gpu], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int):
+    """Algorithmic HBM bytes of one launch of `kernel` (the per-cell figures of the roofline
+    model: uint8 cost volume written once, read once per sweep; the partial aggregate written by
+    one sweep and read by the other).  None for kernels outside the model."""
+    cells = w * h * prm.disparities
+    sb = prm.aggregate_bytes
+    table = {
+        "cost_volume": 1,                 # one view's uint8 cost volume, written once
+        "paths_line": 1 + 2 * sb,         # one direction: cost read + aggregate read-modify-write
+        "winners": 1 + sb,                # cost validity + aggregate read
+        "sweep_down": 2 * (1 + sb),       # both views: cost read + partial aggregate write
+        "sweep_up": 2 * (1 + sb),         # both views: cost read + partial aggregate read
+        "cost_pair": 2,                   # both views' uint8 cost volumes, written once
+    }
+    if kernel not in table:
+        return None
+    return table[kernel] * cells
+
+
+def read_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch from the committed ncu summary of this workload, if any."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{workload}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return int(float(parts[1]))
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_baseline(prm, left, right, w, h, rows: int, threads: int):
+    """The oracle on a bounded band of the workload (full width, `rows` rows)."""
+    import numpy as np
+
+    import oracle.oracle as orc
+
+    y0 = (h - rows) // 2
+    band_l = np.ascontiguousarray(left.reshape(h, w)[y0:y0 + rows]).reshape(-1)
+    band_r = np.ascontiguousarray(right.reshape(h, w)[y0:y0 + rows]).reshape(-1)
+    orc.set_threads(threads)
+    t = time.perf_counter()
+    orc.pair(prm, band_l, band_r, w, rows)
+    dt = time.perf_counter() - t
+    return w * rows * prm.disparities / dt / 1e9, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from pose_b200.synthetic import make_pair, spec_for
+
+    prm = workload_params(args.workload)
+    spec = spec_for(WORKLOADS[args.workload]["spec"])
+    left, right, _ = make_pair(spec)
+    w, h = spec.width, spec.height
+    threads = os.cpu_count() or 1
+    rows = args.cpu_rows or max(prm.window_y + 2, h // 8)
+    values = []
+    for i in range(args.warmup + args.steps):
+        v, _ = cpu_baseline(prm, left, right, w, h, rows, threads)
+        if i >= args.warmup:
+            values.append(v)
+    value = statistics.median(values)
+    cells = w * rows * prm.disparities
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": cells / (value * 1e9) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "cfg1 " + workload_desc(args.workload, prm),
+                   "sample": f"{w}x{rows} full-width band of the pair"},
+        "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
+                         "sample": f"{w}x{rows} band, census+both views+LR, {threads} threads"},
+        "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from pose_b200 import _abi
+    from pose_b200._abi import CsgmStats, check
+    from pose_b200.sgm import GpuSgm
+    from pose_b200.synthetic import make_pair, spec_for
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    prm = workload_params(args.workload)
+    spec = spec_for(WORKLOADS[args.workload]["spec"], seed_offset=rank)
+    left, right, _ = make_pair(spec)
+    w, h, n = spec.width, spec.height, spec.width * spec.height
+    cells = n * prm.disparities
+    lib = _abi.load()
+    session = GpuSgm(local)
+
+    # Device-resident inputs/outputs (torch is only the allocator here).
+    d_left = torch.from_numpy(left).to(f"cuda:{local}")
+    d_right = torch.from_numpy(right).to(f"cuda:{local}")
+    d_checked = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step_device():
+        check(lib.csgm_pair_device(session.handle, ctypes.byref(prm), d_left.data_ptr(),
+                                   d_right.data_ptr(), None, None, w, h, d_checked.data_ptr(),
+                                   None, None, None, None, None, 1))
+
+    def flush_l2():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    session.set_profiling(2)
+    for _ in range(args.warmup):
+        flush_l2()
+        step_device()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    session.profile(reset=True)
+    session.kernel_times(reset=True)
+    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local] \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else str(local)
+    clocks = ClockSampler(gpu_index)
+    clocks.start()
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush_l2()
+        step_device()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop()
+    prof = session.profile(reset=True)
+    kernels = session.kernel_times(reset=True)
+    device_s = prof["kernel_ns"] / 1e9
+    launches = int(prof["launches"])
+    if dist:
+        t = torch.tensor([device_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        device_s = float(t.item())
+        dist.barrier()
+    value = cells * args.steps * world / device_s / 1e9
+    ms_per_step = device_s / args.steps * 1e3
+
+    # End to end through csgm_pair with pinned host buffers.
+    pin_l = torch.from_numpy(left).pin_memory()
+    pin_r = torch.from_numpy(right).pin_memory()
+    pin_out = torch.empty(n, dtype=torch.float32).pin_memory()
+    stats = CsgmStats()
+    session.set_profiling(0)
+
+    def step_host():
+        check(lib.csgm_pair(session.handle, ctypes.byref(prm), pin_l.data_ptr(), pin_r.data_ptr(),
+                            None, None, w, h, pin_out.data_ptr(), None, None, None, None,
+                            ctypes.byref(stats)))
+
+    for _ in range(max(1, args.warmup)):
+        step_host()
+    if dist:
+        dist.barrier()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_host()
+    e2e_s = time.perf_counter() - e0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = cells * args.steps * world / e2e_s / 1e9
+
+    # Roofline of the dominant kernel (largest share of device time in the timed region).
+    roofline = None
+    if kernels:
+        name, (count, total_ns) = max(kernels.items(), key=lambda kv: kv[1][1])
+        per_launch = algorithmic_bytes_per_launch(name, prm, w, h)
+        peak, peak_kind = measured_peak_gbs()
+        if per_launch and count:
+            achieved = per_launch / (total_ns / count / 1e9) / 1e9
+            roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1),
+                        "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4),
+                        "traffic": read_traffic(args.workload, name),
+                        "algorithmic_bytes_per_launch": per_launch,
+                        "avg_launch_ms": round(total_ns / count / 1e6, 4),
+                        "share": round(total_ns / max(1, sum(v[1] for v in kernels.values())), 3)}
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rows = args.cpu_rows or max(prm.window_y + 2, h // 8)
+        v, dt = cpu_baseline(prm, left, right, w, h, rows, 1)
+        baseline = {"value": v, "unit": "Gcells/s", "cores": 1, "kind": "port",
+                    "sample": f"{w}x{rows} full-width band of the pair, both views + LR "
+                              f"({dt:.1f} s, 1 thread)"}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Gcells/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+        "data": "synthetic",
+        "config": {"workload": args.workload + " " + workload_desc(args.workload, prm),
+                   "pairs_per_step_per_gpu": 1,
+                   "l2": "flushed before every step (256 MiB memset, untimed)",
+                   "parallelism": f"replicas x{world}", "wall_ms_per_step": round(
+                       wall / args.steps * 1e3, 4)},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Gcells/s", "h2d_bytes_per_step": 2 * n,
+                "d2h_bytes_per_step": 4 * n + ctypes.sizeof(CsgmStats)},
+        "roofline": roofline,
+        "cpu_baseline": baseline,
+        "clocks": clock_info,
+        "gpu_launches": launches,
+        "kernels": {k: {"launches": c, "ms": round(t / 1e6, 3)} for k, (c, t) in kernels.items()},
+    }
+    session.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

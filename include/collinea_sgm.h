@@ -165,6 +165,25 @@ int csgm_disparity_limit(csgm_session* session, const csgm_params* params, int32
 /* Accumulated device timing since the last reset (reset != 0 clears it afterwards). */
 int csgm_profile_get(csgm_session* session, csgm_profile* out, int32_t reset);
 
+/* Per-kernel device time, measured with CUDA events on the session's stream when profiling
+ * level 2 is on.  The reference collects the same per-kernel sums from OpenCL profiling events
+ * (src/main/java/sgm/GpuSgm.java:558-590). */
+typedef struct csgm_kernel_time {
+  char name[32];
+  int64_t launches;
+  int64_t total_ns;
+} csgm_kernel_time;
+
+/* 0 = off, 1 = per-call timing (csgm_profile), 2 = per-call and per-kernel timing. */
+int csgm_session_set_profiling(csgm_session* session, int32_t level);
+
+/* Copies up to `capacity` per-kernel records; *count receives the number of kernels seen. */
+int csgm_kernel_times(csgm_session* session, csgm_kernel_time* out, int32_t capacity,
+                      int32_t* count, int32_t reset);
+
+/* Waits for all work queued on the session's stream. */
+int csgm_session_synchronize(csgm_session* session);
+
 /* ---- the hot path ------------------------------------------------------------------------ */
 
 /*
@@ -208,6 +227,18 @@ int csgm_pair(csgm_session* session, const csgm_params* params, const uint8_t* l
               const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r, int32_t w,
               int32_t h, float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
               uint8_t* boundary, csgm_stats* stats);
+
+/*
+ * csgm_pair on device-resident buffers: every image/mask/output pointer is a device pointer on the
+ * session's device (outputs may be NULL except lr_checked).  For callers whose rectified images
+ * are already in HBM (a GPU rectifier upstream, or a batch driver).  With sync == 0 the call only
+ * queues work on the session's stream and `stats` must be NULL; csgm_session_synchronize waits.
+ * Same semantics as csgm_pair otherwise.
+ */
+int csgm_pair_device(csgm_session* session, const csgm_params* params, const uint8_t* left,
+                     const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
+                     int32_t w, int32_t h, float* lr_checked, float* disp_l, float* disp_r,
+                     uint8_t* reasons, uint8_t* boundary, csgm_stats* stats, int32_t sync);
 
 #ifdef __cplusplus
 }

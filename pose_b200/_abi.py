@@ -94,6 +94,14 @@ class CsgmProfile(ctypes.Structure):
     ]
 
 
+class CsgmKernelTime(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches", ctypes.c_int64),
+        ("total_ns", ctypes.c_int64),
+    ]
+
+
 class CsgmError(RuntimeError):
     """A non-zero status from the C ABI, with the library's thread-local message."""
 
@@ -132,6 +140,17 @@ SIGNATURES = {
         [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(_I32)],
     ),
     "csgm_profile_get": (ctypes.c_int, [_P, ctypes.POINTER(CsgmProfile), _I32]),
+    "csgm_session_set_profiling": (ctypes.c_int, [_P, _I32]),
+    "csgm_kernel_times": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmKernelTime), _I32, ctypes.POINTER(_I32), _I32],
+    ),
+    "csgm_session_synchronize": (ctypes.c_int, [_P]),
+    "csgm_pair_device": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
+         ctypes.POINTER(CsgmStats), _I32],
+    ),
     "csgm_match": (
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P,

@@ -1,0 +1,336 @@
+// pipeline.cu - stage sequences of the matcher on one CUDA stream.
+//
+// A pair (CensusSgm.computeRecorded :56-201): census + texture of both images, the left view
+// (CensusSgm.match with reverse=false), the right view (reverse=true), the left-right check.
+// A view: cost volume, path aggregation, winner selection.
+#include <cmath>
+#include <cstring>
+
+#include "pipeline.h"
+#include "stereo_fused.h"
+#include "stereo_kernels.h"
+
+namespace csgm {
+
+#define CK(expr, what)                                 \
+  do {                                                 \
+    cudaError_t e_ = (expr);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+#define WS(var, type, slot, bytes)                            \
+  type* var = (type*)ctx.ws->get((slot), (bytes), &status);   \
+  if (!var) return status;
+
+static int words_of(const csgm_params& p) { return (p.window_x * p.window_y - 1 + 63) / 64; }
+
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
+  size_t n = (size_t)w * h, D = (size_t)p.disparities, words = (size_t)words_of(p);
+  size_t bytes = 0;
+  bytes += 2 * n * words * 8;  // descriptors
+  bytes += 2 * n;              // texture masks
+  bytes += 2 * n * 4;          // raw view disparities
+  bytes += sizeof(DeviceStats);
+  if (fused_supported(p))
+    bytes += fused_workspace_bytes(p, w, h);
+  else
+    bytes += n * D * 2 + n * D * p.aggregate_bytes;  // one cost volume + one aggregate
+  if (host_inputs) bytes += 4 * n + n * 4 + 2 * n;  // images, masks, checked, reasons, boundary
+  return bytes;
+}
+
+// One view through the general kernels: cost volume, every path, selection.
+static int run_view_general(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                            const uint64_t* desc_b, const uint8_t* tex_a, const uint8_t* tex_b,
+                            const uint8_t* gray_a, const uint8_t* gray_b, int w, int h,
+                            int reverse, float* out, int32_t* summary, uint8_t* reasons,
+                            uint8_t* boundary, DeviceStats* dstats) {
+  int status = CSGM_OK;
+  size_t n = (size_t)w * h, D = (size_t)p.disparities;
+  WS(cost, uint16_t, kCostL, n * D * 2);
+  WS(sum, void, kSum, n * D * p.aggregate_bytes);
+  CostArgs c{desc_a, desc_b, tex_a, tex_b, gray_a, gray_b, cost, w, h, p.disparities,
+             p.min_disparity, reverse, p.window_x, p.window_y, words_of(p), p.cost_mode,
+             p.census_weight_milli, p.ad_truncation, p.gradient_truncation,
+             p.window_x * p.window_y - 1};
+  ctx.prof->kernel_begin();
+  CK(launch_cost_volume(c, ctx.sm_count, ctx.stream), "cost kernel launch");
+  ctx.prof->kernel_end("cost_volume");
+  CK(cudaMemsetAsync(sum, 0, n * D * p.aggregate_bytes, ctx.stream), "aggregate clear");
+  for (int d = 0; d < p.directions; d++) {
+    PathArgs a{cost, tex_a, gray_a, w, h, p.disparities, 0, 0, p.p1, p.p2, p.edge_scale};
+    direction(d, a.dx, a.dy);
+    ctx.prof->kernel_begin();
+    CK(launch_paths_line(a, sum, p.aggregate_bytes, ctx.sm_count, ctx.stream),
+       "paths kernel launch");
+    ctx.prof->kernel_end("paths_line");
+  }
+  SelectArgs s{cost, out, summary, reasons, boundary, dstats, w, h, p.disparities,
+               p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+  ctx.prof->kernel_begin();
+  CK(launch_winners(s, sum, p.aggregate_bytes, ctx.sm_count, ctx.stream), "winners kernel launch");
+  ctx.prof->kernel_end("winners");
+  return CSGM_OK;
+}
+
+static void copy_stats(const DeviceStats& d, csgm_stats* out, bool add) {
+  if (!add) memset(out, 0, sizeof *out);
+  out->lower_boundary_rejected += (int64_t)d.lower_boundary_rejected;
+  out->full_interval_pixels += (int64_t)d.full_interval_pixels;
+  out->boundary_rejected += (int64_t)d.boundary_rejected;
+  out->upper_boundary_rejected += (int64_t)d.upper_boundary_rejected;
+  out->ambiguity_rejected += (int64_t)d.ambiguity_rejected;
+  out->selected += (int64_t)d.selected;
+  out->lr_rejected += (int64_t)d.lr_rejected;
+}
+
+static float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ms;
+}
+
+// The device part of a pair.  `own_call` = this is the whole call (csgm_pair_device), so it owns
+// the call-level timing; csgm_pair times its own copies around it.
+static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* left,
+                          const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
+                          int w, int h, float* lr_checked, float* disp_l, float* disp_r,
+                          uint8_t* reasons, uint8_t* boundary, csgm_stats* stats, bool sync,
+                          bool own_call) {
+  int status = CSGM_OK;
+  size_t n = (size_t)w * h;
+  int words = words_of(p);
+  if (own_call) ctx.prof->begin_call(ctx.stream);
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (own_call && ctx.prof->level >= 1) {
+    t0 = ctx.prof->event();
+    t1 = ctx.prof->event();
+    CK(cudaEventRecord(t0, ctx.stream), "event record");
+  }
+  WS(desc_l, uint64_t, kDescL, n * words * 8);
+  WS(desc_r, uint64_t, kDescR, n * words * 8);
+  WS(tex_l, uint8_t, kTexL, n);
+  WS(tex_r, uint8_t, kTexR, n);
+  WS(dstats, DeviceStats, kStats, sizeof(DeviceStats));
+  if (!disp_l) {
+    WS(buf, float, kDispL, n * 4);
+    disp_l = buf;
+  }
+  if (!disp_r) {
+    WS(buf, float, kDispR, n * 4);
+    disp_r = buf;
+  }
+  CK(cudaMemsetAsync(dstats, 0, sizeof(DeviceStats), ctx.stream), "stats clear");
+  if (reasons) CK(cudaMemsetAsync(reasons, 1, n, ctx.stream), "reasons init");
+  if (boundary) CK(cudaMemsetAsync(boundary, 0, n, ctx.stream), "boundary init");
+  // CensusSgm.java:122-134: descriptors, texture masks, AND with the validity masks.
+  CensusArgs ca{};
+  ca.image[0] = {left, valid_l, desc_l, tex_l};
+  ca.image[1] = {right, valid_r, desc_r, tex_r};
+  ca.w = w;
+  ca.h = h;
+  ca.wx = p.window_x;
+  ca.wy = p.window_y;
+  ca.words = words;
+  ctx.prof->kernel_begin();
+  CK(launch_census_texture(ca, 2, ctx.stream), "census kernel launch");
+  ctx.prof->kernel_end("census_texture");
+  if (fused_supported(p)) {
+    // Both views in one pass structure (stereo_fused.cu).
+    FusedViews v{desc_l, desc_r, tex_l, tex_r, left, right, disp_l, disp_r, reasons, boundary,
+                 dstats};
+    status = run_views_fused(ctx, p, v, w, h);
+    if (status) return status;
+  } else {
+    status = run_view_general(ctx, p, desc_l, desc_r, tex_l, tex_r, left, right, w, h, 0, disp_l,
+                              nullptr, reasons, boundary, dstats);
+    if (status) return status;
+    // Right view: a/b, masks and grays swapped, reverse=true; its counters are discarded
+    // (CensusSgm.java:149-162 passes a fresh Stats and no reasons).
+    status = run_view_general(ctx, p, desc_r, desc_l, tex_r, tex_l, right, left, w, h, 1, disp_r,
+                              nullptr, nullptr, nullptr, nullptr);
+    if (status) return status;
+  }
+  LrArgs lr{disp_l, disp_r, lr_checked, reasons, dstats, w, h, p.window_x, p.window_y,
+            p.lr_threshold};
+  ctx.prof->kernel_begin();
+  CK(launch_lr_check(lr, ctx.sm_count, ctx.stream), "LR kernel launch");
+  ctx.prof->kernel_end("lr_check");
+  if (t1) CK(cudaEventRecord(t1, ctx.stream), "event record");
+  if (!sync) return CSGM_OK;
+  DeviceStats host{};
+  CK(cudaMemcpyAsync(&host, dstats, sizeof host, cudaMemcpyDeviceToHost, ctx.stream),
+     "stats readback");
+  CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (stats) copy_stats(host, stats, false);
+  if (t1) {
+    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(t0, t1) * 1e6);
+    ctx.profile->calls++;
+  }
+  ctx.prof->collect();
+  return CSGM_OK;
+}
+
+int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
+                    const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
+                    float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                    uint8_t* boundary, csgm_stats* stats, bool sync) {
+  return pair_on_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
+                        reasons, boundary, stats, sync, true);
+}
+
+int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
+                  const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
+                  float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                  uint8_t* boundary, csgm_stats* stats) {
+  int status = CSGM_OK;
+  size_t n = (size_t)w * h;
+  WS(d_left, uint8_t, kImgL, n);
+  WS(d_right, uint8_t, kImgR, n);
+  uint8_t *d_vl = nullptr, *d_vr = nullptr;
+  if (valid_l) {
+    WS(a, uint8_t, kValidL, n);
+    WS(b, uint8_t, kValidR, n);
+    d_vl = a;
+    d_vr = b;
+  }
+  WS(d_checked, float, kChecked, n * 4);
+  WS(d_dl, float, kDispL, n * 4);
+  WS(d_dr, float, kDispR, n * 4);
+  uint8_t* d_reasons = nullptr;
+  uint8_t* d_boundary = nullptr;
+  if (reasons) {
+    WS(r, uint8_t, kReasons, n);
+    d_reasons = r;
+  }
+  if (boundary) {
+    WS(b, uint8_t, kBoundary, n);
+    d_boundary = b;
+  }
+  // Reserve the pipeline's own buffers before the upload so a budget failure costs no copies.
+  int64_t needed = (int64_t)pair_workspace_bytes(p, w, h, true);
+  if ((size_t)needed > ctx.ws->budget)
+    return fail(CSGM_E_NOMEM,
+                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
+                needed / 1048576.0, ctx.ws->budget / 1048576.0);
+  cudaEvent_t u0 = nullptr, u1 = nullptr, d0 = nullptr, d1 = nullptr;
+  bool timed = ctx.prof->level >= 1;
+  ctx.prof->begin_call(ctx.stream);
+  if (timed) {
+    u0 = ctx.prof->event();
+    u1 = ctx.prof->event();
+    d0 = ctx.prof->event();
+    d1 = ctx.prof->event();
+    CK(cudaEventRecord(u0, ctx.stream), "event record");
+  }
+  CK(cudaMemcpyAsync(d_left, left, n, cudaMemcpyHostToDevice, ctx.stream), "image upload");
+  CK(cudaMemcpyAsync(d_right, right, n, cudaMemcpyHostToDevice, ctx.stream), "image upload");
+  if (valid_l) {
+    CK(cudaMemcpyAsync(d_vl, valid_l, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
+    CK(cudaMemcpyAsync(d_vr, valid_r, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
+  }
+  if (timed) CK(cudaEventRecord(u1, ctx.stream), "event record");
+  status = pair_on_device(ctx, p, d_left, d_right, d_vl, d_vr, w, h, d_checked, d_dl, d_dr,
+                          d_reasons, d_boundary, nullptr, false, false);
+  if (status) return status;
+  if (timed) CK(cudaEventRecord(d0, ctx.stream), "event record");
+  CK(cudaMemcpyAsync(lr_checked, d_checked, n * 4, cudaMemcpyDeviceToHost, ctx.stream),
+     "disparity readback");
+  if (disp_l)
+    CK(cudaMemcpyAsync(disp_l, d_dl, n * 4, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  if (disp_r)
+    CK(cudaMemcpyAsync(disp_r, d_dr, n * 4, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  if (reasons)
+    CK(cudaMemcpyAsync(reasons, d_reasons, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  if (boundary)
+    CK(cudaMemcpyAsync(boundary, d_boundary, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  DeviceStats host{};
+  WS(dstats, DeviceStats, kStats, sizeof(DeviceStats));
+  CK(cudaMemcpyAsync(&host, dstats, sizeof host, cudaMemcpyDeviceToHost, ctx.stream),
+     "stats readback");
+  if (timed) CK(cudaEventRecord(d1, ctx.stream), "event record");
+  CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (stats) copy_stats(host, stats, false);
+  if (timed) {
+    ctx.profile->upload_ns += (int64_t)(elapsed_ms(u0, u1) * 1e6);
+    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(u1, d0) * 1e6);
+    ctx.profile->download_ns += (int64_t)(elapsed_ms(d0, d1) * 1e6);
+    ctx.profile->uploaded_bytes += (int64_t)(valid_l ? 4 * n : 2 * n);
+    ctx.profile->downloaded_bytes += (int64_t)(n * 4 * (1 + (disp_l != 0) + (disp_r != 0)) +
+                                               (reasons ? n : 0) + (boundary ? n : 0));
+    ctx.profile->calls++;
+  }
+  ctx.prof->collect();
+  return CSGM_OK;
+}
+
+int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                   const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
+                   const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
+                   float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
+                   csgm_stats* stats) {
+  int status = CSGM_OK;
+  size_t n = (size_t)w * h, D = (size_t)p.disparities;
+  int words = words_of(p);
+  size_t needed = 2 * n * words * 8 + 6 * n + n * 4 + (out_summary ? 24 * n : 0) +
+                  n * D * (2 + p.aggregate_bytes);
+  if (needed > ctx.ws->budget)
+    return fail(CSGM_E_NOMEM,
+                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
+                needed / 1048576.0, ctx.ws->budget / 1048576.0);
+  WS(d_a, uint64_t, kDescL, n * words * 8);
+  WS(d_b, uint64_t, kDescR, n * words * 8);
+  WS(d_ga, uint8_t, kImgL, n);
+  WS(d_gb, uint8_t, kImgR, n);
+  WS(d_ta, uint8_t, kTexL, n);
+  WS(d_tb, uint8_t, kTexR, n);
+  WS(d_out, float, kDispL, n * 4);
+  WS(dstats, DeviceStats, kStats, sizeof(DeviceStats));
+  int32_t* d_summary = nullptr;
+  uint8_t *d_reasons = nullptr, *d_boundary = nullptr;
+  if (out_summary) {
+    WS(s, int32_t, kSummary, n * 24);
+    d_summary = s;
+  }
+  if (reasons) {
+    WS(r, uint8_t, kReasons, n);
+    d_reasons = r;
+  }
+  if (boundary) {
+    WS(b, uint8_t, kBoundary, n);
+    d_boundary = b;
+  }
+  ctx.prof->begin_call(ctx.stream);
+  CK(cudaMemcpyAsync(d_a, desc_a, n * words * 8, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemcpyAsync(d_b, desc_b, n * words * 8, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemcpyAsync(d_ga, gray_a, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemcpyAsync(d_gb, gray_b, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemcpyAsync(d_ta, tex_a, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemcpyAsync(d_tb, tex_b, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  // Untouched pixels keep the caller's codes, as GpuSgm.match clones and copies them back.
+  if (reasons) CK(cudaMemcpyAsync(d_reasons, reasons, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  if (boundary)
+    CK(cudaMemcpyAsync(d_boundary, boundary, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
+  CK(cudaMemsetAsync(dstats, 0, sizeof(DeviceStats), ctx.stream), "stats clear");
+  status = run_view_general(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
+                            d_summary, d_reasons, d_boundary, dstats);
+  if (status) return status;
+  CK(cudaMemcpyAsync(out_disp, d_out, n * 4, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  if (out_summary)
+    CK(cudaMemcpyAsync(out_summary, d_summary, n * 24, cudaMemcpyDeviceToHost, ctx.stream),
+       "readback");
+  if (reasons) CK(cudaMemcpyAsync(reasons, d_reasons, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  if (boundary)
+    CK(cudaMemcpyAsync(boundary, d_boundary, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  DeviceStats host{};
+  CK(cudaMemcpyAsync(&host, dstats, sizeof host, cudaMemcpyDeviceToHost, ctx.stream), "readback");
+  CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (stats) copy_stats(host, stats, true);
+  ctx.prof->collect();
+  return CSGM_OK;
+}
+
+}  // namespace csgm

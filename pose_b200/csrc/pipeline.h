@@ -1,0 +1,90 @@
+// pipeline.h - session workspace, profiler and the stage sequences behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/collinea_sgm.h"
+
+namespace csgm {
+
+int fail(int status, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+int validate_params(const csgm_params* p, int w, int h);
+
+enum Slot {
+  kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
+  kCostL, kCostR, kSum, kSumR, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
+  kCarry, kFlags, kSlotCount
+};
+
+// Device buffers owned by a session, grown on demand inside the memory budget.
+struct Workspace {
+  struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+  };
+  Buffer buffers[kSlotCount];
+  size_t allocated = 0;
+  size_t budget = 0;
+  void* get(int slot, size_t bytes, int* status);
+  void release_all();
+};
+
+struct Profiler {
+  struct Pending {
+    std::string name;
+    cudaEvent_t start, stop;
+  };
+  struct KernelTotal {
+    std::string name;
+    int64_t launches;
+    int64_t total_ns;
+  };
+  int level = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaEvent_t> events;
+  size_t used = 0;
+  cudaEvent_t current_start = nullptr;
+  std::vector<Pending> pending;
+  std::vector<KernelTotal> kernels;
+  int64_t launches = 0;
+  void begin_call(cudaStream_t s);
+  cudaEvent_t event();
+  void kernel_begin();
+  void kernel_end(const char* name);
+  void collect();
+  ~Profiler();
+};
+
+struct Context {
+  cudaStream_t stream;
+  int sm_count;
+  Workspace* ws;
+  Profiler* prof;
+  csgm_profile* profile;
+};
+
+// Bytes of device workspace a pair needs (host_inputs: include the upload/download staging).
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs);
+
+int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
+                    const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
+                    float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                    uint8_t* boundary, csgm_stats* stats, bool sync);
+
+int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
+                  const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
+                  float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                  uint8_t* boundary, csgm_stats* stats);
+
+int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                   const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
+                   const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
+                   float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
+                   csgm_stats* stats);
+
+}  // namespace csgm

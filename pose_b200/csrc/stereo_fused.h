@@ -1,0 +1,29 @@
+// stereo_fused.h - fast path for D <= 256: both views aggregated by fused sweeps.
+#pragma once
+
+#include <cstdint>
+
+#include "pipeline.h"
+#include "sgm_device.cuh"
+
+namespace csgm {
+
+struct FusedViews {
+  const uint64_t* desc_l;
+  const uint64_t* desc_r;
+  const uint8_t* tex_l;
+  const uint8_t* tex_r;
+  const uint8_t* gray_l;
+  const uint8_t* gray_r;
+  float* disp_l;
+  float* disp_r;
+  uint8_t* reasons;   // left view only
+  uint8_t* boundary;  // left view only
+  DeviceStats* stats; // left view only
+};
+
+bool fused_supported(const csgm_params& p);
+size_t fused_workspace_bytes(const csgm_params& p, int w, int h);
+int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h);
+
+}  // namespace csgm

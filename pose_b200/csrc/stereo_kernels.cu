@@ -1,0 +1,379 @@
+// stereo_kernels.cu - general stereo kernels for sm_100a: census + texture masks, the cost
+// volume (four cost modes), path aggregation with one warp per line (any D up to 4096, any
+// direction set, uint16 or uint32 aggregate), winner selection with subpixel refinement, and the
+// left-right check.  These are the general path; stereo_fused.cu holds the fast path for D <= 256.
+//
+// Reference semantics (paths relative to the reference project root):
+//   census / texture     src/main/java/sgm/CensusSgm.java:523-555
+//   cost modes           src/main/java/sgm/StereoCost.java:50-90
+//   aggregation          src/main/java/sgm/CensusSgm.java:421-459
+//   selection            src/main/java/sgm/CensusSgm.java:460-515, GpuStereo.java:631-687,758-769
+//   left-right check     src/main/java/sgm/CensusSgm.java:181-201
+#include "stereo_kernels.h"
+
+#include <cfloat>
+#include <climits>
+
+namespace csgm {
+
+// ---------------------------------------------------------------------------------------------
+// Census descriptors and texture masks (CensusSgm.java:523-555), both images in one launch.
+// blockIdx.z selects the image.  Border pixels get zero descriptors and are untextured.
+__global__ void census_texture_kernel(CensusArgs args) {
+  const CensusImage& im = args.image[blockIdx.z];
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int w = args.w, h = args.h;
+  if (x >= w || y >= h) return;
+  int rx = args.wx / 2, ry = args.wy / 2;
+  int64_t n = (int64_t)w * h, p = (int64_t)y * w + x;
+  uint64_t w0 = 0, w1 = 0;
+  uint8_t textured = 0;
+  if (x >= rx && x < w - rx && y >= ry && y < h - ry) {
+    int center = im.img[p], bit = 0, low = 255, high = 0;
+    for (int yy = -ry; yy <= ry; yy++) {
+      const uint8_t* row = im.img + (int64_t)(y + yy) * w + x;
+      for (int xx = -rx; xx <= rx; xx++) {
+        int v = row[xx];
+        low = min(low, v);
+        high = max(high, v);
+        if (xx == 0 && yy == 0) continue;
+        if (v < center) {
+          if (bit < 64)
+            w0 |= 1ull << bit;
+          else
+            w1 |= 1ull << (bit - 64);
+        }
+        bit++;
+      }
+    }
+    textured = high - low >= 4 && (im.valid == nullptr || im.valid[p] != 0);
+  }
+  im.desc[p] = w0;
+  if (args.words > 1) im.desc[n + p] = w1;
+  im.tex[p] = textured;
+}
+
+// ---------------------------------------------------------------------------------------------
+// StereoCost.value (StereoCost.java:50-90) for matching pixel p and target q.
+__device__ __forceinline__ int cell_cost(const CostArgs& a, int64_t p, int64_t q, int64_t n) {
+  int hamming = __popcll(a.desc_a[p] ^ a.desc_b[q]);
+  if (a.words > 1) hamming += __popcll(a.desc_a[n + p] ^ a.desc_b[n + q]);
+  if (a.mode == CSGM_COST_CENSUS) return hamming;
+  if (a.mode == CSGM_COST_AD_CENSUS || a.mode == CSGM_COST_CENSUS_GRADIENT) {
+    int difference, cap;
+    if (a.mode == CSGM_COST_AD_CENSUS) {
+      difference = abs((int)a.gray_a[p] - (int)a.gray_b[q]);
+      cap = a.ad_cap;
+    } else {
+      int w = a.w;
+      int ax = (int)a.gray_a[p + 1] - (int)a.gray_a[p - 1];
+      int ay = (int)a.gray_a[p + w] - (int)a.gray_a[p - w];
+      int bx = (int)a.gray_b[q + 1] - (int)a.gray_b[q - 1];
+      int by = (int)a.gray_b[q + w] - (int)a.gray_b[q - w];
+      difference = abs(ax - bx) + abs(ay - by);
+      cap = a.grad_cap;
+    }
+    int denominator = 1000 * cap;
+    return (a.weight * hamming * cap + (1000 - a.weight) * min(difference, cap) * a.bits +
+            denominator / 2) /
+           denominator;
+  }
+  // ZNCC: int64 window sums, FP64 correlation with Java's operation order and rounding.
+  int rx = a.wx / 2, ry = a.wy / 2, count = a.wx * a.wy, w = a.w;
+  long long sa = 0, sb = 0, saa = 0, sbb = 0, sab = 0;
+  for (int dy = -ry; dy <= ry; dy++)
+    for (int dx = -rx; dx <= rx; dx++) {
+      int x = a.gray_a[p + dy * w + dx], y = a.gray_b[q + dy * w + dx];
+      sa += x;
+      sb += y;
+      saa += x * x;
+      sbb += y * y;
+      sab += x * y;
+    }
+  long long va = count * saa - sa * sa, vb = count * sbb - sb * sb;
+  if (va <= 0 || vb <= 0) return kInvalidCost;
+  double correlation =
+      __ddiv_rn((double)(count * sab - sa * sb), sqrt(__dmul_rn((double)va, (double)vb)));
+  double clamped = fmax(-1.0, fmin(1.0, correlation));
+  return (int)java_round(__dmul_rn(__dmul_rn(__dsub_rn(1.0, clamped), 0.5), (double)a.bits));
+}
+
+// One cost cell per thread-lane: a warp covers one pixel's disparities (coalesced uint16 stores).
+__global__ void cost_volume_kernel(CostArgs a) {
+  int w = a.w, h = a.h, D = a.D;
+  int64_t n = (int64_t)w * h;
+  int rx = a.wx / 2, ry = a.wy / 2;
+  int lane = threadIdx.x & 31;
+  int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = warp; p < n; p += warps) {
+    int x = (int)(p % w), y = (int)(p / w);
+    bool inside = x >= rx && x < w - rx && y >= ry && y < h - ry && a.tex_a[p];
+    uint16_t* out = a.out + p * D;
+    for (int k = lane; k < D; k += 32) {
+      int value = kInvalidCost;
+      if (inside) {
+        long long disparity = (long long)a.min_disparity + k;
+        long long target = (long long)x + (a.reverse ? disparity : -disparity);
+        if (target >= rx && target < w - rx) {
+          int64_t q = (int64_t)y * w + target;
+          if (a.tex_b[q]) value = cell_cost(a, p, q, n);
+        }
+      }
+      out[k] = (uint16_t)value;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Path aggregation, one warp per line (CensusSgm.java:421-459; the reference GPU kernel walks a
+// line per work-group in the same way, GpuStereo.java:732-757).  The line state lives in shared
+// memory as int32, so any D <= 4096 and any penalty fit.  Each lane owns disparities k = lane +
+// 32 j.  The aggregate is read-modify-written once per direction.
+template <typename SumT>
+__global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
+  extern __shared__ int smem[];
+  int D = a.D, w = a.w, h = a.h;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  int* prev = smem + (size_t)warp * 2 * D;
+  int* cur = prev + D;
+  int64_t lines = line_count(w, h, a.dx, a.dy);
+  for (int64_t line = (int64_t)blockIdx.x * warps + warp; line < lines;
+       line += (int64_t)gridDim.x * warps) {
+    int x, y;
+    line_start(line, w, h, a.dx, a.dy, x, y);
+    int64_t prev_p = -1;
+    while (x >= 0 && x < w && y >= 0 && y < h) {
+      int64_t p = (int64_t)y * w + x;
+      bool has = prev_p >= 0 && a.tex[prev_p];
+      int minimum = 0, local_p2 = a.p2;
+      if (has) {
+        int m = INT_MAX;
+        for (int k = lane; k < D; k += 32) m = min(m, prev[k]);
+        minimum = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
+        local_p2 = path_p2(a.p1, a.p2, a.edge_scale, a.gray[p], a.gray[prev_p]);
+      }
+      const uint16_t* c = a.cost + p * D;
+      SumT* s = sum + p * D;
+      for (int k = lane; k < D; k += 32) {
+        int v = c[k];
+        if (has) {
+          int t = min(prev[k], minimum + local_p2);
+          if (k > 0) t = min(t, prev[k - 1] + a.p1);
+          if (k + 1 < D) t = min(t, prev[k + 1] + a.p1);
+          v += t - minimum;
+        }
+        cur[k] = v;
+        s[k] = (SumT)(s[k] + (SumT)v);
+      }
+      __syncwarp();
+      int* swap = prev;
+      prev = cur;
+      cur = swap;
+      prev_p = p;
+      x += a.dx;
+      y += a.dy;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Winner selection (CensusSgm.java:460-515) with the winners record of GpuStereo.java:758-769
+// and the arithmetic of the host select (GpuStereo.java:644-686).  One warp per pixel.
+__device__ void select_pixel(const SelectArgs& a, int64_t p, int best, int value, int second,
+                             int before, int after, int flags, unsigned long long* counts) {
+  if (best < 0) return;
+  bool full = flags == 3;
+  if (full) {
+    counts[1]++;
+    if (a.boundary) a.boundary[p] = 4;
+  }
+  if (best == 0 || best == a.D - 1) {
+    counts[2]++;
+    if (a.reasons) a.reasons[p] = 2;
+    if (full && best == 0) {
+      counts[0]++;
+      if (a.boundary) a.boundary[p] |= 1;
+    }
+    if (full && best == a.D - 1) {
+      counts[3]++;
+      if (a.boundary) a.boundary[p] |= 2;
+    }
+    return;
+  }
+  if (second != INT_MAX) {
+    double slack = fmax(1.0, __dmul_rn((double)value, a.uniqueness));
+    if ((double)(second - value) <= slack) {
+      counts[4]++;
+      if (a.reasons) a.reasons[p] = 3;
+      return;
+    }
+  }
+  double offset = 0;
+  if (before >= 0 && after >= 0) {
+    double curvature =
+        __dsub_rn(__dadd_rn((double)before, (double)after), __dmul_rn(2.0, (double)value));
+    if (curvature > 0) {
+      double o = __ddiv_rn(__dmul_rn(0.5, __dsub_rn((double)before, (double)after)), curvature);
+      offset = fmax(-0.5, fmin(0.5, o));
+    }
+  }
+  a.out[p] = __double2float_rn(__dadd_rn((double)(a.min_disparity + best), offset));
+  counts[5]++;
+  if (a.reasons) a.reasons[p] = 0;
+}
+
+template <typename SumT>
+__global__ void winners_kernel(SelectArgs a, const SumT* __restrict__ sum) {
+  int w = a.w, h = a.h, D = a.D, rx = a.wx / 2, ry = a.wy / 2;
+  int64_t n = (int64_t)w * h;
+  int lane = threadIdx.x & 31;
+  int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long counts[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t p = warp; p < n; p += warps) {
+    int x = (int)(p % w), y = (int)(p / w);
+    const uint16_t* c = a.cost + p * D;
+    const SumT* s = sum + p * D;
+    int flags = (c[0] != kInvalidCost ? 1 : 0) | (c[D - 1] != kInvalidCost ? 2 : 0);
+    bool region = x >= rx && x < w - rx && y >= ry && y < h - ry;
+    int best = -1, value = INT_MAX, second = INT_MAX, before = -1, after = -1;
+    if (region) {
+      unsigned long long key = ~0ull;
+      for (int k = lane; k < D; k += 32)
+        if (c[k] != kInvalidCost) {
+          unsigned long long kk = ((unsigned long long)(uint32_t)s[k] << 32) | (uint32_t)k;
+          key = kk < key ? kk : key;
+        }
+      key = shfl_min_u64(key);
+      if (key != ~0ull) {
+        best = (int)(key & 0xffffffffu);
+        value = (int)(key >> 32);
+        unsigned m = INT_MAX;
+        for (int k = lane; k < D; k += 32)
+          if (abs(k - best) > 1 && c[k] != kInvalidCost) m = min(m, (unsigned)s[k]);
+        second = (int)__reduce_min_sync(0xffffffffu, m);
+        if (best > 0 && c[best - 1] != kInvalidCost) before = (int)s[best - 1];
+        if (best + 1 < D && c[best + 1] != kInvalidCost) after = (int)s[best + 1];
+      }
+    }
+    if (lane == 0) {
+      if (a.summary) {
+        int32_t* r = a.summary + 6 * p;
+        r[0] = best;
+        r[1] = value;
+        r[2] = second;
+        r[3] = before;
+        r[4] = after;
+        r[5] = flags;
+      }
+      a.out[p] = __int_as_float(0x7fc00000);
+      if (region) select_pixel(a, p, best, value, second, before, after, flags, counts);
+    }
+  }
+  if (lane == 0 && a.stats) {
+    if (counts[0]) atomicAdd(&a.stats->lower_boundary_rejected, counts[0]);
+    if (counts[1]) atomicAdd(&a.stats->full_interval_pixels, counts[1]);
+    if (counts[2]) atomicAdd(&a.stats->boundary_rejected, counts[2]);
+    if (counts[3]) atomicAdd(&a.stats->upper_boundary_rejected, counts[3]);
+    if (counts[4]) atomicAdd(&a.stats->ambiguity_rejected, counts[4]);
+    if (counts[5]) atomicAdd(&a.stats->selected, counts[5]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Left-right check (CensusSgm.java:181-201).
+__global__ void lr_check_kernel(LrArgs a) {
+  int64_t n = (int64_t)a.w * a.h;
+  int rx = a.wx / 2, ry = a.wy / 2;
+  int rejected = 0;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int x = (int)(p % a.w), y = (int)(p / a.w);
+    float result = __int_as_float(0x7fc00000);
+    if (x >= rx && x < a.w - rx && y >= ry && y < a.h - ry) {
+      float d = a.dl[p];
+      if (isfinite(d)) {
+        int xr = java_round_float(__fsub_rn((float)x, d));
+        if (xr < rx || xr >= a.w - rx) {
+          if (a.reasons) a.reasons[p] = 4;
+        } else {
+          float other = a.dr[(int64_t)y * a.w + xr];
+          if (isfinite(other) && (double)fabsf(__fsub_rn(d, other)) <= a.threshold)
+            result = d;
+          else {
+            rejected++;
+            if (a.reasons) a.reasons[p] = 4;
+          }
+        }
+      }
+    }
+    a.out[p] = result;
+  }
+  if (a.stats) {
+    int lane = threadIdx.x & 31;
+    unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)rejected);
+    if (lane == 0 && total) atomicAdd(&a.stats->lr_rejected, (unsigned long long)total);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Launchers.
+static int grid_for(int64_t work, int threads, int max_blocks) {
+  int64_t blocks = (work + threads - 1) / threads;
+  if (blocks < 1) blocks = 1;
+  return (int)(blocks < max_blocks ? blocks : max_blocks);
+}
+
+cudaError_t launch_census_texture(const CensusArgs& a, int images, cudaStream_t stream) {
+  dim3 block(32, 8), grid((a.w + 31) / 32, (a.h + 7) / 8, images);
+  census_texture_kernel<<<grid, block, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cost_volume(const CostArgs& a, int sm_count, cudaStream_t stream) {
+  int64_t n = (int64_t)a.w * a.h;
+  cost_volume_kernel<<<grid_for(n * 32, 256, sm_count * 32), 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int sm_count,
+                              cudaStream_t stream) {
+  const int warps = 4;
+  size_t shared = (size_t)warps * 2 * a.D * sizeof(int);
+  int64_t lines = line_count(a.w, a.h, a.dx, a.dy);
+  int grid = grid_for(lines, warps, sm_count * 64);
+  if (sum_bytes == 2) {
+    if (shared > 48 * 1024)
+      cudaFuncSetAttribute(paths_line_kernel<uint16_t>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared);
+    paths_line_kernel<uint16_t><<<grid, warps * 32, shared, stream>>>(a, (uint16_t*)sum);
+  } else {
+    if (shared > 48 * 1024)
+      cudaFuncSetAttribute(paths_line_kernel<uint32_t>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared);
+    paths_line_kernel<uint32_t><<<grid, warps * 32, shared, stream>>>(a, (uint32_t*)sum);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, int sm_count,
+                           cudaStream_t stream) {
+  int64_t n = (int64_t)a.w * a.h;
+  int grid = grid_for(n * 32, 256, sm_count * 16);
+  if (sum_bytes == 2)
+    winners_kernel<uint16_t><<<grid, 256, 0, stream>>>(a, (const uint16_t*)sum);
+  else
+    winners_kernel<uint32_t><<<grid, 256, 0, stream>>>(a, (const uint32_t*)sum);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lr_check(const LrArgs& a, int sm_count, cudaStream_t stream) {
+  int64_t n = (int64_t)a.w * a.h;
+  lr_check_kernel<<<grid_for(n, 256, sm_count * 8), 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace csgm

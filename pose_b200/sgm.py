@@ -1,0 +1,243 @@
+"""Host-side mirror of Collinea's matcher interface over the C ABI.
+
+``GpuSgm`` mirrors src/main/java/sgm/GpuSgm.java (device list, session, budget, ``match``,
+``disparityLimit``, profiling) and ``CensusSgm`` mirrors src/main/java/sgm/CensusSgm.java
+(``compute`` -> ``Result`` with ``Stats``).  Every computation runs in libcollinea_sgm.so on the
+GPU; there is no CPU fallback (a missing library or device raises).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import CsgmDeviceInfo, CsgmParams, CsgmProfile, CsgmStats, check
+from .stereo_cost import params_from_options
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _u8(a, n):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.uint8).reshape(-1)
+    if a.size != n:
+        raise ValueError("Invalid stereo image dimensions")
+    return a
+
+
+@dataclass
+class Stats:
+    """CensusSgm.Stats (CensusSgm.java:683-737)."""
+
+    lowerBoundaryRejected: int = 0
+    fullIntervalPixels: int = 0
+    boundaryRejected: int = 0
+    upperBoundaryRejected: int = 0
+    ambiguityRejected: int = 0
+    selected: int = 0
+    lrRejected: int = 0
+    postMedianLrRejected: int = 0
+    photometricRejected: int = 0
+    speckleRejected: int = 0
+    valid: int = 0
+
+    _C_NAMES = dict(zip(_abi.STATS_FIELDS, [
+        "lowerBoundaryRejected", "fullIntervalPixels", "boundaryRejected",
+        "upperBoundaryRejected", "ambiguityRejected", "selected", "lrRejected",
+        "postMedianLrRejected", "photometricRejected", "speckleRejected", "valid"]))
+
+    @classmethod
+    def from_c(cls, s: CsgmStats) -> "Stats":
+        out = cls()
+        for c_name, name in cls._C_NAMES.items():
+            setattr(out, name, int(getattr(s, c_name)))
+        return out
+
+    def to_c(self) -> CsgmStats:
+        s = CsgmStats()
+        for c_name, name in self._C_NAMES.items():
+            setattr(s, c_name, int(getattr(self, name)))
+        return s
+
+    def csv(self) -> str:
+        """Stats.csv (CensusSgm.java:718-736)."""
+        return ",".join(str(v) for v in (
+            self.boundaryRejected, self.upperBoundaryRejected, self.ambiguityRejected,
+            self.selected, self.lrRejected, self.postMedianLrRejected, self.photometricRejected,
+            self.speckleRejected, self.valid))
+
+
+@dataclass
+class Result:
+    """CensusSgm.Result (CensusSgm.java:739-767)."""
+
+    width: int
+    height: int
+    disparity: np.ndarray
+    stats: Stats = field(default_factory=Stats)
+    left: np.ndarray | None = None
+    right: np.ndarray | None = None
+    reasons: np.ndarray | None = None
+    searchBoundary: np.ndarray | None = None
+
+
+class GpuSgm:
+    """A session on one CUDA device (GpuSgm.java:163-221, closeSession :392-397)."""
+
+    def __init__(self, device: int = 0, memory_mb: int = 0):
+        self.lib = _abi.load()
+        handle = ctypes.c_void_p()
+        check(self.lib.csgm_session_open(int(device), ctypes.byref(handle)))
+        self.handle = handle
+        self.device = device
+        if memory_mb:
+            self.set_budget(memory_mb * 1048576)
+
+    # -- lifecycle -------------------------------------------------------------------------
+    def close(self) -> None:
+        if self.handle:
+            self.lib.csgm_session_close(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- devices -----------------------------------------------------------------------------
+    @staticmethod
+    def devices() -> list:
+        """GpuSgm.devices (GpuSgm.java:79-141)."""
+        lib = _abi.load()
+        count = ctypes.c_int32()
+        check(lib.csgm_device_count(ctypes.byref(count)))
+        out = []
+        for i in range(count.value):
+            info = CsgmDeviceInfo()
+            check(lib.csgm_device_info_get(i, ctypes.byref(info)))
+            out.append({"index": i, "name": info.name.decode(), "memory": info.memory_bytes,
+                        "sm_count": info.sm_count, "cc": (info.cc_major, info.cc_minor)})
+        return out
+
+    # -- budget and planning -----------------------------------------------------------------
+    def set_budget(self, nbytes: int) -> None:
+        check(self.lib.csgm_session_set_budget(self.handle, int(nbytes)))
+
+    def plan(self, params: CsgmParams, w: int, h: int) -> int:
+        out = ctypes.c_int64()
+        check(self.lib.csgm_plan(self.handle, ctypes.byref(params), w, h, ctypes.byref(out)))
+        return out.value
+
+    def disparityLimit(self, params: CsgmParams, w: int, h: int) -> int:
+        """GpuSgm.disparityLimit (GpuSgm.java:237-245)."""
+        out = ctypes.c_int32()
+        check(self.lib.csgm_disparity_limit(self.handle, ctypes.byref(params), w, h,
+                                            ctypes.byref(out)))
+        return out.value
+
+    # -- profiling ---------------------------------------------------------------------------
+    def set_profiling(self, level: int) -> None:
+        check(self.lib.csgm_session_set_profiling(self.handle, int(level)))
+
+    def profile(self, reset: bool = False) -> dict:
+        """GpuSgm.Compute.profile (GpuSgm.java:592-604)."""
+        p = CsgmProfile()
+        check(self.lib.csgm_profile_get(self.handle, ctypes.byref(p), int(reset)))
+        return {name: getattr(p, name) for name, _ in CsgmProfile._fields_}
+
+    def kernel_times(self, reset: bool = False) -> dict:
+        count = ctypes.c_int32()
+        records = (_abi.CsgmKernelTime * 64)()
+        check(self.lib.csgm_kernel_times(self.handle, records, 64, ctypes.byref(count),
+                                         int(reset)))
+        return {r.name.decode(): (r.launches, r.total_ns) for r in records[:min(64, count.value)]}
+
+    def synchronize(self) -> None:
+        check(self.lib.csgm_session_synchronize(self.handle))
+
+    # -- the hot path ------------------------------------------------------------------------
+    def match(self, params: CsgmParams, a, b, grayA, grayB, ta, tb, w: int, h: int,
+              reverse: bool, stats: Stats | None = None, reasons=None, searchBoundary=None,
+              summary: bool = False):
+        """GpuSgm.match (GpuSgm.java:267-303): one view from host descriptors and masks.
+        Returns the float disparities (and the winners record if ``summary``)."""
+        n = w * h
+        words = (params.window_x * params.window_y - 1 + 63) // 64
+        a = np.ascontiguousarray(a, dtype=np.uint64).reshape(-1)
+        b = np.ascontiguousarray(b, dtype=np.uint64).reshape(-1)
+        if a.size != words * n or b.size != words * n:
+            raise ValueError("descriptor planes do not match the window and image size")
+        grayA, grayB, ta, tb = _u8(grayA, n), _u8(grayB, n), _u8(ta, n), _u8(tb, n)
+        out = np.empty(n, np.float32)
+        rec = np.empty(6 * n, np.int32) if summary else None
+        cstats = stats.to_c() if stats is not None else CsgmStats()
+        for arr in (reasons, searchBoundary):
+            if arr is not None and (arr.dtype != np.uint8 or arr.size != n
+                                    or not arr.flags.c_contiguous):
+                raise ValueError("reasons/searchBoundary must be contiguous uint8[w*h]")
+        check(self.lib.csgm_match(self.handle, ctypes.byref(params), _ptr(a), _ptr(b),
+                                  _ptr(grayA), _ptr(grayB), _ptr(ta), _ptr(tb), w, h,
+                                  int(bool(reverse)), _ptr(out), _ptr(rec), _ptr(reasons),
+                                  _ptr(searchBoundary), ctypes.byref(cstats)))
+        if stats is not None:
+            for c_name, name in Stats._C_NAMES.items():
+                setattr(stats, name, int(getattr(cstats, c_name)))
+        return (out, rec) if summary else out
+
+    def pair(self, params: CsgmParams, left, right, w: int, h: int, validLeft=None,
+             validRight=None, want_views: bool = False, want_reasons: bool = False) -> Result:
+        """Census, both views and the LR check on the GPU (CensusSgm.computeRecorded :56-201)."""
+        n = w * h
+        left, right = _u8(left, n), _u8(right, n)
+        validLeft, validRight = _u8(validLeft, n), _u8(validRight, n)
+        if (validLeft is None) != (validRight is None):
+            raise ValueError("Invalid stereo mask dimensions")
+        checked = np.empty(n, np.float32)
+        dl = np.empty(n, np.float32) if want_views else None
+        dr = np.empty(n, np.float32) if want_views else None
+        reasons = np.empty(n, np.uint8) if want_reasons else None
+        boundary = np.empty(n, np.uint8) if want_reasons else None
+        cstats = CsgmStats()
+        check(self.lib.csgm_pair(self.handle, ctypes.byref(params), _ptr(left), _ptr(right),
+                                 _ptr(validLeft), _ptr(validRight), w, h, _ptr(checked), _ptr(dl),
+                                 _ptr(dr), _ptr(reasons), _ptr(boundary), ctypes.byref(cstats)))
+        return Result(w, h, checked, Stats.from_c(cstats), dl, dr, reasons, boundary)
+
+
+class CensusSgm:
+    """CensusSgm (CensusSgm.java:10-280) over a GpuSgm session."""
+
+    def __init__(self, options, session: GpuSgm | None = None):
+        self.options = options.validate()
+        self._own = session is None
+        self.session = session or GpuSgm(options.gpuDevice, options.gpuMemoryMb)
+
+    def params(self) -> CsgmParams:
+        return params_from_options(self.options)
+
+    def match_pair(self, left, right, width: int, height: int, validLeft=None, validRight=None,
+                   want_views=False, want_reasons=False) -> Result:
+        """The matcher up to the LR check (CensusSgm.java:56-201)."""
+        o = self.options
+        if width < o.window_x + 2 or height < o.window_y + 2:
+            raise ValueError("Invalid stereo image dimensions")
+        if o.censusMode != "gray":
+            raise NotImplementedError("color-distance census is not on the GPU path yet")
+        return self.session.pair(self.params(), left, right, width, height, validLeft,
+                                 validRight, want_views, want_reasons)
+
+    def close(self):
+        if self._own:
+            self.session.close()

@@ -1,0 +1,190 @@
+"""CUDA matcher == CPU oracle, bit for bit, on the reference's own CPU==GPU fixtures.
+
+Restates StorageGpuRegression.java:68-104, ScalingRegression.java:56-99 and
+UpgradeStereoRegression.java:35-80,98-125 with "GPU" = libcollinea_sgm.so through the C ABI and
+"CPU" = the oracle.  Disparities are compared as raw float bits (subpixel values are bit-exact,
+far inside the 1e-4 px tolerance), counters and per-pixel reason codes exactly.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import (scaling_pair, storage_gpu_pair, upgrade_large_pair, upgrade_pair)
+from pose_b200 import _abi
+from pose_b200.options import Options
+from pose_b200.stereo_cost import params_from_options
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def session():
+    from pose_b200.sgm import GpuSgm
+
+    orc.set_threads(8)
+    s = GpuSgm(0)
+    yield s
+    s.close()
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def stats_tuple(s):
+    return tuple(int(getattr(s, k)) for k in _abi.STATS_FIELDS)
+
+
+def assert_pair_equal(session, o, a, b, w, h, ma=None, mb=None, params=None):
+    prm = params if params is not None else params_from_options(o)
+    want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
+    got = session.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+    assert np.array_equal(bits(got.left), bits(want["dl"])), "left view disparities"
+    assert np.array_equal(bits(got.right), bits(want["dr"])), "right view disparities"
+    assert np.array_equal(bits(got.disparity), bits(want["checked"])), "LR-checked disparities"
+    assert np.array_equal(got.reasons, want["reasons"]), "reason codes"
+    assert np.array_equal(got.searchBoundary, want["boundary"]), "search-boundary flags"
+    assert stats_tuple(got.stats.to_c()) == stats_tuple(want["stats"]), "counters"
+    return got
+
+
+@pytest.mark.parametrize("cost", ["census", "ad-census", "census-gradient", "zncc"])
+@pytest.mark.parametrize("directions,agg", [(4, "16"), (8, "16"), (4, "32"), (8, "32")])
+@pytest.mark.parametrize("reverse", [0, 1])
+def test_match_scaling_fixture(session, cost, directions, agg, reverse):
+    """csgm_match (GpuSgm.match drop-in) on ScalingRegression's fixture: D=33, minD=-5."""
+    w, h, a, b, ma, mb = scaling_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 33, -5
+    o.matchingCost, o.directions, o.sgmAggregate = cost, directions, agg
+    prm = params_from_options(o)
+    da, db = orc.census(a, w, h, 5, 5), orc.census(b, w, h, 5, 5)
+    ta = orc.texture(a, w, h, 5, 5) & (ma != 0)
+    tb = orc.texture(b, w, h, 5, 5) & (mb != 0)
+    if reverse:
+        da, db, ta, tb, a, b = db, da, tb, ta, b, a
+    n = w * h
+    reasons_want = np.ones(n, np.uint8)
+    boundary_want = np.zeros(n, np.uint8)
+    want = orc.match(prm, da, db, a, b, ta, tb, w, h, reverse, want_summary=True,
+                     reasons=reasons_want, boundary=boundary_want)
+    from pose_b200.sgm import Stats
+
+    st = Stats()
+    reasons = np.ones(n, np.uint8)
+    boundary = np.zeros(n, np.uint8)
+    disp, summary = session.match(prm, da, db, a, b, ta, tb, w, h, reverse, st, reasons,
+                                  boundary, summary=True)
+    assert np.array_equal(summary, want["summary"]), "winners record"
+    assert np.array_equal(bits(disp), bits(want["disp"]))
+    assert np.array_equal(reasons, reasons_want) and np.array_equal(boundary, boundary_want)
+    s = want["stats"]
+    assert (st.fullIntervalPixels, st.boundaryRejected, st.lowerBoundaryRejected,
+            st.upperBoundaryRejected, st.ambiguityRejected, st.selected) == (
+        s.full_interval_pixels, s.boundary_rejected, s.lower_boundary_rejected,
+        s.upper_boundary_rejected, s.ambiguity_rejected, s.selected)
+
+
+@pytest.mark.parametrize("census", [5, 11])
+@pytest.mark.parametrize("directions", [4, 8])
+def test_pair_storage_fixture(session, census, directions):
+    """StorageGpuRegression.java:68-90 (gray mode): D=37 (5x5) or 177 (11x11), masked hole."""
+    w, h, a, b, mask = storage_gpu_pair()
+    o = Options()
+    o.census, o.directions = census, directions
+    o.disparities = 177 if census == 11 else 37
+    assert_pair_equal(session, o, a, b, w, h, mask, mask)
+
+
+def test_pair_signed_range(session):
+    """StorageGpuRegression.java:91-104: D=29, minDisparity -16, swapped images."""
+    w, h, a, b, _ = storage_gpu_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 29, -16
+    assert_pair_equal(session, o, b, a, w, h)
+
+
+@pytest.mark.parametrize("cost", ["census", "ad-census", "census-gradient", "zncc"])
+@pytest.mark.parametrize("directions", [4, 8])
+def test_pair_upgrade_fixture(session, cost, directions):
+    """UpgradeStereoRegression.java:35-80: D=41, minD=-3, masks on both sides."""
+    w, h, shift, a, b, ma, mb = upgrade_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 41, -3
+    o.matchingCost, o.directions = cost, directions
+    assert_pair_equal(session, o, a, b, w, h, ma, mb)
+
+
+def test_pair_693_hypotheses(session):
+    """UpgradeStereoRegression.java:98-125: 800x64, D=693 (many banks in the reference)."""
+    w, h, a, b = upgrade_large_pair()
+    o = Options()
+    o.disparities = 693
+    assert_pair_equal(session, o, a, b, w, h)
+
+
+@pytest.mark.parametrize("wx,wy,cost", [(9, 7, "census"), (9, 7, "census-gradient"),
+                                        (9, 9, "census"), (7, 7, "zncc"), (7, 7, "ad-census")])
+def test_pair_synthetic_windows(session, wx, wy, cost):
+    """The benchmark's window/cost combinations on a small synthetic pair (9x7 is the
+    rectangular extension; its square special cases are the reference's)."""
+    from pose_b200.synthetic import PairSpec, make_pair
+
+    spec = PairSpec(224, 96, planes=3, d_min=4, d_max=40, seed=7)
+    a, b, _ = make_pair(spec)
+    o = Options()
+    o.census, o.censusHeight, o.matchingCost, o.disparities = wx, wy, cost, 48
+    prm = params_from_options(o)
+    prm.p1, prm.p2 = 10, 120
+    assert_pair_equal(session, o, a, b, spec.width, spec.height, params=prm)
+
+
+def test_pair_uint32_large_penalty(session):
+    """P2 large enough that path costs exceed 16 bits: the uint32 aggregate and int32 path state."""
+    w, h, a, b, ma, mb = scaling_pair()
+    o = Options()
+    o.disparities, o.p1, o.p2 = 20, 100, 40000
+    o.sgmEdgeScale = 0
+    prm = params_from_options(o)
+    assert prm.aggregate_bytes == 4 and prm.p2 > 32000
+    assert_pair_equal(session, o, a, b, w, h, ma, mb, params=prm)
+
+
+def test_invalid_arguments_are_rejected(session):
+    prm = params_from_options(Options())
+    img = np.zeros(64 * 48, np.uint8)
+    bad = params_from_options(Options())
+    bad.directions = 6
+    with pytest.raises(_abi.CsgmError) as e:
+        session.pair(bad, img, img, 64, 48)
+    assert e.value.status == _abi.CSGM_E_INVALID
+    with pytest.raises(_abi.CsgmError) as e:
+        session.pair(prm, img, img, 6, 6)
+    assert e.value.status == _abi.CSGM_E_INVALID
+
+
+def test_budget_rejects_before_allocation():
+    """StorageGpuRegression.java:135-144: an impossible budget is refused before any work."""
+    from pose_b200.sgm import GpuSgm
+
+    with GpuSgm(0, memory_mb=1) as s:
+        w, h, a, b, _ = storage_gpu_pair()
+        prm = params_from_options(Options())
+        with pytest.raises(_abi.CsgmError) as e:
+            s.pair(prm, a, b, w, h)
+        assert e.value.status == _abi.CSGM_E_NOMEM
+        assert s.disparityLimit(prm, w, h) == 0
+    with GpuSgm(0) as s:
+        assert s.disparityLimit(prm, w, h) == 4096
+        # the session stays usable after a rejected call
+        s.pair(prm, a, b, w, h)
+
+
+def test_repeatable(session):
+    w, h, a, b, mask = storage_gpu_pair()
+    prm = params_from_options(Options())
+    r1 = session.pair(prm, a, b, w, h, mask, mask)
+    r2 = session.pair(prm, a, b, w, h, mask, mask)
+    assert np.array_equal(bits(r1.disparity), bits(r2.disparity))
