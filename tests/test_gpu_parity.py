@@ -160,9 +160,12 @@ def test_invalid_arguments_are_rejected(session):
     with pytest.raises(_abi.CsgmError) as e:
         session.pair(bad, img, img, 64, 48)
     assert e.value.status == _abi.CSGM_E_INVALID
-    with pytest.raises(_abi.CsgmError) as e:
-        session.pair(prm, img, img, 6, 6)
+    tiny = np.zeros(6 * 6, np.uint8)
+    with pytest.raises(_abi.CsgmError) as e:  # smaller than census + 2 (CensusSgm.java:56-60)
+        session.pair(prm, tiny, tiny, 6, 6)
     assert e.value.status == _abi.CSGM_E_INVALID
+    with pytest.raises(ValueError):  # buffer size does not match w*h
+        session.pair(prm, img, img, 6, 6)
 
 
 def test_budget_rejects_before_allocation():
@@ -175,7 +178,15 @@ def test_budget_rejects_before_allocation():
         with pytest.raises(_abi.CsgmError) as e:
             s.pair(prm, a, b, w, h)
         assert e.value.status == _abi.CSGM_E_NOMEM
-        assert s.disparityLimit(prm, w, h) == 0
+        limit = s.disparityLimit(prm, w, h)  # GpuStereo.limit: largest D whose plan fits
+        assert 0 <= limit < prm.disparities
+        if limit >= 3:
+            prm.disparities = limit
+            s.plan(prm, w, h)
+            prm.disparities = limit + 1
+            with pytest.raises(_abi.CsgmError):
+                s.plan(prm, w, h)
+        prm = params_from_options(Options())
     with GpuSgm(0) as s:
         assert s.disparityLimit(prm, w, h) == 4096
         # the session stays usable after a rejected call
