@@ -44,6 +44,10 @@ extern "C" {
 #define CSGM_E_BUSY (-6)        /* batch queue full or request not finished */
 #define CSGM_E_UNSUPPORTED (-7) /* parameter combination outside what the kernels implement */
 
+/* params.flags: run the general kernels (one warp per path line, any D) even where the fused
+ * sweep would apply.  Same results; used to compare the two paths and as the plain per-pair path. */
+#define CSGM_FLAG_GENERAL 1
+
 /* Matching-cost codes: StereoCost.code (src/main/java/sgm/StereoCost.java:7-15). */
 #define CSGM_COST_CENSUS 0
 #define CSGM_COST_AD_CENSUS 1
@@ -71,7 +75,7 @@ typedef struct csgm_params {
   int32_t edge_scale;          /* Options.sgmEdgeScale, 0..255 (0 = constant P2) */
   int32_t directions;          /* 4 or 8 (reference); 16 adds the (+-1,+-2),(+-2,+-1) paths */
   int32_t aggregate_bytes;     /* 2 (uint16) or 4 (uint32): StereoCost.aggregateBytes */
-  int32_t flags;               /* reserved, must be 0 */
+  int32_t flags;               /* 0, or CSGM_FLAG_GENERAL */
   double uniqueness;           /* Options.uniqueness */
   double lr_threshold;         /* Options.lrThreshold */
 } csgm_params;

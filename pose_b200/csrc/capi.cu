@@ -184,7 +184,7 @@ int validate_params(const csgm_params* p, int w, int h) {
   if (!(p->uniqueness >= 0 && p->uniqueness < 1))
     return fail(CSGM_E_INVALID, "Require 0 <= uniqueness < 1");
   if (!(p->lr_threshold > 0)) return fail(CSGM_E_INVALID, "lr_threshold must be positive");
-  if (p->flags != 0) return fail(CSGM_E_INVALID, "params.flags must be 0");
+  if (p->flags & ~CSGM_FLAG_GENERAL) return fail(CSGM_E_INVALID, "unknown params.flags bits");
   if (w < p->window_x + 2 || h < p->window_y + 2)
     return fail(CSGM_E_INVALID, "Invalid stereo image dimensions");
   if ((int64_t)w * h > (int64_t)INT32_MAX)

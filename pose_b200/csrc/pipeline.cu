@@ -24,6 +24,10 @@ namespace csgm {
 
 static int words_of(const csgm_params& p) { return (p.window_x * p.window_y - 1 + 63) / 64; }
 
+static bool use_fused(const csgm_params& p) {
+  return !(p.flags & CSGM_FLAG_GENERAL) && fused_supported(p);
+}
+
 size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
   size_t n = (size_t)w * h, D = (size_t)p.disparities, words = (size_t)words_of(p);
   size_t bytes = 0;
@@ -31,7 +35,7 @@ size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs
   bytes += 2 * n;              // texture masks
   bytes += 2 * n * 4;          // raw view disparities
   bytes += sizeof(DeviceStats);
-  if (fused_supported(p))
+  if (use_fused(p))
     bytes += fused_workspace_bytes(p, w, h);
   else
     bytes += n * D * 2 + n * D * p.aggregate_bytes;  // one cost volume + one aggregate
@@ -138,12 +142,16 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* lef
   ctx.prof->kernel_begin();
   CK(launch_census_texture(ca, 2, ctx.stream), "census kernel launch");
   ctx.prof->kernel_end("census_texture");
-  if (fused_supported(p)) {
+  if (use_fused(p)) {
     // Both views in one pass structure (stereo_fused.cu).
     FusedViews v{desc_l, desc_r, tex_l, tex_r, left, right, disp_l, disp_r, reasons, boundary,
                  dstats};
-    status = run_views_fused(ctx, p, v, w, h);
+    int* error_flag = nullptr;
+    status = run_views_fused(ctx, p, v, w, h, &error_flag);
     if (status) return status;
+    CK(cudaMemcpyAsync(&dstats->pad, error_flag, sizeof(int), cudaMemcpyDeviceToDevice,
+                       ctx.stream),
+       "error flag copy");
   } else {
     status = run_view_general(ctx, p, desc_l, desc_r, tex_l, tex_r, left, right, w, h, 0, disp_l,
                               nullptr, reasons, boundary, dstats);
@@ -165,6 +173,7 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* lef
   CK(cudaMemcpyAsync(&host, dstats, sizeof host, cudaMemcpyDeviceToHost, ctx.stream),
      "stats readback");
   CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (host.pad) return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host.pad);
   if (stats) copy_stats(host, stats, false);
   if (t1) {
     ctx.profile->kernel_ns += (int64_t)(elapsed_ms(t0, t1) * 1e6);
@@ -253,6 +262,7 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
      "stats readback");
   if (timed) CK(cudaEventRecord(d1, ctx.stream), "event record");
   CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (host.pad) return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host.pad);
   if (stats) copy_stats(host, stats, false);
   if (timed) {
     ctx.profile->upload_ns += (int64_t)(elapsed_ms(u0, u1) * 1e6);

@@ -24,6 +24,9 @@ struct FusedViews {
 
 bool fused_supported(const csgm_params& p);
 size_t fused_workspace_bytes(const csgm_params& p, int w, int h);
-int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h);
+// Queues both views on ctx.stream; *error_flag receives the device address of the sweep's error
+// word (non-zero after a bounded wait ran out).
+int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h,
+                    int** error_flag);
 
 }  // namespace csgm

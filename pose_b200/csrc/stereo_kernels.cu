@@ -54,51 +54,6 @@ __global__ void census_texture_kernel(CensusArgs args) {
   im.tex[p] = textured;
 }
 
-// ---------------------------------------------------------------------------------------------
-// StereoCost.value (StereoCost.java:50-90) for matching pixel p and target q.
-__device__ __forceinline__ int cell_cost(const CostArgs& a, int64_t p, int64_t q, int64_t n) {
-  int hamming = __popcll(a.desc_a[p] ^ a.desc_b[q]);
-  if (a.words > 1) hamming += __popcll(a.desc_a[n + p] ^ a.desc_b[n + q]);
-  if (a.mode == CSGM_COST_CENSUS) return hamming;
-  if (a.mode == CSGM_COST_AD_CENSUS || a.mode == CSGM_COST_CENSUS_GRADIENT) {
-    int difference, cap;
-    if (a.mode == CSGM_COST_AD_CENSUS) {
-      difference = abs((int)a.gray_a[p] - (int)a.gray_b[q]);
-      cap = a.ad_cap;
-    } else {
-      int w = a.w;
-      int ax = (int)a.gray_a[p + 1] - (int)a.gray_a[p - 1];
-      int ay = (int)a.gray_a[p + w] - (int)a.gray_a[p - w];
-      int bx = (int)a.gray_b[q + 1] - (int)a.gray_b[q - 1];
-      int by = (int)a.gray_b[q + w] - (int)a.gray_b[q - w];
-      difference = abs(ax - bx) + abs(ay - by);
-      cap = a.grad_cap;
-    }
-    int denominator = 1000 * cap;
-    return (a.weight * hamming * cap + (1000 - a.weight) * min(difference, cap) * a.bits +
-            denominator / 2) /
-           denominator;
-  }
-  // ZNCC: int64 window sums, FP64 correlation with Java's operation order and rounding.
-  int rx = a.wx / 2, ry = a.wy / 2, count = a.wx * a.wy, w = a.w;
-  long long sa = 0, sb = 0, saa = 0, sbb = 0, sab = 0;
-  for (int dy = -ry; dy <= ry; dy++)
-    for (int dx = -rx; dx <= rx; dx++) {
-      int x = a.gray_a[p + dy * w + dx], y = a.gray_b[q + dy * w + dx];
-      sa += x;
-      sb += y;
-      saa += x * x;
-      sbb += y * y;
-      sab += x * y;
-    }
-  long long va = count * saa - sa * sa, vb = count * sbb - sb * sb;
-  if (va <= 0 || vb <= 0) return kInvalidCost;
-  double correlation =
-      __ddiv_rn((double)(count * sab - sa * sb), sqrt(__dmul_rn((double)va, (double)vb)));
-  double clamped = fmax(-1.0, fmin(1.0, correlation));
-  return (int)java_round(__dmul_rn(__dmul_rn(__dsub_rn(1.0, clamped), 0.5), (double)a.bits));
-}
-
 // One cost cell per thread-lane: a warp covers one pixel's disparities (coalesced uint16 stores).
 __global__ void cost_volume_kernel(CostArgs a) {
   int w = a.w, h = a.h, D = a.D;

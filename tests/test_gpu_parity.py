@@ -37,16 +37,25 @@ def stats_tuple(s):
     return tuple(int(getattr(s, k)) for k in _abi.STATS_FIELDS)
 
 
+GENERAL = 1  # CSGM_FLAG_GENERAL
+
+
 def assert_pair_equal(session, o, a, b, w, h, ma=None, mb=None, params=None):
+    """Both GPU paths (the fused sweep where it applies, and the general kernels) == oracle."""
     prm = params if params is not None else params_from_options(o)
     want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
-    got = session.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
-    assert np.array_equal(bits(got.left), bits(want["dl"])), "left view disparities"
-    assert np.array_equal(bits(got.right), bits(want["dr"])), "right view disparities"
-    assert np.array_equal(bits(got.disparity), bits(want["checked"])), "LR-checked disparities"
-    assert np.array_equal(got.reasons, want["reasons"]), "reason codes"
-    assert np.array_equal(got.searchBoundary, want["boundary"]), "search-boundary flags"
-    assert stats_tuple(got.stats.to_c()) == stats_tuple(want["stats"]), "counters"
+    got = None
+    for flags in (0, GENERAL):
+        prm.flags = flags
+        got = session.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+        path = "general" if flags else "default"
+        assert np.array_equal(bits(got.left), bits(want["dl"])), f"{path}: left view disparities"
+        assert np.array_equal(bits(got.right), bits(want["dr"])), f"{path}: right view"
+        assert np.array_equal(bits(got.disparity), bits(want["checked"])), f"{path}: LR-checked"
+        assert np.array_equal(got.reasons, want["reasons"]), f"{path}: reason codes"
+        assert np.array_equal(got.searchBoundary, want["boundary"]), f"{path}: boundary flags"
+        assert stats_tuple(got.stats.to_c()) == stats_tuple(want["stats"]), f"{path}: counters"
+    prm.flags = 0
     return got
 
 
@@ -199,3 +208,63 @@ def test_repeatable(session):
     r1 = session.pair(prm, a, b, w, h, mask, mask)
     r2 = session.pair(prm, a, b, w, h, mask, mask)
     assert np.array_equal(bits(r1.disparity), bits(r2.disparity))
+
+
+def bench_params(wx=9, wy=7, D=128, cost="census"):
+    o = Options()
+    o.census, o.censusHeight, o.disparities, o.matchingCost = wx, wy, D, cost
+    prm = params_from_options(o)
+    prm.p1, prm.p2 = 10, 120
+    return prm
+
+
+@pytest.mark.parametrize("D", [64, 128, 192, 256])
+def test_pair_band_of_cfg1(session, D):
+    """A full-width 1600 x 48 band of the benchmark pair, every fused register layout, vs oracle."""
+    from pose_b200.synthetic import make_pair, spec_for
+
+    left, right, _ = make_pair(spec_for("cfg1"))
+    w, h = 1600, 48
+    y0 = 500
+    band_l = np.ascontiguousarray(left.reshape(1067, w)[y0:y0 + h]).reshape(-1)
+    band_r = np.ascontiguousarray(right.reshape(1067, w)[y0:y0 + h]).reshape(-1)
+    o = Options()
+    o.census, o.censusHeight = 9, 7
+    assert_pair_equal(session, o, band_l, band_r, w, h, params=bench_params(D=D))
+
+
+@pytest.mark.parametrize("cost", ["census", "census-gradient"])
+def test_full_size_cfg1_fused_equals_general(session, cost):
+    """1600x1067xD128: the fused sweep and the general kernels agree bit for bit at full size,
+    and the LR-checked map recovers the synthetic ground truth."""
+    from pose_b200.synthetic import make_pair, spec_for
+
+    spec = spec_for("cfg1")
+    left, right, truth = make_pair(spec)
+    w, h = spec.width, spec.height
+    prm = bench_params(cost=cost)
+    fused = session.pair(prm, left, right, w, h, want_views=True, want_reasons=True)
+    prm.flags = GENERAL
+    general = session.pair(prm, left, right, w, h, want_views=True, want_reasons=True)
+    prm.flags = 0
+    assert np.array_equal(bits(fused.disparity), bits(general.disparity))
+    assert np.array_equal(bits(fused.left), bits(general.left))
+    assert np.array_equal(bits(fused.right), bits(general.right))
+    assert np.array_equal(fused.reasons, general.reasons)
+    assert stats_tuple(fused.stats.to_c()) == stats_tuple(general.stats.to_c())
+    d = fused.disparity
+    ok = np.isfinite(d)
+    assert ok.mean() > 0.5
+    assert (np.abs(d[ok] - truth[ok]) < 1.0).mean() > 0.9
+
+
+def test_full_size_repeatable(session):
+    from pose_b200.synthetic import make_pair, spec_for
+
+    spec = spec_for("cfg1")
+    left, right, _ = make_pair(spec)
+    prm = bench_params()
+    r1 = session.pair(prm, left, right, spec.width, spec.height)
+    r2 = session.pair(prm, left, right, spec.width, spec.height)
+    assert np.array_equal(bits(r1.disparity), bits(r2.disparity))
+    assert r1.stats == r2.stats
