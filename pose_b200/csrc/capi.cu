@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/collinea_sgm.h"
+#include "collinea_sgm.h"
 #include "pipeline.h"
 #include "stereo_kernels.h"
 

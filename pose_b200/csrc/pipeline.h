@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/collinea_sgm.h"
+#include "collinea_sgm.h"
 
 namespace csgm {
 

@@ -4,7 +4,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/collinea_sgm.h"
+#include "collinea_sgm.h"
 
 namespace csgm {
 

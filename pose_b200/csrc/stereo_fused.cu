@@ -35,8 +35,6 @@ namespace csgm {
 
 namespace {
 
-constexpr int kRows = 8;      // rows (warps) per CTA
-constexpr int kRing = 4;      // ring slots per row
 constexpr int kRecords = 32;  // selections buffered per warp before the scalar select
 
 __host__ __device__ inline int padded_d(int D) { return (D + 63) / 64 * 64; }
@@ -90,15 +88,16 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return d;
 }
 
-// Bounded waits.  The whole warp waits; `error` short-circuits every later wait.
+// Bounded waits.  `error` short-circuits every later wait unless `shortcut` is false (the final
+// drain, which must see its copies land).
 __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
-                                         long long limit) {
+                                         long long limit, bool shortcut = true) {
   long long start = clock64();
   while (!mbar_test(bar, parity)) {
-    if (*(volatile int*)error) return;
+    if (shortcut && *(volatile int*)error) break;
     if (clock64() - start > limit) {
       atomicExch(error, 1);
-      return;
+      break;
     }
   }
 }
@@ -107,10 +106,10 @@ __device__ __forceinline__ void wait_flag(const int* flag, int target, int* erro
                                           long long limit) {
   long long start = clock64();
   while (*(volatile const int*)flag < target) {
-    if (*(volatile int*)error) return;
+    if (*(volatile int*)error) break;
     if (clock64() - start > limit) {
       atomicExch(error, 2);
-      return;
+      break;
     }
     __nanosleep(64);
   }
@@ -118,14 +117,134 @@ __device__ __forceinline__ void wait_flag(const int* flag, int target, int* erro
 }
 
 // ---------------------------------------------------------------------------------------------
-// Cost volumes of both views (uint8, 0x80 = invalid).  One warp per pixel of one view; lanes own
-// contiguous groups of Dp/32 disparities.
+// Cost volumes of both views (uint8, 0x80 = invalid), StereoCost.value semantics
+// (StereoCost.java:50-90) with CensusSgm.java:405-420 validity.  A CTA handles a segment of
+// kCostSeg pixels of one row of one view: the segment's descriptors, textures and grays (with the
+// disparity range of the target view) are staged in shared memory; one thread computes one
+// pixel's Dp costs into a per-warp staging tile that the warp then writes out as coalesced
+// 16-byte stores.  ZNCC (FP64 window sums) stays on the general per-cell path.
 struct CostPairArgs {
   CostArgs view[2];  // per view: a = matching image, b = target image, reverse 0/1
   uint8_t* out[2];
   int Dp;
 };
 
+constexpr int kCostSeg = 128;  // pixels per CTA segment (4 warps x 32 pixels)
+
+__global__ void __launch_bounds__(kCostSeg) cost_rows_kernel(CostPairArgs a) {
+  extern __shared__ __align__(16) uint8_t csm[];
+  const CostArgs& c = a.view[blockIdx.y];
+  uint8_t* out = a.out[blockIdx.y];
+  const int w = c.w, h = c.h, D = c.D, Dp = a.Dp, words = c.words;
+  const int rx = c.wx / 2, ry = c.wy / 2;
+  const int segs = (w + kCostSeg - 1) / kCostSeg;
+  // Target columns of a segment [x0, x0+seg): left view q = x - d, right view q = x + d.
+  const int span = kCostSeg + D;  // staged target pixels
+  uint64_t* da = (uint64_t*)csm;                       // [words][kCostSeg]
+  uint64_t* db = da + 2 * kCostSeg;                    // [words][span]
+  uint8_t* stage = (uint8_t*)(db + 2 * span);          // [4 warps][32][Dp]
+  uint8_t* ta = stage + 4 * 32 * Dp;                   // [kCostSeg]
+  uint8_t* tb = ta + kCostSeg;                         // [span]
+  uint8_t* ga = tb + span;                             // [3][kCostSeg + 2] rows y-1..y+1, x0-1..
+  uint8_t* gb = ga + 3 * (kCostSeg + 2);               // [3][span + 2]
+  const int64_t n = (int64_t)w * h;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t item = blockIdx.x; item < (int64_t)h * segs; item += gridDim.x) {
+    const int y = (int)(item / segs), x0 = (int)(item % segs) * kCostSeg;
+    const int qlo = c.reverse ? x0 + c.min_disparity : x0 - c.min_disparity - (D - 1);
+    const bool row_inside = y >= ry && y < h - ry;
+    __syncthreads();
+    // Stage the segment.
+    for (int i = threadIdx.x; i < kCostSeg; i += blockDim.x) {
+      const int x = x0 + i;
+      const bool ok = x < w;
+      const int64_t p = (int64_t)y * w + x;
+      for (int j = 0; j < words; j++) da[j * kCostSeg + i] = ok ? c.desc_a[j * n + p] : 0;
+      ta[i] = ok ? c.tex_a[p] : 0;
+    }
+    for (int i = threadIdx.x; i < span; i += blockDim.x) {
+      const int q = qlo + i;
+      const bool ok = q >= 0 && q < w;
+      const int64_t p = (int64_t)y * w + q;
+      for (int j = 0; j < words; j++) db[j * span + i] = ok ? c.desc_b[j * n + p] : 0;
+      tb[i] = ok ? c.tex_b[p] : 0;
+    }
+    if (c.mode == CSGM_COST_AD_CENSUS || c.mode == CSGM_COST_CENSUS_GRADIENT) {
+      for (int i = threadIdx.x; i < 3 * (kCostSeg + 2); i += blockDim.x) {
+        const int r = i / (kCostSeg + 2), x = x0 - 1 + i % (kCostSeg + 2), yy = y - 1 + r;
+        ga[i] = (yy >= 0 && yy < h && x >= 0 && x < w) ? c.gray_a[(int64_t)yy * w + x] : 0;
+      }
+      for (int i = threadIdx.x; i < 3 * (span + 2); i += blockDim.x) {
+        const int r = i / (span + 2), x = qlo - 1 + i % (span + 2), yy = y - 1 + r;
+        gb[i] = (yy >= 0 && yy < h && x >= 0 && x < w) ? c.gray_b[(int64_t)yy * w + x] : 0;
+      }
+    }
+    __syncthreads();
+    // One pixel per thread.
+    const int xi = threadIdx.x, x = x0 + xi;
+    uint8_t* mine = stage + (warp * 32 + lane) * Dp;
+    const bool inside = x < w && row_inside && x >= rx && x < w - rx && ta[xi];
+    const int ax = inside && c.mode == CSGM_COST_CENSUS_GRADIENT
+                       ? (int)ga[(kCostSeg + 2) + xi + 2] - (int)ga[(kCostSeg + 2) + xi] : 0;
+    const int ay = inside && c.mode == CSGM_COST_CENSUS_GRADIENT
+                       ? (int)ga[2 * (kCostSeg + 2) + xi + 1] - (int)ga[xi + 1] : 0;
+    const int gav = inside ? (int)ga[(kCostSeg + 2) + xi + 1] : 0;
+    const int denominator = 1000 * (c.mode == CSGM_COST_AD_CENSUS ? c.ad_cap : c.grad_cap);
+    for (int k0 = 0; k0 < Dp; k0 += 4) {
+      uint32_t packed = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k = k0 + j;
+        int value = 0x80;
+        if (inside && k < D) {
+          const long long disparity = (long long)c.min_disparity + k;
+          const long long target = (long long)x + (c.reverse ? disparity : -disparity);
+          if (target >= rx && target < w - rx) {
+            const int qi = (int)(target - qlo);
+            if (tb[qi]) {
+              int ham = __popcll(da[xi] ^ db[qi]);
+              if (words > 1) ham += __popcll(da[kCostSeg + xi] ^ db[span + qi]);
+              value = ham;
+              if (c.mode == CSGM_COST_AD_CENSUS || c.mode == CSGM_COST_CENSUS_GRADIENT) {
+                int difference, cap;
+                if (c.mode == CSGM_COST_AD_CENSUS) {
+                  difference = abs(gav - (int)gb[(span + 2) + qi + 1]);
+                  cap = c.ad_cap;
+                } else {
+                  const int bx = (int)gb[(span + 2) + qi + 2] - (int)gb[(span + 2) + qi];
+                  const int by = (int)gb[2 * (span + 2) + qi + 1] - (int)gb[qi + 1];
+                  difference = abs(ax - bx) + abs(ay - by);
+                  cap = c.grad_cap;
+                }
+                value = (c.weight * ham * cap + (1000 - c.weight) * min(difference, cap) * c.bits +
+                         denominator / 2) /
+                        denominator;
+              }
+            }
+          }
+        }
+        packed |= (uint32_t)value << (8 * j);
+      }
+      *(uint32_t*)(mine + k0) = packed;
+    }
+    __syncwarp();
+    // Coalesced write-out of the warp's 32 pixels (contiguous in memory).
+    const int wx0 = x0 + warp * 32;
+    const int npx = max(0, min(32, w - wx0));
+    const int64_t base = ((int64_t)y * w + wx0) * Dp;
+    const uint8_t* tile = stage + warp * 32 * Dp;
+    for (int b = lane * 16; b < npx * Dp; b += 32 * 16)
+      *(uint4*)(out + base + b) = *(const uint4*)(tile + b);
+  }
+}
+
+size_t cost_rows_shared(int D, int Dp) {
+  const int span = kCostSeg + D;
+  return 2 * kCostSeg * 8 + 2 * (size_t)span * 8 + 4 * 32 * (size_t)Dp + kCostSeg + span +
+         3 * (kCostSeg + 2) + 3 * ((size_t)span + 2) + 16;
+}
+
+// ZNCC and other fallbacks: one warp per pixel, lanes own contiguous disparity groups.
 __global__ void cost_pair_kernel(CostPairArgs a) {
   const CostArgs& c = a.view[blockIdx.y];
   uint8_t* out = a.out[blockIdx.y];
@@ -188,22 +307,19 @@ struct SweepArgs {
   long long timeout;
 };
 
-// Shared-memory layout (byte offsets), identical on host and device.
+// Shared-memory layout (byte offsets), compile-time for a kernel instance.
+template <int REGS, int K, int RING, int R>
 struct SweepLayout {
-  int slot;       // one ring slot: 3 paths x Dp uint16 + 4 uint32 minima
-  int lut, bars, cost, sum, ring, carry, rec, total;
-  __host__ __device__ SweepLayout(int Dp, int K) {
-    slot = 3 * Dp * 2 + 16;
-    lut = 0;                                     // 256 x uint32
-    bars = lut + 256 * 4;                        // kRows x 4 + 3 mbarriers
-    cost = bars + (kRows * 4 + 3) * 8;
-    cost = (cost + 127) / 128 * 128;
-    sum = cost + kRows * 2 * K * Dp;             // cost chunks, double-buffered per warp
-    ring = sum + kRows * 2 * K * Dp * 2;         // partial-aggregate chunks
-    carry = ring + kRows * kRing * slot;         // row-to-row ring
-    rec = carry + 3 * K * slot;                  // carry chunks of the row above the CTA
-    total = rec + kRows * kRecords * 6 * 4;      // winners records
-  }
+  static constexpr int Dp = 64 * REGS;
+  static constexpr int slot = 3 * Dp * 2 + 16;             // 3 paths x Dp uint16 + 4 minima
+  static constexpr int lut = 0;                            // 256 x uint32
+  static constexpr int bars = lut + 256 * 4;               // R x 4 + 4 mbarriers
+  static constexpr int cost = (bars + (R * 4 + 4) * 8 + 127) / 128 * 128;
+  static constexpr int sum = cost + R * 2 * K * Dp;        // cost chunks, double-buffered per warp
+  static constexpr int ring = sum + R * 2 * K * Dp * 2;    // partial-aggregate chunks
+  static constexpr int carry = ring + R * RING * slot;     // row-to-row rings
+  static constexpr int rec = carry + 4 * K * slot;         // carry chunks (4 in flight)
+  static constexpr int total = rec + R * kRecords * 6 * 4; // winners records
 };
 
 // The (P2' - P1) table of StereoCost.pathP2 for every |gray difference|, replicated to u16x2.
@@ -221,7 +337,7 @@ struct PathState {
 
 // One min-plus step of one path for the lane's 2*REGS disparities.
 //   prev  predecessor path costs (zeros = no predecessor: the result is then the cost itself)
-//   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1 = P1 replicated.
+//   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1x2 = P1 replicated.
 template <int REGS>
 __device__ __forceinline__ void path_step(const PathState<REGS>& prev, uint32_t q, uint32_t p1x2,
                                           const uint32_t (&c)[REGS], const uint32_t (&pad)[REGS],
@@ -232,15 +348,16 @@ __device__ __forceinline__ void path_step(const PathState<REGS>& prev, uint32_t 
   if (lane == 31) above = 0xffffffffu;
   uint32_t e[REGS];
 #pragma unroll
-  for (int j = 0; j < REGS; j++) e[j] = __byte_perm(prev.v[j], j + 1 < REGS ? prev.v[j + 1] : above, 0x5432);
-  uint32_t dn0 = __byte_perm(below, prev.v[0], 0x5432);
+  for (int j = 0; j < REGS; j++)
+    e[j] = __byte_perm(prev.v[j], j + 1 < REGS ? prev.v[j + 1] : above, 0x5432);
+  const uint32_t dn0 = __byte_perm(below, prev.v[0], 0x5432);
   uint32_t mm = 0xffffffffu;
 #pragma unroll
   for (int j = 0; j < REGS; j++) {
-    uint32_t dn = j == 0 ? dn0 : e[j - 1];
-    uint32_t m3 = __vimin3_u16x2(dn, e[j], q);
-    uint32_t t = __viaddmin_u16x2(m3, p1x2, prev.v[j]);
-    uint32_t L = (t + c[j] - prev.m) | pad[j];
+    const uint32_t dn = j == 0 ? dn0 : e[j - 1];
+    const uint32_t m3 = __vimin3_u16x2(dn, e[j], q);
+    const uint32_t t = __viaddmin_u16x2(m3, p1x2, prev.v[j]);
+    const uint32_t L = (t + c[j] - prev.m) | pad[j];
     out.v[j] = L;
     mm = __vminu2(mm, L);
   }
@@ -248,16 +365,59 @@ __device__ __forceinline__ void path_step(const PathState<REGS>& prev, uint32_t 
   out.m = __reduce_min_sync(0xffffffffu, mm);
 }
 
+// All paths of one pixel, phase by phase (shuffles, then min-plus, then the warp minima) so the
+// independent per-path latency chains overlap.
+template <int REGS, int NP>
+__device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
+                                           const uint32_t (&q)[NP], uint32_t p1x2,
+                                           const uint32_t (&c)[REGS], const uint32_t (&pad)[REGS],
+                                           int lane, PathState<REGS> (&out)[NP]) {
+  uint32_t below[NP], above[NP], mm[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1);
+    above[i] = __shfl_down_sync(0xffffffffu, prev[i].v[0], 1);
+  }
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    if (lane == 0) below[i] = 0xffffffffu;
+    if (lane == 31) above[i] = 0xffffffffu;
+    uint32_t e[REGS];
+#pragma unroll
+    for (int j = 0; j < REGS; j++)
+      e[j] = __byte_perm(prev[i].v[j], j + 1 < REGS ? prev[i].v[j + 1] : above[i], 0x5432);
+    const uint32_t dn0 = __byte_perm(below[i], prev[i].v[0], 0x5432);
+    mm[i] = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < REGS; j++) {
+      const uint32_t dn = j == 0 ? dn0 : e[j - 1];
+      const uint32_t m3 = __vimin3_u16x2(dn, e[j], q[i]);
+      const uint32_t t = __viaddmin_u16x2(m3, p1x2, prev[i].v[j]);
+      const uint32_t L = (t + c[j] - prev[i].m) | pad[j];
+      out[i].v[j] = L;
+      mm[i] = __vminu2(mm[i], L);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NP; i++) mm[i] = __vminu2(mm[i], __byte_perm(mm[i], 0, 0x1032));
+#pragma unroll
+  for (int i = 0; i < NP; i++) out[i].m = __reduce_min_sync(0xffffffffu, mm[i]);
+}
+
 template <int REGS>
 __device__ __forceinline__ void load_state(const uint8_t* slot, int path, int Dp, int lane,
                                            PathState<REGS>& s) {
   const uint32_t* src = (const uint32_t*)(slot + 2 * (path * Dp + lane * 2 * REGS));
   if (REGS == 4) {
-    uint4 v = *(const uint4*)src;
-    s.v[0] = v.x; s.v[REGS > 1 ? 1 : 0] = v.y; s.v[REGS > 2 ? 2 : 0] = v.z; s.v[REGS > 3 ? 3 : 0] = v.w;
+    const uint4 v = *(const uint4*)src;
+    s.v[0] = v.x;
+    s.v[REGS > 1 ? 1 : 0] = v.y;
+    s.v[REGS > 2 ? 2 : 0] = v.z;
+    s.v[REGS > 3 ? 3 : 0] = v.w;
   } else if (REGS == 2) {
-    uint2 v = *(const uint2*)src;
-    s.v[0] = v.x; s.v[REGS > 1 ? 1 : 0] = v.y;
+    const uint2 v = *(const uint2*)src;
+    s.v[0] = v.x;
+    s.v[REGS > 1 ? 1 : 0] = v.y;
   } else {
 #pragma unroll
     for (int j = 0; j < REGS; j++) s.v[j] = src[j];
@@ -270,7 +430,8 @@ __device__ __forceinline__ void store_state(uint8_t* slot, int path, int Dp, int
                                             const PathState<REGS>& s) {
   uint32_t* dst = (uint32_t*)(slot + 2 * (path * Dp + lane * 2 * REGS));
   if (REGS == 4) {
-    *(uint4*)dst = make_uint4(s.v[0], s.v[REGS > 1 ? 1 : 0], s.v[REGS > 2 ? 2 : 0], s.v[REGS > 3 ? 3 : 0]);
+    *(uint4*)dst = make_uint4(s.v[0], s.v[REGS > 1 ? 1 : 0], s.v[REGS > 2 ? 2 : 0],
+                              s.v[REGS > 3 ? 3 : 0]);
   } else if (REGS == 2) {
     *(uint2*)dst = make_uint2(s.v[0], s.v[REGS > 1 ? 1 : 0]);
   } else {
@@ -290,12 +451,12 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
 // Scalar selection of one buffered winners record (CensusSgm.java:471-513 semantics).
 __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, int64_t p,
                               unsigned (&counts)[6]) {
-  int best = r[0], value = r[1], second = r[2], before = r[3], after = r[4], flags = r[5];
+  const int best = r[0], value = r[1], second = r[2], before = r[3], after = r[4], flags = r[5];
   float out = __int_as_float(0x7fc00000);
   uint8_t* reasons = view == 0 ? a.reasons : nullptr;
   uint8_t* boundary = view == 0 ? a.boundary : nullptr;
   if (best >= 0) {
-    bool full = flags == 3;
+    const bool full = flags == 3;
     bool done = false;
     if (full) {
       counts[1]++;
@@ -315,7 +476,7 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
       done = true;
     }
     if (!done && second != INT_MAX) {
-      double slack = fmax(1.0, __dmul_rn((double)value, a.uniqueness));
+      const double slack = fmax(1.0, __dmul_rn((double)value, a.uniqueness));
       if ((double)(second - value) <= slack) {
         counts[4]++;
         if (reasons) reasons[p] = 3;
@@ -325,10 +486,10 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
     if (!done) {
       double offset = 0;
       if (before >= 0 && after >= 0) {
-        double curvature =
+        const double curvature =
             __dsub_rn(__dadd_rn((double)before, (double)after), __dmul_rn(2.0, (double)value));
         if (curvature > 0) {
-          double o =
+          const double o =
               __ddiv_rn(__dmul_rn(0.5, __dsub_rn((double)before, (double)after)), curvature);
           offset = fmax(-0.5, fmin(0.5, o));
         }
@@ -341,23 +502,74 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
   a.disp[view][p] = out;
 }
 
-template <int REGS, int NPATH>
-__global__ void __launch_bounds__(kRows * 32) sweep_kernel(const SweepArgs a) {
+// Winners record of one pixel (GpuStereo.java:758-769 layout) from the lane's aggregate words.
+template <int REGS>
+__device__ __forceinline__ void winners_record(const uint32_t (&s)[REGS], const uint8_t* cb,
+                                               int lane, int D, bool in_region, int32_t* slot) {
+  const int k0 = lane * 2 * REGS;
+  bool valid[2 * REGS];
+#pragma unroll
+  for (int j = 0; j < 2 * REGS; j++) valid[j] = cb[j] != 0x80;
+  const bool f0 = __any_sync(0xffffffffu, lane == 0 && valid[0]);
+  const int last = D - 1 - k0;
+  bool fl = false;
+#pragma unroll
+  for (int j = 0; j < 2 * REGS; j++) fl |= (j == last) && valid[j];
+  fl = __any_sync(0xffffffffu, fl);
+  int r0 = -1, r1 = INT_MAX, r2 = INT_MAX, r3 = -1, r4 = -1;
+  const int r5 = (f0 ? 1 : 0) | (fl ? 2 : 0);
+  if (in_region) {
+    uint32_t key = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < 2 * REGS; j++) {
+      const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
+      if (valid[j]) key = min(key, (sv << 12) | (uint32_t)(k0 + j));
+    }
+    key = __reduce_min_sync(0xffffffffu, key);
+    if (key != 0xffffffffu) {
+      const int best = (int)(key & 0xfffu);
+      uint32_t sec = 0x7fffffffu, bef = 0xffffffffu, aft = 0xffffffffu;
+#pragma unroll
+      for (int j = 0; j < 2 * REGS; j++) {
+        const int k = k0 + j;
+        const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
+        if (valid[j] && abs(k - best) > 1) sec = min(sec, sv);
+        if (valid[j] && k == best - 1) bef = sv;
+        if (valid[j] && k == best + 1) aft = sv;
+      }
+      r0 = best;
+      r1 = (int)(key >> 12);
+      r2 = (int)__reduce_min_sync(0xffffffffu, sec);
+      bef = __reduce_min_sync(0xffffffffu, bef);
+      aft = __reduce_min_sync(0xffffffffu, aft);
+      r3 = bef == 0xffffffffu ? -1 : (int)bef;
+      r4 = aft == 0xffffffffu ? -1 : (int)aft;
+    }
+  }
+  if (lane < 6)
+    slot[lane] = lane == 0 ? r0 : lane == 1 ? r1 : lane == 2 ? r2 : lane == 3 ? r3 : lane == 4 ? r4 : r5;
+}
+
+// K: pixels per staged chunk (power of two); RING: ring slots between consecutive rows;
+// R: rows (warps) per CTA.
+template <int REGS, int NPATH, int K, int RING, int R>
+__global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  const int K = a.chunk;
-  const SweepLayout L(a.Dp, K);
-  uint32_t* lut = (uint32_t*)(smem + L.lut);
-  uint64_t* bars = (uint64_t*)(smem + L.bars);
+  using L = SweepLayout<REGS, K, RING, R>;
+  constexpr int kRows = R;
+  constexpr int Dp = L::Dp;
+  uint32_t* lut = (uint32_t*)(smem + L::lut);
+  uint64_t* bars = (uint64_t*)(smem + L::bars);
   __shared__ int s_ticket;
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int W = a.W, H = a.H, Dp = a.Dp;
+  const int W = a.W, H = a.H;
   if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
   if (lane == 0) {
     for (int i = 0; i < 4; i++) mbar_init(&bars[w * 4 + i], 1);
     if (w == 0)
-      for (int i = 0; i < 3; i++) mbar_init(&bars[kRows * 4 + i], 1);
+      for (int i = 0; i < 4; i++) mbar_init(&bars[kRows * 4 + i], 1);
   }
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
@@ -366,87 +578,95 @@ __global__ void __launch_bounds__(kRows * 32) sweep_kernel(const SweepArgs a) {
   const int stream = ticket & 3, b = ticket >> 2;
   const int view = stream >> 1;
   const bool mirror = (stream & 1) != 0;
-  const int yp = b * kRows + w;                 // row in stream coordinates
-  const int y = mirror ? a.Hp - 1 - yp : yp;    // image row
+  const int yp = b * kRows + w;               // row in stream coordinates
+  const int y = mirror ? a.Hp - 1 - yp : yp;  // image row
   const bool exists = y >= 0 && y < H;
-  const bool first = exists && ((y < a.split) != mirror);
-  const bool finalize = exists && !first;
-  const bool has_next = b + 1 < a.nb;
-  const int ya = mirror ? y + 1 : y - 1;        // image row of the row above (stream order)
-  const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
-
-  const uint8_t* cost = a.cost[view];
-  const uint8_t* gray = a.gray[view];
-  const uint8_t* tex = a.tex[view];
-  uint16_t* sum = a.sum[view];
-  const int nchunks = (W + K - 1) / K;
-  uint8_t* cost_buf = smem + L.cost + w * 2 * K * Dp;
-  uint16_t* sum_buf = (uint16_t*)(smem + L.sum + w * 2 * K * Dp * 2);
-  uint8_t* ring = smem + L.ring + w * kRing * L.slot;
-  const uint8_t* ring_above = smem + L.ring + (w - 1) * kRing * L.slot;
-  uint8_t* carry_buf = smem + L.carry;
-  int32_t* rec = (int32_t*)(smem + L.rec) + w * kRecords * 6;
-  uint64_t* cost_bar = &bars[w * 4];
-  uint64_t* sum_bar = &bars[w * 4 + 2];
-  uint64_t* carry_bar = &bars[kRows * 4];
   const long long limit = a.timeout;
+  unsigned counts[6] = {0, 0, 0, 0, 0, 0};
 
-  // Stream x' -> image column, and the contiguous memory range of a chunk.
-  auto col = [&](int xs) { return mirror ? W - 1 - xs : xs; };
-  auto chunk_first_col = [&](int c) {
-    int lo = c * K, hi = min(W, lo + K);
-    return mirror ? W - hi : lo;
-  };
-  auto chunk_pixels = [&](int c) { return min(W, c * K + K) - c * K; };
-  auto chunk_slot = [&](int xs) {  // position of stream pixel xs inside its chunk buffer
-    int c = xs / K;
-    return mirror ? (min(W, c * K + K) - 1 - xs) : xs - c * K;
-  };
-  int issued_cost = 0, issued_sum = 0, issued_carry = 0;  // chunks issued (uniform per warp)
-  auto issue_cost = [&](int c) {
-    issued_cost = c + 1;
-    if (lane == 0) {
-      fence_proxy_async_shared();
-      bulk_load(cost_buf + (c & 1) * K * Dp, cost + ((int64_t)y * W + chunk_first_col(c)) * Dp,
-                (uint32_t)(chunk_pixels(c) * Dp), &cost_bar[c & 1]);
-    }
-  };
-  auto issue_sum = [&](int c) {
-    issued_sum = c + 1;
-    if (lane == 0) {
-      fence_proxy_async_shared();
-      bulk_load(sum_buf + (c & 1) * K * Dp, sum + ((int64_t)y * W + chunk_first_col(c)) * Dp,
-                (uint32_t)(chunk_pixels(c) * Dp * 2), &sum_bar[c & 1]);
-    }
-  };
-  const int up_index = (stream * a.nb + b - 1);  // carry row written by the previous CTA
-  auto issue_carry = [&](int c) {
-    issued_carry = c + 1;
-    if (lane == 0) {
-      int need = min(W, c * K + K);
-      wait_flag(&a.progress[up_index], need, a.error, limit);
-      fence_proxy_async_global();
-      fence_proxy_async_shared();
-      bulk_load(carry_buf + (c % 3) * K * L.slot,
-                a.carry + ((int64_t)up_index * W + c * K) * L.slot,
-                (uint32_t)(chunk_pixels(c) * L.slot), &carry_bar[c % 3]);
-    }
-  };
-
-  // Per-lane padding mask: disparities >= D stay at 0xffff so they never win a minimum.
-  uint32_t pad[REGS];
-#pragma unroll
-  for (int j = 0; j < REGS; j++) {
-    int k = lane * 2 * REGS + 2 * j;
-    pad[j] = (k >= a.D ? 0xffffu : 0u) | (k + 1 >= a.D ? 0xffff0000u : 0u);
-  }
-  const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
-  const bool use_carry = w == 0 && b > 0;
-
-  // Prologue.
   if (exists) {
+    const bool first = (y < a.split) != mirror;
+    const bool has_next = b + 1 < a.nb;
+    const int ya = mirror ? y + 1 : y - 1;  // image row of the row above (stream order)
+    const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
+    const bool use_carry = w == 0 && b > 0;  // the row above lives in the previous CTA
+    const int dir = mirror ? -1 : 1;
+    const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
+    const int nchunks = (W + K - 1) / K;
+
+    const uint8_t* gray_row = a.gray[view] + (int64_t)y * W + x0;
+    const uint8_t* tex_row = a.tex[view] + (int64_t)y * W + x0;
+    const uint8_t* gray_up = a.gray[view] + (int64_t)(above_exists ? ya : y) * W + x0;
+    const uint8_t* cost_img = a.cost[view] + (int64_t)y * W * Dp;
+    uint16_t* sum_img = a.sum[view] + (int64_t)y * W * Dp;
+    uint8_t* cost_buf = smem + L::cost + w * 2 * K * Dp;
+    uint16_t* sum_buf = (uint16_t*)(smem + L::sum + w * 2 * K * Dp * 2);
+    uint8_t* ring = smem + L::ring + w * RING * L::slot;
+    const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::slot;
+    uint8_t* carry_buf = smem + L::carry;
+    int32_t* rec = (int32_t*)(smem + L::rec) + w * kRecords * 6;
+    uint64_t* cost_bar = &bars[w * 4];
+    uint64_t* sum_bar = &bars[w * 4 + 2];
+    uint64_t* carry_bar = &bars[kRows * 4];
+    uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::slot;
+    const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::slot;
+    const int* carry_progress = &a.progress[stream * a.nb + b - 1];
+
+    // Chunk c of this row in memory order: image columns [first, first + n).
+    auto chunk_n = [&](int c) { return min(K, W - c * K); };
+    auto chunk_first = [&](int c) { return mirror ? W - c * K - chunk_n(c) : c * K; };
+    auto issue_cost = [&](int c) {
+      if (lane == 0) {
+        fence_proxy_async_shared();
+        bulk_load(cost_buf + (c & 1) * K * Dp, cost_img + (int64_t)chunk_first(c) * Dp,
+                  (uint32_t)(chunk_n(c) * Dp), &cost_bar[c & 1]);
+      }
+    };
+    auto issue_sum = [&](int c) {
+      if (lane == 0) {
+        fence_proxy_async_shared();
+        bulk_load(sum_buf + (c & 1) * K * Dp, sum_img + (int64_t)chunk_first(c) * Dp,
+                  (uint32_t)(chunk_n(c) * Dp * 2), &sum_bar[c & 1]);
+      }
+    };
+    // Carry chunks (stream order) of the row above this CTA in a 4-chunk circular buffer.  At
+    // most one chunk is prefetched beyond the last one needed, so the chunk holding pixel xs-1
+    // is never overwritten.
+    int carry_issued = 0, carry_ready = 0;
+    auto carry_issue = [&](bool block) {  // issue the next carry chunk if its data is published
+      if (carry_issued >= nchunks || carry_issued >= carry_ready + 2) return;
+      const int need = min(W, carry_issued * K + K);
+      if (!block) {
+        int published = 0;
+        if (lane == 0) published = *(volatile const int*)carry_progress;
+        published = __shfl_sync(0xffffffffu, published, 0);
+        if (published < need) return;
+      }
+      if (lane == 0) {
+        wait_flag(carry_progress, need, a.error, limit);
+        fence_proxy_async_global();
+        fence_proxy_async_shared();
+        bulk_load(carry_buf + (carry_issued & 3) * K * L::slot, carry_in + (int64_t)carry_issued * K * L::slot,
+                  (uint32_t)(chunk_n(carry_issued) * L::slot), &carry_bar[carry_issued & 3]);
+      }
+      carry_issued++;
+    };
+
+    // Per-lane padding mask: disparities >= D stay at 0xffff so they never win a minimum.
+    uint32_t pad[REGS];
+#pragma unroll
+    for (int j = 0; j < REGS; j++) {
+      const int k = lane * 2 * REGS + 2 * j;
+      pad[j] = (k >= a.D ? 0xffffu : 0u) | (k + 1 >= a.D ? 0xffff0000u : 0u);
+    }
+    const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
+    const bool region_row = y >= a.ry && y < H - a.ry;
+    const int rx = a.rx;
+
+    // Prologue: first chunks in flight; a finalizing row waits until the other stream has stored
+    // its partial aggregate for the whole row.
     issue_cost(0);
-    if (finalize) {
+    if (!first) {
       if (lane == 0) {
         wait_flag(&a.row_done[view * H + y], 1, a.error, limit);
         fence_proxy_async_global();
@@ -454,210 +674,128 @@ __global__ void __launch_bounds__(kRows * 32) sweep_kernel(const SweepArgs a) {
       __syncwarp();
       issue_sum(0);
     }
-  }
-  if (use_carry) issue_carry(0);
+    if (use_carry) carry_issue(true);
 
-  PathState<REGS> horiz;  // (1,0) path in stream coordinates
-  zero_state(horiz);
-  int g_left = 0, ga_l = 0, ga_c = 0, ga_r = 0;
-  if (above_exists) ga_r = __ldg(&gray[(int64_t)ya * W + col(0)]);
-  unsigned counts[6] = {0, 0, 0, 0, 0, 0};
-  const bool region_row = y >= a.ry && y < H - a.ry;
-
-  const int steps = W + 2 * (kRows - 1);
-  for (int step = 0; step < steps; step++) {
-    const int xs = step - 2 * w;
-    if (xs >= 0 && xs < W) {
-      uint8_t* out_slot = ring + (xs & (kRing - 1)) * L.slot;
-      // Carry chunks of the row above this CTA.
-      if (use_carry) {
-        int c = xs / K;
-        if (xs % K == 0) {
-          if (xs == 0) wait_bar(&carry_bar[0], 0, a.error, limit);
-          if (c + 1 < nchunks) issue_carry(c + 1);
-        }
-        if (xs % K == K - 1 && c + 1 < nchunks)
-          wait_bar(&carry_bar[(c + 1) % 3], ((c + 1) / 3) & 1, a.error, limit);
-      }
-      if (exists) {
-        const int c = xs / K;
-        if (xs % K == 0) {
-          wait_bar(&cost_bar[c & 1], (c >> 1) & 1, a.error, limit);
-          if (finalize) wait_bar(&sum_bar[c & 1], (c >> 1) & 1, a.error, limit);
-          __syncwarp();
-          if (c + 1 < nchunks) {
-            issue_cost(c + 1);
-            if (finalize) issue_sum(c + 1);
-          }
-        }
-        const int slot = chunk_slot(xs);
-        const int x = col(xs);
-        const int64_t p = (int64_t)y * W + x;
-        // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
-        const uint8_t* cb = cost_buf + (c & 1) * K * Dp + slot * Dp + lane * 2 * REGS;
-        uint32_t cst[REGS];
-        if (REGS % 2 == 0) {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) {
-            uint32_t word = ((const uint32_t*)cb)[j / 2];
-            uint32_t sel = (j & 1) ? 0xb3a2u : 0x9180u;  // bytes 2j,2j+1, sign-replicated high bytes
-            cst[j] = prmt(word, 0, sel) & 0x027f027fu;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < REGS; j++)
-            cst[j] = prmt(((const uint16_t*)cb)[j], 0, 0x9180u) & 0x027f027fu;
-        }
-        // Gray values for the edge-aware penalties (stream coordinates).
-        const int g_cur = __ldg(&gray[p]);
-        ga_l = ga_c;
-        ga_c = ga_r;
-        ga_r = (above_exists && xs + 1 < W) ? __ldg(&gray[(int64_t)ya * W + col(xs + 1)]) : 0;
-        const bool textured = __ldg(&tex[p]) != 0;
-
-        PathState<REGS> out[NPATH];
-        // (1,0): predecessor xs-1 in this row.
-        {
-          uint32_t q = horiz.m + lut[abs(g_cur - g_left)];
-          path_step<REGS>(horiz, q, p1x2, cst, pad, lane, out[0]);
-        }
-        // Paths from the row above: (0,1) at xs, (1,1) at xs-1, (-1,1) at xs+1.
-        const uint8_t* above_slot[3] = {nullptr, nullptr, nullptr};
+    PathState<REGS> horiz;  // (1,0) path in stream coordinates
+    zero_state(horiz);
+    int g_left = 0, ga_c = 0;
+    int off = 0, c = 0, n_c = chunk_n(0);
+    // Per-chunk pixel data, one pixel per lane (lane i <-> pixel c*K + i): gray | tex << 8 |
+    // gray above << 16 | gray above of the next pixel << 24.  Loaded a chunk ahead.
+    auto chunk_pixels = [&](int cc) -> uint32_t {
+      const int xs_l = cc * K + lane;
+      uint32_t v = 0;
+      if (lane < K && xs_l < W) {
+        v = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
         if (above_exists) {
-          if (w > 0) {
-            above_slot[0] = ring_above + (xs & 3) * L.slot;
-            if (xs >= 1) above_slot[1] = ring_above + ((xs - 1) & 3) * L.slot;
-            if (xs + 1 < W) above_slot[2] = ring_above + ((xs + 1) & 3) * L.slot;
-          } else if (use_carry) {
-            auto cslot = [&](int xx) {
-              return carry_buf + ((xx / K) % 3) * K * L.slot + (xx % K) * L.slot;
-            };
-            above_slot[0] = cslot(xs);
-            if (xs >= 1) above_slot[1] = cslot(xs - 1);
-            if (xs + 1 < W) above_slot[2] = cslot(xs + 1);
-          }
+          v |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
+          if (xs_l + 1 < W) v |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
         }
-        const int g_above[3] = {ga_c, ga_l, ga_r};
+      }
+      return v;
+    };
+    uint32_t px_cur = chunk_pixels(0);
+    uint32_t px_next = nchunks > 1 ? chunk_pixels(1) : 0u;
+    if (above_exists) ga_c = 0;
+
+    // Lock step: warp w handles pixel xs = step - 2w; one CTA barrier per step makes the ring
+    // slots of the row above (pixels xs-1, xs, xs+1, written in earlier steps) visible.
+    const int steps = W + 2 * (kRows - 1);
+    for (int step = 0; step < steps; step++) {
+      const int xs = step - 2 * w;
+      if (xs < 0 || xs >= W) {
+        __syncthreads();
+        continue;
+      }
+      if (use_carry) {
+        const int need_chunk = min(nchunks - 1, (xs + 1) / K);
+        while (carry_ready <= need_chunk) {
+          if (carry_issued <= carry_ready) carry_issue(true);
+          wait_bar(&carry_bar[carry_ready & 3], (carry_ready >> 2) & 1, a.error, limit);
+          carry_ready++;
+        }
+        carry_issue(false);
+      }
+      // Cost / partial-aggregate chunks and the pixel data of the chunk after next.
+      if (off == 0) {
+        if (xs > 0) {
+          px_cur = px_next;
+          px_next = c + 1 < nchunks ? chunk_pixels(c + 1) : 0u;
+        }
+        wait_bar(&cost_bar[c & 1], (c >> 1) & 1, a.error, limit);
+        if (!first) wait_bar(&sum_bar[c & 1], (c >> 1) & 1, a.error, limit);
+        __syncwarp();
+        if (c + 1 < nchunks) {
+          issue_cost(c + 1);
+          if (!first) issue_sum(c + 1);
+        }
+      }
+      const int pos = (c & 1) * K + (mirror ? n_c - 1 - off : off);
+      const int x = x0 + dir * xs;
+      // Ring inputs first (their latency overlaps the cost conversion below).
+      PathState<REGS> prev[NPATH];
+      prev[0] = horiz;
+      const int nbr[3] = {xs, xs - 1, xs + 1};
 #pragma unroll
-        for (int i = 0; i < NPATH - 1; i++) {
-          PathState<REGS> prev;
-          if (above_slot[i])
-            load_state<REGS>(above_slot[i], i, Dp, lane, prev);
-          else
-            zero_state(prev);
-          uint32_t q = prev.m + lut[abs(g_cur - g_above[i])];
-          path_step<REGS>(prev, q, p1x2, cst, pad, lane, out[i + 1]);
+      for (int i = 0; i < NPATH - 1; i++) {
+        const int xx = nbr[i];
+        if (above_exists && (w > 0 || use_carry) && xx >= 0 && xx < W) {
+          const uint8_t* src = w > 0 ? ring_up + (xx & (RING - 1)) * L::slot
+                                     : carry_buf + (xx & (4 * K - 1)) * L::slot;
+          load_state<REGS>(src, i, Dp, lane, prev[i + 1]);
+        } else {
+          zero_state(prev[i + 1]);
         }
-        // Partial aggregate of this stream's paths.
-        uint32_t s[REGS];
+      }
+      // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
+      const uint8_t* cb = cost_buf + pos * Dp + lane * 2 * REGS;
+      uint32_t cst[REGS];
+      if (REGS % 2 == 0) {
 #pragma unroll
         for (int j = 0; j < REGS; j++) {
-          uint32_t acc = out[0].v[j];
-#pragma unroll
-          for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
-          s[j] = acc;
-        }
-        // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured.
-        if (NPATH > 1) {
-#pragma unroll
-          for (int i = 0; i < NPATH - 1; i++) {
-            PathState<REGS> o = out[i + 1];
-            if (!textured) zero_state(o);
-            store_state<REGS>(out_slot, i, Dp, lane, o);
-            if (w == kRows - 1 && has_next)
-              store_state<REGS>(a.carry + ((int64_t)(stream * a.nb + b) * W + xs) * L.slot, i, Dp,
-                                lane, o);
-          }
-        }
-        horiz = out[0];
-        if (!textured) zero_state(horiz);
-        g_left = g_cur;
-
-        if (first) {
-          uint32_t* dst = (uint32_t*)(sum + p * Dp + lane * 2 * REGS);
-#pragma unroll
-          for (int j = 0; j < REGS; j++) dst[j] = s[j];
-        } else {
-          const uint32_t* other =
-              (const uint32_t*)(sum_buf + (c & 1) * K * Dp + slot * Dp + lane * 2 * REGS);
-#pragma unroll
-          for (int j = 0; j < REGS; j++) s[j] += other[j];
-          // Winners record (GpuStereo.java:758-769) for pixels inside the census border.
-          int r0 = -1, r1 = INT_MAX, r2 = INT_MAX, r3 = -1, r4 = -1, r5;
-          const int k0 = lane * 2 * REGS;
-          bool valid[2 * REGS];
-#pragma unroll
-          for (int j = 0; j < 2 * REGS; j++) valid[j] = cb[j] != 0x80;
-          bool f0 = __any_sync(0xffffffffu, lane == 0 && valid[0]);
-          int last = a.D - 1 - k0;
-          bool fl = false;
-#pragma unroll
-          for (int j = 0; j < 2 * REGS; j++) fl |= (j == last) && valid[j];
-          fl = __any_sync(0xffffffffu, fl);
-          r5 = (f0 ? 1 : 0) | (fl ? 2 : 0);
-          if (region_row && x >= a.rx && x < W - a.rx) {
-            uint32_t key = 0xffffffffu;
-#pragma unroll
-            for (int j = 0; j < 2 * REGS; j++) {
-              uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
-              uint32_t kk = (sv << 12) | (uint32_t)(k0 + j);
-              if (valid[j]) key = min(key, kk);
-            }
-            key = __reduce_min_sync(0xffffffffu, key);
-            if (key != 0xffffffffu) {
-              int best = (int)(key & 0xfffu);
-              uint32_t sec = 0x7fffffffu, bef = 0xffffffffu, aft = 0xffffffffu;
-#pragma unroll
-              for (int j = 0; j < 2 * REGS; j++) {
-                int k = k0 + j;
-                uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
-                if (valid[j] && abs(k - best) > 1) sec = min(sec, sv);
-                if (valid[j] && k == best - 1) bef = sv;
-                if (valid[j] && k == best + 1) aft = sv;
-              }
-              r0 = best;
-              r1 = (int)(key >> 12);
-              r2 = (int)__reduce_min_sync(0xffffffffu, sec);
-              bef = __reduce_min_sync(0xffffffffu, bef);
-              aft = __reduce_min_sync(0xffffffffu, aft);
-              r3 = bef == 0xffffffffu ? -1 : (int)bef;
-              r4 = aft == 0xffffffffu ? -1 : (int)aft;
-            }
-          }
-          const int ri = xs % kRecords;
-          if (lane < 6) {
-            int v = lane == 0 ? r0 : lane == 1 ? r1 : lane == 2 ? r2 : lane == 3 ? r3 : lane == 4 ? r4 : r5;
-            rec[ri * 6 + lane] = v;
-          }
-          if (ri == kRecords - 1 || xs == W - 1) {
-            __syncwarp();
-            const int base = xs - ri;
-            if (lane <= ri) {
-              int xx = col(base + lane);
-              select_record(a, view, rec + lane * 6, (int64_t)y * W + xx, counts);
-            }
-            __syncwarp();
-          }
-        }
-        if (first && xs == W - 1) {  // whole row of partial aggregate stored: publish it
-          __syncwarp();
-          if (lane == 0) {
-            __threadfence();
-            atomicExch(&a.row_done[view * H + y], 1);
-          }
+          const uint32_t word = ((const uint32_t*)cb)[j / 2];
+          cst[j] = prmt(word, 0, (j & 1) ? 0xb3a2u : 0x9180u) & 0x027f027fu;
         }
       } else {
-        // Rows beyond the image: the row below sees no predecessor.
-        PathState<REGS> z;
-        zero_state(z);
-        for (int i = 0; i < NPATH - 1; i++) {
-          store_state<REGS>(out_slot, i, Dp, lane, z);
-          if (w == kRows - 1 && has_next)
-            store_state<REGS>(a.carry + ((int64_t)(stream * a.nb + b) * W + xs) * L.slot, i, Dp,
-                              lane, z);
-        }
+#pragma unroll
+        for (int j = 0; j < REGS; j++)
+          cst[j] = prmt(((const uint16_t*)cb)[j], 0, 0x9180u) & 0x027f027fu;
       }
-      // Publish carry progress every chunk (and at the end of the row).
+      // Gray values for the edge-aware penalties (stream order).
+      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, off);
+      const int g_cur = pxv & 0xff;
+      const bool textured = (pxv >> 8) & 1;
+      const int ga_l = ga_c;
+      ga_c = (pxv >> 16) & 0xff;
+      const int ga_r = pxv >> 24;
+      const int g_above[3] = {ga_c, ga_l, ga_r};
+      uint32_t q[NPATH];
+      q[0] = horiz.m + lut[abs(g_cur - g_left)];
+#pragma unroll
+      for (int i = 0; i < NPATH - 1; i++) q[i + 1] = prev[i + 1].m + lut[abs(g_cur - g_above[i])];
+      PathState<REGS> out[NPATH];
+      paths_step<REGS, NPATH>(prev, q, p1x2, cst, pad, lane, out);
+      // Partial aggregate of this stream's paths.
+      uint32_t s[REGS];
+#pragma unroll
+      for (int j = 0; j < REGS; j++) {
+        uint32_t acc = out[0].v[j];
+#pragma unroll
+        for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
+        s[j] = acc;
+      }
+      // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured.
+      uint8_t* out_slot = ring + (xs & (RING - 1)) * L::slot;
+#pragma unroll
+      for (int i = 0; i < NPATH - 1; i++) {
+        PathState<REGS> o = out[i + 1];
+        if (!textured) zero_state(o);
+        store_state<REGS>(out_slot, i, Dp, lane, o);
+        if (w == kRows - 1 && has_next) store_state<REGS>(carry_out + (int64_t)xs * L::slot, i, Dp, lane, o);
+      }
+      horiz = out[0];
+      if (!textured) zero_state(horiz);
+      g_left = g_cur;
       if (w == kRows - 1 && has_next && ((xs + 1) % K == 0 || xs == W - 1)) {
         __syncwarp();
         if (lane == 0) {
@@ -665,20 +803,53 @@ __global__ void __launch_bounds__(kRows * 32) sweep_kernel(const SweepArgs a) {
           atomicExch(&a.progress[stream * a.nb + b], xs + 1);
         }
       }
+
+      if (first) {
+        uint32_t* dst = (uint32_t*)(sum_img + (int64_t)x * Dp + lane * 2 * REGS);
+#pragma unroll
+        for (int j = 0; j < REGS; j++) dst[j] = s[j];
+        if (xs == W - 1) {  // whole row of partial aggregate stored: publish it
+          __syncwarp();
+          if (lane == 0) {
+            __threadfence();
+            atomicExch(&a.row_done[view * H + y], 1);
+          }
+        }
+      } else {
+        const uint32_t* other = (const uint32_t*)(sum_buf + pos * Dp + lane * 2 * REGS);
+#pragma unroll
+        for (int j = 0; j < REGS; j++) s[j] += other[j];
+        const int ri = xs & (kRecords - 1);
+        winners_record<REGS>(s, cb, lane, a.D, region_row && x >= rx && x < W - rx,
+                             rec + ri * 6);
+        if (ri == kRecords - 1 || xs == W - 1) {
+          __syncwarp();
+          if (lane <= ri)
+            select_record(a, view, rec + lane * 6, (int64_t)y * W + x0 + dir * (xs - ri + lane),
+                          counts);
+          __syncwarp();
+        }
+      }
+      if (++off == n_c) {
+        off = 0;
+        c++;
+        if (c < nchunks) n_c = chunk_n(c);
+      }
+      __syncthreads();
     }
-    __syncthreads();
-  }
-  // Drain: every bulk copy this warp issued has landed before the CTA's shared memory is released
-  // (normally already true; after a timed-out wait this bounds the exit on the copies in flight).
-  {
-    int dummy = 0;
-    const long long drain = a.timeout / 4;
-    for (int c = max(0, issued_cost - 2); c < issued_cost; c++)
-      wait_bar(&cost_bar[c & 1], (c >> 1) & 1, &dummy, drain);
-    for (int c = max(0, issued_sum - 2); c < issued_sum; c++)
-      wait_bar(&sum_bar[c & 1], (c >> 1) & 1, &dummy, drain);
-    for (int c = max(0, issued_carry - 3); c < issued_carry; c++)
-      wait_bar(&carry_bar[c % 3], (c / 3) & 1, &dummy, drain);
+    // Drain: every bulk copy this warp issued has landed before the CTA's shared memory is
+    // released (normally already true; after a timed-out wait this bounds the exit).
+    const long long drain = limit / 4;
+    for (int cc = max(0, nchunks - 2); cc < nchunks; cc++) {
+      wait_bar(&cost_bar[cc & 1], (cc >> 1) & 1, a.error, drain, false);
+      if (!first) wait_bar(&sum_bar[cc & 1], (cc >> 1) & 1, a.error, drain, false);
+    }
+    if (use_carry)
+      for (int cc = max(0, carry_issued - 4); cc < carry_issued; cc++)
+        if (cc >= carry_ready) wait_bar(&carry_bar[cc & 3], (cc >> 2) & 1, a.error, drain, false);
+  } else {
+    // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
+    for (int step = 0; step < a.W + 2 * (kRows - 1); step++) __syncthreads();
   }
   // Selection counters of the left view.
   if (view == 0 && a.stats) {
@@ -688,28 +859,35 @@ __global__ void __launch_bounds__(kRows * 32) sweep_kernel(const SweepArgs a) {
                                   &a.stats->ambiguity_rejected, &a.stats->selected};
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-      unsigned total = __reduce_add_sync(0xffffffffu, counts[i]);
+      const unsigned total = __reduce_add_sync(0xffffffffu, counts[i]);
       if (lane == 0 && total) atomicAdd(dst[i], (unsigned long long)total);
     }
   }
 }
 
-template <int REGS, int NPATH>
-cudaError_t launch_sweep(const SweepArgs& a, int shared, cudaStream_t stream) {
-  auto kernel = sweep_kernel<REGS, NPATH>;
+template <int REGS, int NPATH, int K, int RING, int R>
+cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
+  auto kernel = sweep_kernel<REGS, NPATH, K, RING, R>;
+  const int shared = SweepLayout<REGS, K, RING, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
-  kernel<<<4 * a.nb, kRows * 32, shared, stream>>>(a);
+  kernel<<<4 * a.nb, R * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
+constexpr int chunk_for(int regs) { return 4; }
+constexpr int ring_for(int regs) { return regs <= 1 ? 8 : 4; }
+constexpr int rows_for(int regs) { return regs <= 2 ? 16 : 8; }
+
 struct FusedLayout {
   size_t cost, sum, carry, flags, total;
-  int Dp, nb, K, slot;
+  int Dp, nb, K, ring, slot, rows;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
-    nb = (h + kRows - 1) / kRows;
-    K = Dp <= 128 ? 8 : 4;
+    rows = rows_for(Dp / 64);
+    nb = (h + rows - 1) / rows;
+    K = chunk_for(Dp / 64);
+    ring = ring_for(Dp / 64);
     slot = 3 * Dp * 2 + 16;
     size_t n = (size_t)w * h;
     cost = n * Dp;
@@ -768,13 +946,26 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   ca.out[1] = cost_r;
   ca.Dp = F.Dp;
   {
-    int64_t n = (int64_t)w * h;
-    int64_t blocks = (n * 32 + 255) / 256;
-    int grid = (int)std::min<int64_t>(blocks, (int64_t)ctx.sm_count * 32);
+    cudaError_t le;
     ctx.prof->kernel_begin();
-    cost_pair_kernel<<<dim3(grid, 2), 256, 0, ctx.stream>>>(ca);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "cost kernel launch");
+    if (p.cost_mode == CSGM_COST_ZNCC) {
+      int64_t n = (int64_t)w * h;
+      int64_t blocks = (n * 32 + 255) / 256;
+      int grid = (int)std::min<int64_t>(blocks, (int64_t)ctx.sm_count * 32);
+      cost_pair_kernel<<<dim3(grid, 2), 256, 0, ctx.stream>>>(ca);
+      le = cudaGetLastError();
+    } else {
+      const size_t shared = cost_rows_shared(p.disparities, F.Dp);
+      le = cudaFuncSetAttribute(cost_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)shared);
+      if (le == cudaSuccess) {
+        const int64_t items = (int64_t)h * ((w + kCostSeg - 1) / kCostSeg);
+        const int grid = (int)std::min<int64_t>(items, (int64_t)ctx.sm_count * 16);
+        cost_rows_kernel<<<dim3(grid, 2), kCostSeg, shared, ctx.stream>>>(ca);
+        le = cudaGetLastError();
+      }
+    }
+    if (le != cudaSuccess) return cuda_fail(le, "cost kernel launch");
     ctx.prof->kernel_end("cost_pair");
   }
   cudaError_t e = cudaMemsetAsync(flags, 0, F.flags, ctx.stream);
@@ -805,8 +996,8 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.D = p.disparities;
   a.Dp = F.Dp;
   a.nb = F.nb;
-  a.Hp = F.nb * kRows;
-  a.split = kRows * ((F.nb + 1) / 2);
+  a.Hp = F.nb * F.rows;
+  a.split = F.rows * ((F.nb + 1) / 2);
   a.p1 = p.p1;
   a.p2 = p.p2;
   a.edge_scale = p.edge_scale;
@@ -816,19 +1007,23 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.chunk = F.K;
   a.uniqueness = p.uniqueness;
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
-  int shared = SweepLayout(F.Dp, F.K).total;
-  int regs = F.Dp / 64;
-  bool eight = p.directions == 8;
+  const int regs = F.Dp / 64;
+  const bool eight = p.directions == 8;
   ctx.prof->kernel_begin();
   switch (regs * 2 + (eight ? 1 : 0)) {
-    case 2: e = launch_sweep<1, 2>(a, shared, ctx.stream); break;
-    case 3: e = launch_sweep<1, 4>(a, shared, ctx.stream); break;
-    case 4: e = launch_sweep<2, 2>(a, shared, ctx.stream); break;
-    case 5: e = launch_sweep<2, 4>(a, shared, ctx.stream); break;
-    case 6: e = launch_sweep<3, 2>(a, shared, ctx.stream); break;
-    case 7: e = launch_sweep<3, 4>(a, shared, ctx.stream); break;
-    case 8: e = launch_sweep<4, 2>(a, shared, ctx.stream); break;
-    case 9: e = launch_sweep<4, 4>(a, shared, ctx.stream); break;
+#define CSGM_SWEEP_CASE(R_, NP_)                                                             \
+  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                         \
+    e = launch_sweep<R_, NP_, chunk_for(R_), ring_for(R_), rows_for(R_)>(a, ctx.stream);          \
+    break;
+    CSGM_SWEEP_CASE(1, 2)
+    CSGM_SWEEP_CASE(1, 4)
+    CSGM_SWEEP_CASE(2, 2)
+    CSGM_SWEEP_CASE(2, 4)
+    CSGM_SWEEP_CASE(3, 2)
+    CSGM_SWEEP_CASE(3, 4)
+    CSGM_SWEEP_CASE(4, 2)
+    CSGM_SWEEP_CASE(4, 4)
+#undef CSGM_SWEEP_CASE
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
   if (e != cudaSuccess) return cuda_fail(e, "sweep kernel launch");
