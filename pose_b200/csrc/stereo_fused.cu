@@ -7,20 +7,23 @@
 // Design (B200):
 //  * cost_pair_kernel writes both views' cost volumes once, as uint8 [H][W][Dp] with
 //    Dp = D rounded up to 64 and 0x80 marking the reference's invalid cost 512.
-//  * sweep_kernel runs FOUR wavefront streams in one launch: left-down, left-up, right-down,
-//    right-up.  A "down" stream processes rows top to bottom, pixels left to right, and owns the
-//    paths whose predecessor lies above or to the left: (1,0), (0,1), (1,1), (-1,1).  An "up"
-//    stream is the same code on the image mirrored in x and y and owns the four opposite paths.
-//  * One CTA = R consecutive rows, one warp per row; warp w processes pixel x at step x + 2w.
-//    The (0,1), (1,1), (-1,1) path states of a row reach the next row through a 4-slot ring in
-//    shared memory; the (1,0) state stays in registers.  The last row of a CTA also writes a
-//    global carry row that the next CTA of the stream reads (release/acquire progress counter).
+//  * sweep_kernel runs two wavefront streams in one launch, each over both views: "down"
+//    processes rows top to bottom, pixels left to right, and owns the paths whose predecessor
+//    lies above or to the left: (1,0), (0,1), (1,1), (-1,1); "up" is the same code on the image
+//    mirrored in x and y and owns the four opposite paths.
+//  * One CTA = R consecutive image rows; warp w holds row w of BOTH views (lanes 0-15 the left
+//    view, lanes 16-31 the right view) and processes pixel x at step x + 2w, all warps in lock
+//    step (one CTA barrier per step).  The (0,1), (1,1), (-1,1) path states of a row reach the
+//    next row through a shared-memory ring; the (1,0) state stays in registers.  The last row of
+//    a CTA also writes a global carry row that the next CTA of the stream reads
+//    (release/acquire progress counter).
 //  * Meet in the middle: for rows above `split` the down stream runs first and stores its partial
 //    aggregate (uint16); the up stream adds its four paths and selects the winner in registers.
 //    Below `split` the roles swap.  The partial aggregate crosses HBM once each way.
-//  * Disparities live in registers as packed uint16 pairs (REGS registers per lane per path);
-//    the min-plus step uses the DPX instructions __vimin3_u16x2 / __viaddmin_u16x2 and the
-//    warp-wide minimum __reduce_min_sync.
+//  * Disparities live in registers as packed uint16 pairs (REGS registers per lane per path,
+//    16 lanes per view-row); the min-plus step uses the DPX instructions __vimin3_u16x2 /
+//    __viaddmin_u16x2, and the per-row minima of two paths share one 16-lane shuffle butterfly
+//    on packed uint16 pairs.
 //  * Cost, partial-aggregate and carry slices are staged in shared memory by cp.async.bulk with
 //    mbarrier completion (no multicast).  Every wait is bounded; a wait that runs out sets an
 //    error flag that the host turns into CSGM_E_TIMEOUT.
@@ -35,7 +38,7 @@ namespace csgm {
 
 namespace {
 
-constexpr int kRecords = 32;  // selections buffered per warp before the scalar select
+constexpr int kRecords = 16;  // selections buffered per view-row before the scalar select
 
 __host__ __device__ inline int padded_d(int D) { return (D + 63) / 64 * 64; }
 
@@ -294,32 +297,36 @@ struct SweepArgs {
   const uint8_t* tex[2];   // matching-view texture per view
   uint16_t* sum[2];        // partial aggregate [H][W][Dp] per view
   float* disp[2];
-  uint8_t* carry;     // [4][nb][W][slot] bytes
-  int* progress;      // [4][nb]
-  int* row_done;      // [2][H]
+  uint8_t* carry;     // [2 streams][nb][W][2 views][slot] bytes
+  int* progress;      // [2][nb]
+  int* row_done;      // [H]
   int* ticket;
   int* error;
   uint8_t* reasons;   // left view only
   uint8_t* boundary;  // left view only
   DeviceStats* stats; // left view only
-  int W, H, D, Dp, nb, Hp, split, p1, p2, edge_scale, min_disparity, rx, ry, chunk;
+  int W, H, D, nb, Hp, split, p1, p2, edge_scale, min_disparity, rx, ry;
   double uniqueness;
   long long timeout;
 };
 
+constexpr int kViews = 2;   // views per warp
+constexpr int kLanes = 16;  // lanes per view-row
+
 // Shared-memory layout (byte offsets), compile-time for a kernel instance.
 template <int REGS, int K, int RING, int R>
 struct SweepLayout {
-  static constexpr int Dp = 64 * REGS;
+  static constexpr int Dp = 2 * kLanes * REGS;
   static constexpr int slot = 3 * Dp * 2 + 16;             // 3 paths x Dp uint16 + 4 minima
+  static constexpr int vslot = kViews * slot;              // both views of one pixel
   static constexpr int lut = 0;                            // 256 x uint32
   static constexpr int bars = lut + 256 * 4;               // R x 4 + 4 mbarriers
   static constexpr int cost = (bars + (R * 4 + 4) * 8 + 127) / 128 * 128;
-  static constexpr int sum = cost + R * 2 * K * Dp;        // cost chunks, double-buffered per warp
-  static constexpr int ring = sum + R * 2 * K * Dp * 2;    // partial-aggregate chunks
-  static constexpr int carry = ring + R * RING * slot;     // row-to-row rings
-  static constexpr int rec = carry + 4 * K * slot;         // carry chunks (4 in flight)
-  static constexpr int total = rec + R * kRecords * 6 * 4; // winners records
+  static constexpr int sum = cost + R * kViews * 2 * K * Dp;        // cost chunks per warp
+  static constexpr int ring = sum + R * kViews * 2 * K * Dp * 2;    // aggregate chunks per warp
+  static constexpr int carry = ring + R * RING * vslot;             // row-to-row rings
+  static constexpr int rec = carry + 4 * K * vslot;                 // carry chunks (4 in flight)
+  static constexpr int total = rec + R * kViews * kRecords * 6 * 4; // winners records
 };
 
 // The (P2' - P1) table of StereoCost.pathP2 for every |gray difference|, replicated to u16x2.
@@ -335,53 +342,40 @@ struct PathState {
   uint32_t m;  // replicated minimum
 };
 
-// One min-plus step of one path for the lane's 2*REGS disparities.
-//   prev  predecessor path costs (zeros = no predecessor: the result is then the cost itself)
-//   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1x2 = P1 replicated.
-template <int REGS>
-__device__ __forceinline__ void path_step(const PathState<REGS>& prev, uint32_t q, uint32_t p1x2,
-                                          const uint32_t (&c)[REGS], const uint32_t (&pad)[REGS],
-                                          int lane, PathState<REGS>& out) {
-  uint32_t below = __shfl_up_sync(0xffffffffu, prev.v[REGS - 1], 1);
-  uint32_t above = __shfl_down_sync(0xffffffffu, prev.v[0], 1);
-  if (lane == 0) below = 0xffffffffu;
-  if (lane == 31) above = 0xffffffffu;
-  uint32_t e[REGS];
+// Minimum over the 16 lanes of each view-row of two packed uint16 values at once.
+__device__ __forceinline__ uint32_t row_min2(uint32_t packed) {
 #pragma unroll
-  for (int j = 0; j < REGS; j++)
-    e[j] = __byte_perm(prev.v[j], j + 1 < REGS ? prev.v[j + 1] : above, 0x5432);
-  const uint32_t dn0 = __byte_perm(below, prev.v[0], 0x5432);
-  uint32_t mm = 0xffffffffu;
-#pragma unroll
-  for (int j = 0; j < REGS; j++) {
-    const uint32_t dn = j == 0 ? dn0 : e[j - 1];
-    const uint32_t m3 = __vimin3_u16x2(dn, e[j], q);
-    const uint32_t t = __viaddmin_u16x2(m3, p1x2, prev.v[j]);
-    const uint32_t L = (t + c[j] - prev.m) | pad[j];
-    out.v[j] = L;
-    mm = __vminu2(mm, L);
-  }
-  mm = __vminu2(mm, __byte_perm(mm, 0, 0x1032));
-  out.m = __reduce_min_sync(0xffffffffu, mm);
+  for (int o = kLanes / 2; o > 0; o >>= 1)
+    packed = __vminu2(packed, __shfl_xor_sync(0xffffffffu, packed, o));
+  return packed;
 }
 
-// All paths of one pixel, phase by phase (shuffles, then min-plus, then the warp minima) so the
+// Minimum of a 32-bit value over each view-row (lanes 0-15 and 16-31 separately).
+__device__ __forceinline__ uint32_t row_min_u32(uint32_t x, int v) {
+  const uint32_t m0 = __reduce_min_sync(0xffffffffu, v == 0 ? x : 0xffffffffu);
+  const uint32_t m1 = __reduce_min_sync(0xffffffffu, v == 1 ? x : 0xffffffffu);
+  return v ? m1 : m0;
+}
+
+// All paths of one pixel (each lane: its view's 2*REGS disparities), phase by phase so the
 // independent per-path latency chains overlap.
+//   prev  predecessor path costs (zeros = no predecessor: the result is then the cost itself)
+//   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1x2 = P1 replicated.
 template <int REGS, int NP>
 __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
                                            const uint32_t (&q)[NP], uint32_t p1x2,
                                            const uint32_t (&c)[REGS], const uint32_t (&pad)[REGS],
-                                           int lane, PathState<REGS> (&out)[NP]) {
+                                           int sl, PathState<REGS> (&out)[NP]) {
   uint32_t below[NP], above[NP], mm[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1);
-    above[i] = __shfl_down_sync(0xffffffffu, prev[i].v[0], 1);
+    below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1, kLanes);
+    above[i] = __shfl_down_sync(0xffffffffu, prev[i].v[0], 1, kLanes);
   }
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    if (lane == 0) below[i] = 0xffffffffu;
-    if (lane == 31) above[i] = 0xffffffffu;
+    if (sl == 0) below[i] = 0xffffffffu;
+    if (sl == kLanes - 1) above[i] = 0xffffffffu;
     uint32_t e[REGS];
 #pragma unroll
     for (int j = 0; j < REGS; j++)
@@ -398,47 +392,59 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
       mm[i] = __vminu2(mm[i], L);
     }
   }
+  // Lane minima of two paths packed into one word, then one butterfly per pair of paths.
 #pragma unroll
-  for (int i = 0; i < NP; i++) mm[i] = __vminu2(mm[i], __byte_perm(mm[i], 0, 0x1032));
-#pragma unroll
-  for (int i = 0; i < NP; i++) out[i].m = __reduce_min_sync(0xffffffffu, mm[i]);
+  for (int i = 0; i < NP; i += 2) {
+    const uint32_t lo = __vminu2(mm[i], __byte_perm(mm[i], 0, 0x1032)) & 0xffffu;
+    const uint32_t hi = i + 1 < NP ? __vminu2(mm[i + 1], __byte_perm(mm[i + 1], 0, 0x1032)) & 0xffff0000u
+                                   : 0xffff0000u;
+    const uint32_t r = row_min2(lo | hi);
+    out[i].m = (r & 0xffffu) | (r << 16);
+    if (i + 1 < NP) out[i + 1].m = (r >> 16) | (r & 0xffff0000u);
+  }
 }
 
 template <int REGS>
-__device__ __forceinline__ void load_state(const uint8_t* slot, int path, int Dp, int lane,
+__device__ __forceinline__ void load_state(const uint8_t* slot, int path, int sl,
                                            PathState<REGS>& s) {
-  const uint32_t* src = (const uint32_t*)(slot + 2 * (path * Dp + lane * 2 * REGS));
-  if (REGS == 4) {
-    const uint4 v = *(const uint4*)src;
-    s.v[0] = v.x;
-    s.v[REGS > 1 ? 1 : 0] = v.y;
-    s.v[REGS > 2 ? 2 : 0] = v.z;
-    s.v[REGS > 3 ? 3 : 0] = v.w;
-  } else if (REGS == 2) {
-    const uint2 v = *(const uint2*)src;
-    s.v[0] = v.x;
-    s.v[REGS > 1 ? 1 : 0] = v.y;
+  constexpr int Dp = 2 * kLanes * REGS;
+  const uint32_t* src = (const uint32_t*)(slot + 2 * (path * Dp + sl * 2 * REGS));
+  if (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4) {
+      const uint4 v = *(const uint4*)(src + j);
+      s.v[j] = v.x;
+      s.v[j + 1 < REGS ? j + 1 : 0] = v.y;
+      s.v[j + 2 < REGS ? j + 2 : 0] = v.z;
+      s.v[j + 3 < REGS ? j + 3 : 0] = v.w;
+    }
   } else {
 #pragma unroll
-    for (int j = 0; j < REGS; j++) s.v[j] = src[j];
+    for (int j = 0; j < REGS; j += 2) {
+      const uint2 v = *(const uint2*)(src + j);
+      s.v[j] = v.x;
+      s.v[j + 1 < REGS ? j + 1 : 0] = v.y;
+    }
   }
   s.m = ((const uint32_t*)(slot + 6 * Dp))[path];
 }
 
 template <int REGS>
-__device__ __forceinline__ void store_state(uint8_t* slot, int path, int Dp, int lane,
+__device__ __forceinline__ void store_state(uint8_t* slot, int path, int sl,
                                             const PathState<REGS>& s) {
-  uint32_t* dst = (uint32_t*)(slot + 2 * (path * Dp + lane * 2 * REGS));
-  if (REGS == 4) {
-    *(uint4*)dst = make_uint4(s.v[0], s.v[REGS > 1 ? 1 : 0], s.v[REGS > 2 ? 2 : 0],
-                              s.v[REGS > 3 ? 3 : 0]);
-  } else if (REGS == 2) {
-    *(uint2*)dst = make_uint2(s.v[0], s.v[REGS > 1 ? 1 : 0]);
+  constexpr int Dp = 2 * kLanes * REGS;
+  uint32_t* dst = (uint32_t*)(slot + 2 * (path * Dp + sl * 2 * REGS));
+  if (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4)
+      *(uint4*)(dst + j) = make_uint4(s.v[j], s.v[j + 1 < REGS ? j + 1 : 0],
+                                      s.v[j + 2 < REGS ? j + 2 : 0], s.v[j + 3 < REGS ? j + 3 : 0]);
   } else {
 #pragma unroll
-    for (int j = 0; j < REGS; j++) dst[j] = s.v[j];
+    for (int j = 0; j < REGS; j += 2)
+      *(uint2*)(dst + j) = make_uint2(s.v[j], s.v[j + 1 < REGS ? j + 1 : 0]);
   }
-  if (lane == 0) ((uint32_t*)(slot + 6 * Dp))[path] = s.m;
+  if (sl == 0) ((uint32_t*)(slot + 6 * Dp))[path] = s.m;
 }
 
 template <int REGS>
@@ -455,22 +461,23 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
   float out = __int_as_float(0x7fc00000);
   uint8_t* reasons = view == 0 ? a.reasons : nullptr;
   uint8_t* boundary = view == 0 ? a.boundary : nullptr;
+  const bool count = view == 0;
   if (best >= 0) {
     const bool full = flags == 3;
     bool done = false;
     if (full) {
-      counts[1]++;
+      counts[1] += count;
       if (boundary) boundary[p] = 4;
     }
     if (best == 0 || best == a.D - 1) {
-      counts[2]++;
+      counts[2] += count;
       if (reasons) reasons[p] = 2;
       if (full && best == 0) {
-        counts[0]++;
+        counts[0] += count;
         if (boundary) boundary[p] |= 1;
       }
       if (full && best == a.D - 1) {
-        counts[3]++;
+        counts[3] += count;
         if (boundary) boundary[p] |= 2;
       }
       done = true;
@@ -478,7 +485,7 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
     if (!done && second != INT_MAX) {
       const double slack = fmax(1.0, __dmul_rn((double)value, a.uniqueness));
       if ((double)(second - value) <= slack) {
-        counts[4]++;
+        counts[4] += count;
         if (reasons) reasons[p] = 3;
         done = true;
       }
@@ -495,59 +502,66 @@ __device__ void select_record(const SweepArgs& a, int view, const int32_t* r, in
         }
       }
       out = __double2float_rn(__dadd_rn((double)(a.min_disparity + best), offset));
-      counts[5]++;
+      counts[5] += count;
       if (reasons) reasons[p] = 0;
     }
   }
   a.disp[view][p] = out;
 }
 
-// Winners record of one pixel (GpuStereo.java:758-769 layout) from the lane's aggregate words.
+// Winners record of one pixel (GpuStereo.java:758-769 layout) from the lane's aggregate words;
+// every view-row computes its own record.
 template <int REGS>
 __device__ __forceinline__ void winners_record(const uint32_t (&s)[REGS], const uint8_t* cb,
-                                               int lane, int D, bool in_region, int32_t* slot) {
-  const int k0 = lane * 2 * REGS;
+                                               int lane, int v, int sl, int D, bool in_region,
+                                               int32_t* slot) {
+  const int k0 = sl * 2 * REGS;
   bool valid[2 * REGS];
 #pragma unroll
   for (int j = 0; j < 2 * REGS; j++) valid[j] = cb[j] != 0x80;
-  const bool f0 = __any_sync(0xffffffffu, lane == 0 && valid[0]);
+  const unsigned b0 = __ballot_sync(0xffffffffu, sl == 0 && valid[0]);
   const int last = D - 1 - k0;
   bool fl = false;
 #pragma unroll
   for (int j = 0; j < 2 * REGS; j++) fl |= (j == last) && valid[j];
-  fl = __any_sync(0xffffffffu, fl);
+  const unsigned bl = __ballot_sync(0xffffffffu, fl);
+  const unsigned half = v ? 0xffff0000u : 0x0000ffffu;
   int r0 = -1, r1 = INT_MAX, r2 = INT_MAX, r3 = -1, r4 = -1;
-  const int r5 = (f0 ? 1 : 0) | (fl ? 2 : 0);
+  const int r5 = ((b0 & half) ? 1 : 0) | ((bl & half) ? 2 : 0);
+  uint32_t key = 0xffffffffu;
   if (in_region) {
-    uint32_t key = 0xffffffffu;
 #pragma unroll
     for (int j = 0; j < 2 * REGS; j++) {
       const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
       if (valid[j]) key = min(key, (sv << 12) | (uint32_t)(k0 + j));
     }
-    key = __reduce_min_sync(0xffffffffu, key);
-    if (key != 0xffffffffu) {
-      const int best = (int)(key & 0xfffu);
-      uint32_t sec = 0x7fffffffu, bef = 0xffffffffu, aft = 0xffffffffu;
-#pragma unroll
-      for (int j = 0; j < 2 * REGS; j++) {
-        const int k = k0 + j;
-        const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
-        if (valid[j] && abs(k - best) > 1) sec = min(sec, sv);
-        if (valid[j] && k == best - 1) bef = sv;
-        if (valid[j] && k == best + 1) aft = sv;
-      }
-      r0 = best;
-      r1 = (int)(key >> 12);
-      r2 = (int)__reduce_min_sync(0xffffffffu, sec);
-      bef = __reduce_min_sync(0xffffffffu, bef);
-      aft = __reduce_min_sync(0xffffffffu, aft);
-      r3 = bef == 0xffffffffu ? -1 : (int)bef;
-      r4 = aft == 0xffffffffu ? -1 : (int)aft;
-    }
   }
-  if (lane < 6)
-    slot[lane] = lane == 0 ? r0 : lane == 1 ? r1 : lane == 2 ? r2 : lane == 3 ? r3 : lane == 4 ? r4 : r5;
+  key = row_min_u32(key, v);
+  const int best = key != 0xffffffffu ? (int)(key & 0xfffu) : -1;
+  uint32_t sec = 0x7fffffffu, bef = 0xffffffffu, aft = 0xffffffffu;
+#pragma unroll
+  for (int j = 0; j < 2 * REGS; j++) {
+    const int k = k0 + j;
+    const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
+    if (valid[j] && abs(k - best) > 1) sec = min(sec, sv);
+    if (valid[j] && k == best - 1) bef = sv;
+    if (valid[j] && k == best + 1) aft = sv;
+  }
+  sec = row_min_u32(sec, v);
+  // The owner lanes of best-1 and best+1 hand their values to the whole view-row.
+  const int own_b = v * kLanes + (best >= 1 ? (best - 1) / (2 * REGS) : 0);
+  const int own_a = v * kLanes + min(kLanes - 1, best >= 0 ? (best + 1) / (2 * REGS) : 0);
+  bef = __shfl_sync(0xffffffffu, bef, own_b);
+  aft = __shfl_sync(0xffffffffu, aft, own_a);
+  if (best >= 0) {
+    r0 = best;
+    r1 = (int)(key >> 12);
+    r2 = (int)sec;
+    r3 = best >= 1 && bef != 0xffffffffu ? (int)bef : -1;
+    r4 = aft != 0xffffffffu ? (int)aft : -1;
+  }
+  if (sl < 6)
+    slot[sl] = sl == 0 ? r0 : sl == 1 ? r1 : sl == 2 ? r2 : sl == 3 ? r3 : sl == 4 ? r4 : r5;
 }
 
 // K: pixels per staged chunk (power of two); RING: ring slots between consecutive rows;
@@ -556,33 +570,33 @@ template <int REGS, int NPATH, int K, int RING, int R>
 __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   using L = SweepLayout<REGS, K, RING, R>;
-  constexpr int kRows = R;
   constexpr int Dp = L::Dp;
   uint32_t* lut = (uint32_t*)(smem + L::lut);
   uint64_t* bars = (uint64_t*)(smem + L::bars);
   __shared__ int s_ticket;
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int v = lane / kLanes, sl = lane % kLanes;  // view and lane within the view-row
   const int W = a.W, H = a.H;
   if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
   if (lane == 0) {
     for (int i = 0; i < 4; i++) mbar_init(&bars[w * 4 + i], 1);
     if (w == 0)
-      for (int i = 0; i < 4; i++) mbar_init(&bars[kRows * 4 + i], 1);
+      for (int i = 0; i < 4; i++) mbar_init(&bars[R * 4 + i], 1);
   }
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
 
   const int ticket = s_ticket;
-  const int stream = ticket & 3, b = ticket >> 2;
-  const int view = stream >> 1;
-  const bool mirror = (stream & 1) != 0;
-  const int yp = b * kRows + w;               // row in stream coordinates
+  const int stream = ticket & 1, b = ticket >> 1;
+  const bool mirror = stream != 0;
+  const int yp = b * R + w;                   // row in stream coordinates
   const int y = mirror ? a.Hp - 1 - yp : yp;  // image row
   const bool exists = y >= 0 && y < H;
   const long long limit = a.timeout;
   unsigned counts[6] = {0, 0, 0, 0, 0, 0};
+  const int steps = W + 2 * (R - 1);
 
   if (exists) {
     const bool first = (y < a.split) != mirror;
@@ -594,22 +608,21 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
     const int nchunks = (W + K - 1) / K;
 
-    const uint8_t* gray_row = a.gray[view] + (int64_t)y * W + x0;
-    const uint8_t* tex_row = a.tex[view] + (int64_t)y * W + x0;
-    const uint8_t* gray_up = a.gray[view] + (int64_t)(above_exists ? ya : y) * W + x0;
-    const uint8_t* cost_img = a.cost[view] + (int64_t)y * W * Dp;
-    uint16_t* sum_img = a.sum[view] + (int64_t)y * W * Dp;
-    uint8_t* cost_buf = smem + L::cost + w * 2 * K * Dp;
-    uint16_t* sum_buf = (uint16_t*)(smem + L::sum + w * 2 * K * Dp * 2);
-    uint8_t* ring = smem + L::ring + w * RING * L::slot;
-    const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::slot;
+    const uint8_t* gray_row = a.gray[v] + (int64_t)y * W + x0;
+    const uint8_t* tex_row = a.tex[v] + (int64_t)y * W + x0;
+    const uint8_t* gray_up = a.gray[v] + (int64_t)(above_exists ? ya : y) * W + x0;
+    uint16_t* sum_mine = a.sum[v] + (int64_t)y * W * Dp;
+    uint8_t* cost_buf = smem + L::cost + w * kViews * 2 * K * Dp;          // [view][2][K][Dp]
+    uint16_t* sum_buf = (uint16_t*)(smem + L::sum + w * kViews * 2 * K * Dp * 2);
+    uint8_t* ring = smem + L::ring + w * RING * L::vslot;
+    const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::vslot;
     uint8_t* carry_buf = smem + L::carry;
-    int32_t* rec = (int32_t*)(smem + L::rec) + w * kRecords * 6;
+    int32_t* rec = (int32_t*)(smem + L::rec) + (w * kViews + v) * kRecords * 6;
     uint64_t* cost_bar = &bars[w * 4];
     uint64_t* sum_bar = &bars[w * 4 + 2];
-    uint64_t* carry_bar = &bars[kRows * 4];
-    uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::slot;
-    const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::slot;
+    uint64_t* carry_bar = &bars[R * 4];
+    uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
+    const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
     const int* carry_progress = &a.progress[stream * a.nb + b - 1];
 
     // Chunk c of this row in memory order: image columns [first, first + n).
@@ -618,22 +631,44 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     auto issue_cost = [&](int c) {
       if (lane == 0) {
         fence_proxy_async_shared();
-        bulk_load(cost_buf + (c & 1) * K * Dp, cost_img + (int64_t)chunk_first(c) * Dp,
-                  (uint32_t)(chunk_n(c) * Dp), &cost_bar[c & 1]);
+        const int64_t off = ((int64_t)y * W + chunk_first(c)) * Dp;
+        const uint32_t bytes = (uint32_t)(chunk_n(c) * Dp);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_u32(&cost_bar[c & 1])),
+                     "r"(2 * bytes)
+                     : "memory");
+#pragma unroll
+        for (int vv = 0; vv < kViews; vv++)
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+              "[%3];" ::"r"(smem_u32(cost_buf + (vv * 2 + (c & 1)) * K * Dp)),
+              "l"(a.cost[vv] + off), "r"(bytes), "r"(smem_u32(&cost_bar[c & 1]))
+              : "memory");
       }
     };
     auto issue_sum = [&](int c) {
       if (lane == 0) {
         fence_proxy_async_shared();
-        bulk_load(sum_buf + (c & 1) * K * Dp, sum_img + (int64_t)chunk_first(c) * Dp,
-                  (uint32_t)(chunk_n(c) * Dp * 2), &sum_bar[c & 1]);
+        const int64_t off = ((int64_t)y * W + chunk_first(c)) * Dp;
+        const uint32_t bytes = (uint32_t)(chunk_n(c) * Dp * 2);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_u32(&sum_bar[c & 1])),
+                     "r"(2 * bytes)
+                     : "memory");
+#pragma unroll
+        for (int vv = 0; vv < kViews; vv++)
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+              "[%3];" ::"r"(smem_u32(sum_buf + (vv * 2 + (c & 1)) * K * Dp)),
+              "l"(a.sum[vv] + off), "r"(bytes), "r"(smem_u32(&sum_bar[c & 1]))
+              : "memory");
       }
     };
     // Carry chunks (stream order) of the row above this CTA in a 4-chunk circular buffer.  At
     // most one chunk is prefetched beyond the last one needed, so the chunk holding pixel xs-1
     // is never overwritten.
     int carry_issued = 0, carry_ready = 0;
-    auto carry_issue = [&](bool block) {  // issue the next carry chunk if its data is published
+    auto carry_issue = [&](bool block) {
       if (carry_issued >= nchunks || carry_issued >= carry_ready + 2) return;
       const int need = min(W, carry_issued * K + K);
       if (!block) {
@@ -646,8 +681,9 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
         wait_flag(carry_progress, need, a.error, limit);
         fence_proxy_async_global();
         fence_proxy_async_shared();
-        bulk_load(carry_buf + (carry_issued & 3) * K * L::slot, carry_in + (int64_t)carry_issued * K * L::slot,
-                  (uint32_t)(chunk_n(carry_issued) * L::slot), &carry_bar[carry_issued & 3]);
+        bulk_load(carry_buf + (carry_issued & 3) * K * L::vslot,
+                  carry_in + (int64_t)carry_issued * K * L::vslot,
+                  (uint32_t)(chunk_n(carry_issued) * L::vslot), &carry_bar[carry_issued & 3]);
       }
       carry_issued++;
     };
@@ -656,7 +692,7 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     uint32_t pad[REGS];
 #pragma unroll
     for (int j = 0; j < REGS; j++) {
-      const int k = lane * 2 * REGS + 2 * j;
+      const int k = sl * 2 * REGS + 2 * j;
       pad[j] = (k >= a.D ? 0xffffu : 0u) | (k + 1 >= a.D ? 0xffff0000u : 0u);
     }
     const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
@@ -668,7 +704,7 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     issue_cost(0);
     if (!first) {
       if (lane == 0) {
-        wait_flag(&a.row_done[view * H + y], 1, a.error, limit);
+        wait_flag(&a.row_done[y], 1, a.error, limit);
         fence_proxy_async_global();
       }
       __syncwarp();
@@ -680,27 +716,25 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     zero_state(horiz);
     int g_left = 0, ga_c = 0;
     int off = 0, c = 0, n_c = chunk_n(0);
-    // Per-chunk pixel data, one pixel per lane (lane i <-> pixel c*K + i): gray | tex << 8 |
-    // gray above << 16 | gray above of the next pixel << 24.  Loaded a chunk ahead.
+    // Per-chunk pixel data, lane sl < K of each view-row <-> pixel c*K + sl of that view:
+    // gray | tex << 8 | gray above << 16 | gray above of the next pixel << 24.
     auto chunk_pixels = [&](int cc) -> uint32_t {
-      const int xs_l = cc * K + lane;
-      uint32_t v = 0;
-      if (lane < K && xs_l < W) {
-        v = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
+      const int xs_l = cc * K + sl;
+      uint32_t d = 0;
+      if (sl < K && xs_l < W) {
+        d = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
         if (above_exists) {
-          v |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
-          if (xs_l + 1 < W) v |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
+          d |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
+          if (xs_l + 1 < W) d |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
         }
       }
-      return v;
+      return d;
     };
     uint32_t px_cur = chunk_pixels(0);
     uint32_t px_next = nchunks > 1 ? chunk_pixels(1) : 0u;
-    if (above_exists) ga_c = 0;
 
     // Lock step: warp w handles pixel xs = step - 2w; one CTA barrier per step makes the ring
     // slots of the row above (pixels xs-1, xs, xs+1, written in earlier steps) visible.
-    const int steps = W + 2 * (kRows - 1);
     for (int step = 0; step < steps; step++) {
       const int xs = step - 2 * w;
       if (xs < 0 || xs >= W) {
@@ -716,7 +750,7 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
         }
         carry_issue(false);
       }
-      // Cost / partial-aggregate chunks and the pixel data of the chunk after next.
+      // Cost / partial-aggregate chunks and the pixel data of the next chunk.
       if (off == 0) {
         if (xs > 0) {
           px_cur = px_next;
@@ -730,39 +764,35 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
           if (!first) issue_sum(c + 1);
         }
       }
-      const int pos = (c & 1) * K + (mirror ? n_c - 1 - off : off);
+      const int pos = (v * 2 + (c & 1)) * K + (mirror ? n_c - 1 - off : off);
       const int x = x0 + dir * xs;
       // Ring inputs first (their latency overlaps the cost conversion below).
       PathState<REGS> prev[NPATH];
       prev[0] = horiz;
       const int nbr[3] = {xs, xs - 1, xs + 1};
+      const bool from_ring = above_exists && w > 0;
 #pragma unroll
       for (int i = 0; i < NPATH - 1; i++) {
         const int xx = nbr[i];
-        if (above_exists && (w > 0 || use_carry) && xx >= 0 && xx < W) {
-          const uint8_t* src = w > 0 ? ring_up + (xx & (RING - 1)) * L::slot
-                                     : carry_buf + (xx & (4 * K - 1)) * L::slot;
-          load_state<REGS>(src, i, Dp, lane, prev[i + 1]);
+        if ((from_ring || use_carry) && xx >= 0 && xx < W) {
+          const uint8_t* src = from_ring ? ring_up + (xx & (RING - 1)) * L::vslot
+                                         : carry_buf + (xx & (4 * K - 1)) * L::vslot;
+          load_state<REGS>(src + v * L::slot, i, sl, prev[i + 1]);
         } else {
           zero_state(prev[i + 1]);
         }
       }
       // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
-      const uint8_t* cb = cost_buf + pos * Dp + lane * 2 * REGS;
+      const uint8_t* cb = cost_buf + pos * Dp + sl * 2 * REGS;
       uint32_t cst[REGS];
-      if (REGS % 2 == 0) {
 #pragma unroll
-        for (int j = 0; j < REGS; j++) {
-          const uint32_t word = ((const uint32_t*)cb)[j / 2];
-          cst[j] = prmt(word, 0, (j & 1) ? 0xb3a2u : 0x9180u) & 0x027f027fu;
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < REGS; j++)
-          cst[j] = prmt(((const uint16_t*)cb)[j], 0, 0x9180u) & 0x027f027fu;
+      for (int j = 0; j < REGS; j += 2) {
+        const uint32_t word = ((const uint32_t*)cb)[j / 2];
+        cst[j] = prmt(word, 0, 0x9180u) & 0x027f027fu;
+        if (j + 1 < REGS) cst[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xb3a2u) & 0x027f027fu;
       }
-      // Gray values for the edge-aware penalties (stream order).
-      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, off);
+      // Gray values for the edge-aware penalties (stream order), this view's row.
+      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes + off);
       const int g_cur = pxv & 0xff;
       const bool textured = (pxv >> 8) & 1;
       const int ga_l = ga_c;
@@ -774,7 +804,7 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
 #pragma unroll
       for (int i = 0; i < NPATH - 1; i++) q[i + 1] = prev[i + 1].m + lut[abs(g_cur - g_above[i])];
       PathState<REGS> out[NPATH];
-      paths_step<REGS, NPATH>(prev, q, p1x2, cst, pad, lane, out);
+      paths_step<REGS, NPATH>(prev, q, p1x2, cst, pad, sl, out);
       // Partial aggregate of this stream's paths.
       uint32_t s[REGS];
 #pragma unroll
@@ -785,18 +815,19 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
         s[j] = acc;
       }
       // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured.
-      uint8_t* out_slot = ring + (xs & (RING - 1)) * L::slot;
+      uint8_t* out_slot = ring + (xs & (RING - 1)) * L::vslot + v * L::slot;
 #pragma unroll
       for (int i = 0; i < NPATH - 1; i++) {
         PathState<REGS> o = out[i + 1];
         if (!textured) zero_state(o);
-        store_state<REGS>(out_slot, i, Dp, lane, o);
-        if (w == kRows - 1 && has_next) store_state<REGS>(carry_out + (int64_t)xs * L::slot, i, Dp, lane, o);
+        store_state<REGS>(out_slot, i, sl, o);
+        if (w == R - 1 && has_next)
+          store_state<REGS>(carry_out + (int64_t)xs * L::vslot + v * L::slot, i, sl, o);
       }
       horiz = out[0];
       if (!textured) zero_state(horiz);
       g_left = g_cur;
-      if (w == kRows - 1 && has_next && ((xs + 1) % K == 0 || xs == W - 1)) {
+      if (w == R - 1 && has_next && ((xs + 1) % K == 0 || xs == W - 1)) {
         __syncwarp();
         if (lane == 0) {
           __threadfence();
@@ -805,28 +836,34 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
       }
 
       if (first) {
-        uint32_t* dst = (uint32_t*)(sum_img + (int64_t)x * Dp + lane * 2 * REGS);
+        uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
+        if (REGS % 4 == 0) {
 #pragma unroll
-        for (int j = 0; j < REGS; j++) dst[j] = s[j];
-        if (xs == W - 1) {  // whole row of partial aggregate stored: publish it
+          for (int j = 0; j < REGS; j += 4)
+            *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
+                                            s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < REGS; j++) dst[j] = s[j];
+        }
+        if (xs == W - 1) {  // whole row of partial aggregate stored (both views): publish it
           __syncwarp();
           if (lane == 0) {
             __threadfence();
-            atomicExch(&a.row_done[view * H + y], 1);
+            atomicExch(&a.row_done[y], 1);
           }
         }
       } else {
-        const uint32_t* other = (const uint32_t*)(sum_buf + pos * Dp + lane * 2 * REGS);
+        const uint32_t* other = (const uint32_t*)(sum_buf + pos * Dp + sl * 2 * REGS);
 #pragma unroll
         for (int j = 0; j < REGS; j++) s[j] += other[j];
         const int ri = xs & (kRecords - 1);
-        winners_record<REGS>(s, cb, lane, a.D, region_row && x >= rx && x < W - rx,
+        winners_record<REGS>(s, cb, lane, v, sl, a.D, region_row && x >= rx && x < W - rx,
                              rec + ri * 6);
         if (ri == kRecords - 1 || xs == W - 1) {
           __syncwarp();
-          if (lane <= ri)
-            select_record(a, view, rec + lane * 6, (int64_t)y * W + x0 + dir * (xs - ri + lane),
-                          counts);
+          if (sl <= ri)
+            select_record(a, v, rec + sl * 6, (int64_t)y * W + x0 + dir * (xs - ri + sl), counts);
           __syncwarp();
         }
       }
@@ -849,10 +886,10 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
         if (cc >= carry_ready) wait_bar(&carry_bar[cc & 3], (cc >> 2) & 1, a.error, drain, false);
   } else {
     // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
-    for (int step = 0; step < a.W + 2 * (kRows - 1); step++) __syncthreads();
+    for (int step = 0; step < steps; step++) __syncthreads();
   }
-  // Selection counters of the left view.
-  if (view == 0 && a.stats) {
+  // Selection counters of the left view (lanes of the right view hold zeros).
+  if (a.stats) {
     unsigned long long* dst[6] = {&a.stats->lower_boundary_rejected,
                                   &a.stats->full_interval_pixels, &a.stats->boundary_rejected,
                                   &a.stats->upper_boundary_rejected,
@@ -871,12 +908,13 @@ cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
   const int shared = SweepLayout<REGS, K, RING, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
-  kernel<<<4 * a.nb, R * 32, shared, stream>>>(a);
+  kernel<<<2 * a.nb, R * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
-constexpr int chunk_for(int regs) { return 4; }
-constexpr int ring_for(int regs) { return regs <= 1 ? 8 : 4; }
+// Per-register-count configuration: chunk pixels, ring slots, rows per CTA (shared memory fit).
+constexpr int chunk_for(int regs) { return regs >= 8 ? 2 : 4; }
+constexpr int ring_for(int regs) { return regs <= 2 ? 8 : 4; }
 constexpr int rows_for(int regs) { return regs <= 2 ? 16 : 8; }
 
 struct FusedLayout {
@@ -884,16 +922,17 @@ struct FusedLayout {
   int Dp, nb, K, ring, slot, rows;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
-    rows = rows_for(Dp / 64);
+    const int regs = Dp / (2 * kLanes);
+    rows = rows_for(regs);
     nb = (h + rows - 1) / rows;
-    K = chunk_for(Dp / 64);
-    ring = ring_for(Dp / 64);
+    K = chunk_for(regs);
+    ring = ring_for(regs);
     slot = 3 * Dp * 2 + 16;
     size_t n = (size_t)w * h;
     cost = n * Dp;
     sum = n * Dp * 2;
-    carry = (size_t)4 * nb * w * slot;
-    flags = ((size_t)4 * nb + 2 * (size_t)h + 8) * sizeof(int);
+    carry = (size_t)2 * nb * w * kViews * slot;
+    flags = ((size_t)2 * nb + (size_t)h + 8) * sizeof(int);
     total = 2 * cost + 2 * sum + carry + flags + 4 * 256;
   }
 };
@@ -984,8 +1023,8 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.disp[1] = v.disp_r;
   a.carry = carry;
   a.progress = flags;
-  a.row_done = flags + 4 * F.nb;
-  a.ticket = flags + 4 * F.nb + 2 * h;
+  a.row_done = flags + 2 * F.nb;
+  a.ticket = flags + 2 * F.nb + h;
   a.error = a.ticket + 1;
   *error_flag = a.error;
   a.reasons = v.reasons;
@@ -994,7 +1033,6 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.W = w;
   a.H = h;
   a.D = p.disparities;
-  a.Dp = F.Dp;
   a.nb = F.nb;
   a.Hp = F.nb * F.rows;
   a.split = F.rows * ((F.nb + 1) / 2);
@@ -1004,25 +1042,24 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.min_disparity = p.min_disparity;
   a.rx = p.window_x / 2;
   a.ry = p.window_y / 2;
-  a.chunk = F.K;
   a.uniqueness = p.uniqueness;
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
-  const int regs = F.Dp / 64;
+  const int regs = F.Dp / (2 * kLanes);
   const bool eight = p.directions == 8;
   ctx.prof->kernel_begin();
   switch (regs * 2 + (eight ? 1 : 0)) {
-#define CSGM_SWEEP_CASE(R_, NP_)                                                             \
-  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                         \
-    e = launch_sweep<R_, NP_, chunk_for(R_), ring_for(R_), rows_for(R_)>(a, ctx.stream);          \
+#define CSGM_SWEEP_CASE(R_, NP_)                                                            \
+  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                        \
+    e = launch_sweep<R_, NP_, chunk_for(R_), ring_for(R_), rows_for(R_)>(a, ctx.stream);    \
     break;
-    CSGM_SWEEP_CASE(1, 2)
-    CSGM_SWEEP_CASE(1, 4)
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)
-    CSGM_SWEEP_CASE(3, 2)
-    CSGM_SWEEP_CASE(3, 4)
     CSGM_SWEEP_CASE(4, 2)
     CSGM_SWEEP_CASE(4, 4)
+    CSGM_SWEEP_CASE(6, 2)
+    CSGM_SWEEP_CASE(6, 4)
+    CSGM_SWEEP_CASE(8, 2)
+    CSGM_SWEEP_CASE(8, 4)
 #undef CSGM_SWEEP_CASE
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
