@@ -17,9 +17,12 @@
 //    next row through a shared-memory ring; the (1,0) state stays in registers.  The last row of
 //    a CTA also writes a global carry row that the next CTA of the stream reads
 //    (release/acquire progress counter).
-//  * Meet in the middle: for rows above `split` the down stream runs first and stores its partial
-//    aggregate (uint16); the up stream adds its four paths and selects the winner in registers.
-//    Below `split` the roles swap.  The partial aggregate crosses HBM once each way.
+//  * Each stream stores its partial aggregate (uint16, 4 paths); the down stream marks cells whose
+//    cost is invalid with 0xffff (a valid 4-path partial sum stays below 0x8000).  The streams
+//    never wait for each other.
+//  * wta_kernel streams both partial aggregates through shared memory (bulk copies), adds them
+//    and runs winner-take-all, uniqueness and the parabolic sub-pixel step with one thread per
+//    pixel.
 //  * Disparities live in registers as packed uint16 pairs (REGS registers per lane per path,
 //    16 lanes per view-row); the min-plus step uses the DPX instructions __vimin3_u16x2 /
 //    __viaddmin_u16x2, and the per-row minima of two paths share one 16-lane shuffle butterfly
@@ -38,7 +41,6 @@ namespace csgm {
 
 namespace {
 
-constexpr int kRecords = 16;  // selections buffered per view-row before the scalar select
 
 __host__ __device__ inline int padded_d(int D) { return (D + 63) / 64 * 64; }
 
@@ -92,14 +94,15 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 }
 
 // Bounded waits.  `error` short-circuits every later wait unless `shortcut` is false (the final
-// drain, which must see its copies land).
+// drain, which must see its copies land).  A wait that runs out stores `code` (the wait site:
+// 1 sweep cost chunk, 2 carry progress, 3 carry chunk, 4 selection tile, 5 drain).
 __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
-                                         long long limit, bool shortcut = true) {
+                                         long long limit, int code, bool shortcut = true) {
   long long start = clock64();
   while (!mbar_test(bar, parity)) {
     if (shortcut && *(volatile int*)error) break;
     if (clock64() - start > limit) {
-      atomicExch(error, 1);
+      atomicExch(error, code);
       break;
     }
   }
@@ -295,18 +298,12 @@ struct SweepArgs {
   const uint8_t* cost[2];  // [H][W][Dp] per view
   const uint8_t* gray[2];  // matching-view image per view
   const uint8_t* tex[2];   // matching-view texture per view
-  uint16_t* sum[2];        // partial aggregate [H][W][Dp] per view
-  float* disp[2];
-  uint8_t* carry;     // [2 streams][nb][W][2 views][slot] bytes
-  int* progress;      // [2][nb]
-  int* row_done;      // [H]
+  uint16_t* sum[2][2];     // [stream][view] partial aggregate [H][W][Dp]
+  uint8_t* carry;          // [2 streams][nb][W][2 views][slot] bytes
+  int* progress;           // [2][nb]
   int* ticket;
   int* error;
-  uint8_t* reasons;   // left view only
-  uint8_t* boundary;  // left view only
-  DeviceStats* stats; // left view only
-  int W, H, D, nb, Hp, split, p1, p2, edge_scale, min_disparity, rx, ry;
-  double uniqueness;
+  int W, H, D, nb, Hp, p1, p2, edge_scale;
   long long timeout;
 };
 
@@ -314,19 +311,18 @@ constexpr int kViews = 2;   // views per warp
 constexpr int kLanes = 16;  // lanes per view-row
 
 // Shared-memory layout (byte offsets), compile-time for a kernel instance.
-template <int REGS, int K, int RING, int R>
+template <int REGS, int K, int R>
 struct SweepLayout {
+  static constexpr int RING = 4;                           // ring slots between consecutive rows
   static constexpr int Dp = 2 * kLanes * REGS;
   static constexpr int slot = 3 * Dp * 2 + 16;             // 3 paths x Dp uint16 + 4 minima
   static constexpr int vslot = kViews * slot;              // both views of one pixel
   static constexpr int lut = 0;                            // 256 x uint32
-  static constexpr int bars = lut + 256 * 4;               // R x 4 + 4 mbarriers
-  static constexpr int cost = (bars + (R * 4 + 4) * 8 + 127) / 128 * 128;
-  static constexpr int sum = cost + R * kViews * 2 * K * Dp;        // cost chunks per warp
-  static constexpr int ring = sum + R * kViews * 2 * K * Dp * 2;    // aggregate chunks per warp
+  static constexpr int bars = lut + 256 * 4;               // R x 2 + 4 mbarriers
+  static constexpr int cost = (bars + (R * 2 + 4) * 8 + 127) / 128 * 128;
+  static constexpr int ring = cost + R * kViews * 2 * K * Dp;       // cost chunks per warp
   static constexpr int carry = ring + R * RING * vslot;             // row-to-row rings
-  static constexpr int rec = carry + 4 * K * vslot;                 // carry chunks (4 in flight)
-  static constexpr int total = rec + R * kViews * kRecords * 6 * 4; // winners records
+  static constexpr int total = carry + 4 * K * vslot;               // carry chunks (4 in flight)
 };
 
 // The (P2' - P1) table of StereoCost.pathP2 for every |gray difference|, replicated to u16x2.
@@ -348,13 +344,6 @@ __device__ __forceinline__ uint32_t row_min2(uint32_t packed) {
   for (int o = kLanes / 2; o > 0; o >>= 1)
     packed = __vminu2(packed, __shfl_xor_sync(0xffffffffu, packed, o));
   return packed;
-}
-
-// Minimum of a 32-bit value over each view-row (lanes 0-15 and 16-31 separately).
-__device__ __forceinline__ uint32_t row_min_u32(uint32_t x, int v) {
-  const uint32_t m0 = __reduce_min_sync(0xffffffffu, v == 0 ? x : 0xffffffffu);
-  const uint32_t m1 = __reduce_min_sync(0xffffffffu, v == 1 ? x : 0xffffffffu);
-  return v ? m1 : m0;
 }
 
 // All paths of one pixel (each lane: its view's 2*REGS disparities), phase by phase so the
@@ -454,123 +443,13 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// Scalar selection of one buffered winners record (CensusSgm.java:471-513 semantics).
-__device__ void select_record(const SweepArgs& a, int view, const int32_t* r, int64_t p,
-                              unsigned (&counts)[6]) {
-  const int best = r[0], value = r[1], second = r[2], before = r[3], after = r[4], flags = r[5];
-  float out = __int_as_float(0x7fc00000);
-  uint8_t* reasons = view == 0 ? a.reasons : nullptr;
-  uint8_t* boundary = view == 0 ? a.boundary : nullptr;
-  const bool count = view == 0;
-  if (best >= 0) {
-    const bool full = flags == 3;
-    bool done = false;
-    if (full) {
-      counts[1] += count;
-      if (boundary) boundary[p] = 4;
-    }
-    if (best == 0 || best == a.D - 1) {
-      counts[2] += count;
-      if (reasons) reasons[p] = 2;
-      if (full && best == 0) {
-        counts[0] += count;
-        if (boundary) boundary[p] |= 1;
-      }
-      if (full && best == a.D - 1) {
-        counts[3] += count;
-        if (boundary) boundary[p] |= 2;
-      }
-      done = true;
-    }
-    if (!done && second != INT_MAX) {
-      const double slack = fmax(1.0, __dmul_rn((double)value, a.uniqueness));
-      if ((double)(second - value) <= slack) {
-        counts[4] += count;
-        if (reasons) reasons[p] = 3;
-        done = true;
-      }
-    }
-    if (!done) {
-      double offset = 0;
-      if (before >= 0 && after >= 0) {
-        const double curvature =
-            __dsub_rn(__dadd_rn((double)before, (double)after), __dmul_rn(2.0, (double)value));
-        if (curvature > 0) {
-          const double o =
-              __ddiv_rn(__dmul_rn(0.5, __dsub_rn((double)before, (double)after)), curvature);
-          offset = fmax(-0.5, fmin(0.5, o));
-        }
-      }
-      out = __double2float_rn(__dadd_rn((double)(a.min_disparity + best), offset));
-      counts[5] += count;
-      if (reasons) reasons[p] = 0;
-    }
-  }
-  a.disp[view][p] = out;
-}
-
-// Winners record of one pixel (GpuStereo.java:758-769 layout) from the lane's aggregate words;
-// every view-row computes its own record.
-template <int REGS>
-__device__ __forceinline__ void winners_record(const uint32_t (&s)[REGS], const uint8_t* cb,
-                                               int lane, int v, int sl, int D, bool in_region,
-                                               int32_t* slot) {
-  const int k0 = sl * 2 * REGS;
-  bool valid[2 * REGS];
-#pragma unroll
-  for (int j = 0; j < 2 * REGS; j++) valid[j] = cb[j] != 0x80;
-  const unsigned b0 = __ballot_sync(0xffffffffu, sl == 0 && valid[0]);
-  const int last = D - 1 - k0;
-  bool fl = false;
-#pragma unroll
-  for (int j = 0; j < 2 * REGS; j++) fl |= (j == last) && valid[j];
-  const unsigned bl = __ballot_sync(0xffffffffu, fl);
-  const unsigned half = v ? 0xffff0000u : 0x0000ffffu;
-  int r0 = -1, r1 = INT_MAX, r2 = INT_MAX, r3 = -1, r4 = -1;
-  const int r5 = ((b0 & half) ? 1 : 0) | ((bl & half) ? 2 : 0);
-  uint32_t key = 0xffffffffu;
-  if (in_region) {
-#pragma unroll
-    for (int j = 0; j < 2 * REGS; j++) {
-      const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
-      if (valid[j]) key = min(key, (sv << 12) | (uint32_t)(k0 + j));
-    }
-  }
-  key = row_min_u32(key, v);
-  const int best = key != 0xffffffffu ? (int)(key & 0xfffu) : -1;
-  uint32_t sec = 0x7fffffffu, bef = 0xffffffffu, aft = 0xffffffffu;
-#pragma unroll
-  for (int j = 0; j < 2 * REGS; j++) {
-    const int k = k0 + j;
-    const uint32_t sv = (s[j / 2] >> (16 * (j & 1))) & 0xffffu;
-    if (valid[j] && abs(k - best) > 1) sec = min(sec, sv);
-    if (valid[j] && k == best - 1) bef = sv;
-    if (valid[j] && k == best + 1) aft = sv;
-  }
-  sec = row_min_u32(sec, v);
-  // The owner lanes of best-1 and best+1 hand their values to the whole view-row.
-  const int own_b = v * kLanes + (best >= 1 ? (best - 1) / (2 * REGS) : 0);
-  const int own_a = v * kLanes + min(kLanes - 1, best >= 0 ? (best + 1) / (2 * REGS) : 0);
-  bef = __shfl_sync(0xffffffffu, bef, own_b);
-  aft = __shfl_sync(0xffffffffu, aft, own_a);
-  if (best >= 0) {
-    r0 = best;
-    r1 = (int)(key >> 12);
-    r2 = (int)sec;
-    r3 = best >= 1 && bef != 0xffffffffu ? (int)bef : -1;
-    r4 = aft != 0xffffffffu ? (int)aft : -1;
-  }
-  if (sl < 6)
-    slot[sl] = sl == 0 ? r0 : sl == 1 ? r1 : sl == 2 ? r2 : sl == 3 ? r3 : sl == 4 ? r4 : r5;
-}
-
-// K: pixels per staged chunk (power of two); RING: ring slots between consecutive rows;
-// R: rows (warps) per CTA.
-template <int REGS, int NPATH, int K, int RING, int R>
-__global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
+// K: pixels per staged chunk (power of two); R: rows (warps) per CTA; MINB: CTAs per SM.
+template <int REGS, int NPATH, int K, int R, int MINB>
+__global__ void __launch_bounds__(R * 32, MINB) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using L = SweepLayout<REGS, K, RING, R>;
+  using L = SweepLayout<REGS, K, R>;
   constexpr int Dp = L::Dp;
+  constexpr int RING = L::RING;
   uint32_t* lut = (uint32_t*)(smem + L::lut);
   uint64_t* bars = (uint64_t*)(smem + L::bars);
   __shared__ int s_ticket;
@@ -581,9 +460,9 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
   if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
   if (lane == 0) {
-    for (int i = 0; i < 4; i++) mbar_init(&bars[w * 4 + i], 1);
+    for (int i = 0; i < 2; i++) mbar_init(&bars[w * 2 + i], 1);
     if (w == 0)
-      for (int i = 0; i < 4; i++) mbar_init(&bars[R * 4 + i], 1);
+      for (int i = 0; i < 4; i++) mbar_init(&bars[R * 2 + i], 1);
   }
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
@@ -595,11 +474,9 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
   const int y = mirror ? a.Hp - 1 - yp : yp;  // image row
   const bool exists = y >= 0 && y < H;
   const long long limit = a.timeout;
-  unsigned counts[6] = {0, 0, 0, 0, 0, 0};
   const int steps = W + 2 * (R - 1);
 
   if (exists) {
-    const bool first = (y < a.split) != mirror;
     const bool has_next = b + 1 < a.nb;
     const int ya = mirror ? y + 1 : y - 1;  // image row of the row above (stream order)
     const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
@@ -608,19 +485,20 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
     const int nchunks = (W + K - 1) / K;
 
-    const uint8_t* gray_row = a.gray[v] + (int64_t)y * W + x0;
-    const uint8_t* tex_row = a.tex[v] + (int64_t)y * W + x0;
-    const uint8_t* gray_up = a.gray[v] + (int64_t)(above_exists ? ya : y) * W + x0;
-    uint16_t* sum_mine = a.sum[v] + (int64_t)y * W * Dp;
-    uint8_t* cost_buf = smem + L::cost + w * kViews * 2 * K * Dp;          // [view][2][K][Dp]
-    uint16_t* sum_buf = (uint16_t*)(smem + L::sum + w * kViews * 2 * K * Dp * 2);
+    const uint8_t* cost_v = v ? a.cost[1] : a.cost[0];
+    const uint8_t* gray_v = v ? a.gray[1] : a.gray[0];
+    const uint8_t* tex_v = v ? a.tex[1] : a.tex[0];
+    uint16_t* sum_v = mirror ? (v ? a.sum[1][1] : a.sum[1][0]) : (v ? a.sum[0][1] : a.sum[0][0]);
+    const uint8_t* gray_row = gray_v + (int64_t)y * W + x0;
+    const uint8_t* tex_row = tex_v + (int64_t)y * W + x0;
+    const uint8_t* gray_up = gray_v + (int64_t)(above_exists ? ya : y) * W + x0;
+    uint16_t* sum_mine = sum_v + (int64_t)y * W * Dp;
+    uint8_t* cost_buf = smem + L::cost + w * kViews * 2 * K * Dp;  // [view][2][K][Dp]
     uint8_t* ring = smem + L::ring + w * RING * L::vslot;
     const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::vslot;
     uint8_t* carry_buf = smem + L::carry;
-    int32_t* rec = (int32_t*)(smem + L::rec) + (w * kViews + v) * kRecords * 6;
-    uint64_t* cost_bar = &bars[w * 4];
-    uint64_t* sum_bar = &bars[w * 4 + 2];
-    uint64_t* carry_bar = &bars[R * 4];
+    uint64_t* cost_bar = &bars[w * 2];
+    uint64_t* carry_bar = &bars[R * 2];
     uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
     const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
     const int* carry_progress = &a.progress[stream * a.nb + b - 1];
@@ -645,24 +523,7 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
               "l"(a.cost[vv] + off), "r"(bytes), "r"(smem_u32(&cost_bar[c & 1]))
               : "memory");
       }
-    };
-    auto issue_sum = [&](int c) {
-      if (lane == 0) {
-        fence_proxy_async_shared();
-        const int64_t off = ((int64_t)y * W + chunk_first(c)) * Dp;
-        const uint32_t bytes = (uint32_t)(chunk_n(c) * Dp * 2);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                         smem_u32(&sum_bar[c & 1])),
-                     "r"(2 * bytes)
-                     : "memory");
-#pragma unroll
-        for (int vv = 0; vv < kViews; vv++)
-          asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-              "[%3];" ::"r"(smem_u32(sum_buf + (vv * 2 + (c & 1)) * K * Dp)),
-              "l"(a.sum[vv] + off), "r"(bytes), "r"(smem_u32(&sum_bar[c & 1]))
-              : "memory");
-      }
+      __syncwarp();  // no lane may spin on the barrier before lane 0 has armed it
     };
     // Carry chunks (stream order) of the row above this CTA in a 4-chunk circular buffer.  At
     // most one chunk is prefetched beyond the last one needed, so the chunk holding pixel xs-1
@@ -685,6 +546,9 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
                   carry_in + (int64_t)carry_issued * K * L::vslot,
                   (uint32_t)(chunk_n(carry_issued) * L::vslot), &carry_bar[carry_issued & 3]);
       }
+      // The other lanes block here instead of spinning on a barrier that lane 0 has not armed
+      // yet (a spinning lane could starve lane 0 under independent thread scheduling).
+      __syncwarp();
       carry_issued++;
     };
 
@@ -696,20 +560,8 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
       pad[j] = (k >= a.D ? 0xffffu : 0u) | (k + 1 >= a.D ? 0xffff0000u : 0u);
     }
     const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
-    const bool region_row = y >= a.ry && y < H - a.ry;
-    const int rx = a.rx;
 
-    // Prologue: first chunks in flight; a finalizing row waits until the other stream has stored
-    // its partial aggregate for the whole row.
     issue_cost(0);
-    if (!first) {
-      if (lane == 0) {
-        wait_flag(&a.row_done[y], 1, a.error, limit);
-        fence_proxy_async_global();
-      }
-      __syncwarp();
-      issue_sum(0);
-    }
     if (use_carry) carry_issue(true);
 
     PathState<REGS> horiz;  // (1,0) path in stream coordinates
@@ -745,24 +597,20 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
         const int need_chunk = min(nchunks - 1, (xs + 1) / K);
         while (carry_ready <= need_chunk) {
           if (carry_issued <= carry_ready) carry_issue(true);
-          wait_bar(&carry_bar[carry_ready & 3], (carry_ready >> 2) & 1, a.error, limit);
+          wait_bar(&carry_bar[carry_ready & 3], (carry_ready >> 2) & 1, a.error, limit, 3);
           carry_ready++;
         }
         carry_issue(false);
       }
-      // Cost / partial-aggregate chunks and the pixel data of the next chunk.
+      // Cost chunk and the pixel data of the next chunk.
       if (off == 0) {
         if (xs > 0) {
           px_cur = px_next;
           px_next = c + 1 < nchunks ? chunk_pixels(c + 1) : 0u;
         }
-        wait_bar(&cost_bar[c & 1], (c >> 1) & 1, a.error, limit);
-        if (!first) wait_bar(&sum_bar[c & 1], (c >> 1) & 1, a.error, limit);
+        wait_bar(&cost_bar[c & 1], (c >> 1) & 1, a.error, limit, 1);
         __syncwarp();
-        if (c + 1 < nchunks) {
-          issue_cost(c + 1);
-          if (!first) issue_sum(c + 1);
-        }
+        if (c + 1 < nchunks) issue_cost(c + 1);
       }
       const int pos = (v * 2 + (c & 1)) * K + (mirror ? n_c - 1 - off : off);
       const int x = x0 + dir * xs;
@@ -782,14 +630,19 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
           zero_state(prev[i + 1]);
         }
       }
-      // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
+      // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512; inv = 0xffff
+      // where the cost is invalid.
       const uint8_t* cb = cost_buf + pos * Dp + sl * 2 * REGS;
-      uint32_t cst[REGS];
+      uint32_t cst[REGS], inv[REGS];
 #pragma unroll
       for (int j = 0; j < REGS; j += 2) {
         const uint32_t word = ((const uint32_t*)cb)[j / 2];
         cst[j] = prmt(word, 0, 0x9180u) & 0x027f027fu;
-        if (j + 1 < REGS) cst[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xb3a2u) & 0x027f027fu;
+        inv[j] = prmt(word, 0, 0x9988u);
+        if (j + 1 < REGS) {
+          cst[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xb3a2u) & 0x027f027fu;
+          inv[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xbbaau);
+        }
       }
       // Gray values for the edge-aware penalties (stream order), this view's row.
       const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes + off);
@@ -805,14 +658,14 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
       for (int i = 0; i < NPATH - 1; i++) q[i + 1] = prev[i + 1].m + lut[abs(g_cur - g_above[i])];
       PathState<REGS> out[NPATH];
       paths_step<REGS, NPATH>(prev, q, p1x2, cst, pad, sl, out);
-      // Partial aggregate of this stream's paths.
+      // Partial aggregate of this stream's paths; the down stream marks invalid costs.
       uint32_t s[REGS];
 #pragma unroll
       for (int j = 0; j < REGS; j++) {
         uint32_t acc = out[0].v[j];
 #pragma unroll
         for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
-        s[j] = acc;
+        s[j] = mirror ? acc : acc | inv[j];
       }
       // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured.
       uint8_t* out_slot = ring + (xs & (RING - 1)) * L::vslot + v * L::slot;
@@ -834,38 +687,16 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
           atomicExch(&a.progress[stream * a.nb + b], xs + 1);
         }
       }
-
-      if (first) {
-        uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
-        if (REGS % 4 == 0) {
+      uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
+      if (REGS % 4 == 0) {
 #pragma unroll
-          for (int j = 0; j < REGS; j += 4)
-            *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
-                                            s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) dst[j] = s[j];
-        }
-        if (xs == W - 1) {  // whole row of partial aggregate stored (both views): publish it
-          __syncwarp();
-          if (lane == 0) {
-            __threadfence();
-            atomicExch(&a.row_done[y], 1);
-          }
-        }
+        for (int j = 0; j < REGS; j += 4)
+          *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
+                                          s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
       } else {
-        const uint32_t* other = (const uint32_t*)(sum_buf + pos * Dp + sl * 2 * REGS);
 #pragma unroll
-        for (int j = 0; j < REGS; j++) s[j] += other[j];
-        const int ri = xs & (kRecords - 1);
-        winners_record<REGS>(s, cb, lane, v, sl, a.D, region_row && x >= rx && x < W - rx,
-                             rec + ri * 6);
-        if (ri == kRecords - 1 || xs == W - 1) {
-          __syncwarp();
-          if (sl <= ri)
-            select_record(a, v, rec + sl * 6, (int64_t)y * W + x0 + dir * (xs - ri + sl), counts);
-          __syncwarp();
-        }
+        for (int j = 0; j < REGS; j += 2)
+          *(uint2*)(dst + j) = make_uint2(s[j], s[j + 1 < REGS ? j + 1 : 0]);
       }
       if (++off == n_c) {
         off = 0;
@@ -877,18 +708,213 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
     // Drain: every bulk copy this warp issued has landed before the CTA's shared memory is
     // released (normally already true; after a timed-out wait this bounds the exit).
     const long long drain = limit / 4;
-    for (int cc = max(0, nchunks - 2); cc < nchunks; cc++) {
-      wait_bar(&cost_bar[cc & 1], (cc >> 1) & 1, a.error, drain, false);
-      if (!first) wait_bar(&sum_bar[cc & 1], (cc >> 1) & 1, a.error, drain, false);
-    }
+    for (int cc = max(0, nchunks - 2); cc < nchunks; cc++)
+      wait_bar(&cost_bar[cc & 1], (cc >> 1) & 1, a.error, drain, 5, false);
     if (use_carry)
       for (int cc = max(0, carry_issued - 4); cc < carry_issued; cc++)
-        if (cc >= carry_ready) wait_bar(&carry_bar[cc & 3], (cc >> 2) & 1, a.error, drain, false);
+        if (cc >= carry_ready) wait_bar(&carry_bar[cc & 3], (cc >> 2) & 1, a.error, drain, 5, false);
   } else {
     // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
     for (int step = 0; step < steps; step++) __syncthreads();
   }
-  // Selection counters of the left view (lanes of the right view hold zeros).
+}
+
+// ---------------------------------------------------------------------------------------------
+// Winner-take-all, uniqueness and sub-pixel selection of both views (CensusSgm.java:460-515).
+// A warp owns a tile of 32 consecutive pixels of one row of one view; lane 0 bulk-copies the
+// tile's two partial aggregates (down, up) into shared memory (double-buffered across tiles) and
+// every lane then selects one pixel.  Lane t reads its pixel's words starting at word t, so the
+// 32 lanes hit 32 different banks although the pixels are Dp words apart.
+struct WtaArgs {
+  const uint16_t* down[2];  // per view; 0xffff = invalid cost
+  const uint16_t* up[2];
+  float* disp[2];
+  uint8_t* reasons;    // left view only
+  uint8_t* boundary;   // left view only
+  DeviceStats* stats;  // left view only
+  int* error;
+  int W, H, D, min_disparity, rx, ry;
+  double uniqueness;
+  long long timeout;
+};
+
+template <int DP>
+struct WtaLayout {
+  static constexpr int warps = DP <= 64 ? 8 : DP <= 128 ? 6 : DP <= 192 ? 4 : 3;
+  static constexpr int tile = 32 * DP * 2;             // bytes of one stream's tile
+  static constexpr int per_warp = 2 * 2 * tile;        // 2 buffers x (down, up)
+  static constexpr int bars = 0;                        // warps x 2 mbarriers
+  static constexpr int tiles = 128;
+  static constexpr int total = tiles + warps * per_warp;
+};
+
+// Selection of one pixel from its winners record (CensusSgm.java:471-513).
+__device__ __forceinline__ void select_pixel_record(int best, int value, int second, int before,
+                                                    int after, int flags, int D, int min_disparity,
+                                                    double uniqueness, float* out,
+                                                    uint8_t* reasons, uint8_t* boundary,
+                                                    unsigned (&counts)[6], bool count) {
+  float result = __int_as_float(0x7fc00000);
+  if (best >= 0) {
+    const bool full = flags == 3;
+    bool done = false;
+    if (full) {
+      counts[1] += count;
+      if (boundary) *boundary = 4;
+    }
+    if (best == 0 || best == D - 1) {
+      counts[2] += count;
+      if (reasons) *reasons = 2;
+      if (full && best == 0) {
+        counts[0] += count;
+        if (boundary) *boundary |= 1;
+      }
+      if (full && best == D - 1) {
+        counts[3] += count;
+        if (boundary) *boundary |= 2;
+      }
+      done = true;
+    }
+    if (!done && second != INT_MAX) {
+      const double slack = fmax(1.0, __dmul_rn((double)value, uniqueness));
+      if ((double)(second - value) <= slack) {
+        counts[4] += count;
+        if (reasons) *reasons = 3;
+        done = true;
+      }
+    }
+    if (!done) {
+      double offset = 0;
+      if (before >= 0 && after >= 0) {
+        const double curvature =
+            __dsub_rn(__dadd_rn((double)before, (double)after), __dmul_rn(2.0, (double)value));
+        if (curvature > 0) {
+          const double o =
+              __ddiv_rn(__dmul_rn(0.5, __dsub_rn((double)before, (double)after)), curvature);
+          offset = fmax(-0.5, fmin(0.5, o));
+        }
+      }
+      result = __double2float_rn(__dadd_rn((double)(min_disparity + best), offset));
+      counts[5] += count;
+      if (reasons) *reasons = 0;
+    }
+  }
+  *out = result;
+}
+
+template <int DP>
+__global__ void __launch_bounds__(WtaLayout<DP>::warps * 32) wta_kernel(const WtaArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = WtaLayout<DP>;
+  constexpr int NW = DP / 2;  // 32-bit words per pixel and stream
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* bars = (uint64_t*)(smem + L::bars) + warp * 2;
+  uint8_t* tiles = smem + L::tiles + warp * L::per_warp;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+
+  const int W = a.W, H = a.H, D = a.D;
+  const int per_row = (W + 31) / 32;
+  const int64_t items = 2LL * H * per_row;  // (view, row, tile)
+  const int64_t stride = (int64_t)gridDim.x * L::warps;
+  int64_t item = (int64_t)blockIdx.x * L::warps + warp;
+  auto decode = [&](int64_t it, int& view, int& y, int& x0) {
+    view = (int)(it / ((int64_t)H * per_row));
+    const int64_t r = it - (int64_t)view * H * per_row;
+    y = (int)(r / per_row);
+    x0 = (int)(r - (int64_t)y * per_row) * 32;
+  };
+  auto issue = [&](int64_t it, int buf) {
+    if (lane == 0) {
+      int view, y, x0;
+      decode(it, view, y, x0);
+      const uint32_t bytes = (uint32_t)(min(32, W - x0) * DP * 2);
+      const int64_t off = ((int64_t)y * W + x0) * DP;
+      fence_proxy_async_shared();
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                       smem_u32(&bars[buf])),
+                   "r"(2 * bytes)
+                   : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(smem_u32(tiles + (buf * 2) * L::tile)),
+          "l"((view ? a.down[1] : a.down[0]) + off), "r"(bytes), "r"(smem_u32(&bars[buf]))
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(smem_u32(tiles + (buf * 2 + 1) * L::tile)),
+          "l"((view ? a.up[1] : a.up[0]) + off), "r"(bytes), "r"(smem_u32(&bars[buf]))
+          : "memory");
+    }
+    __syncwarp();  // no lane may spin on the barrier before lane 0 has armed it
+  };
+
+  unsigned counts[6] = {0, 0, 0, 0, 0, 0};
+  int it = 0;
+  if (item < items) issue(item, 0);
+  for (; item < items; item += stride, it++) {
+    const int buf = it & 1;
+    if (item + stride < items) issue(item + stride, buf ^ 1);
+    wait_bar(&bars[buf], (it >> 1) & 1, a.error, a.timeout, 4);
+    int view, y, x0;
+    decode(item, view, y, x0);
+    const int x = x0 + lane;
+    if (x < W) {
+      const uint32_t* pa = (const uint32_t*)(tiles + (buf * 2) * L::tile) + lane * NW;
+      const uint32_t* pb = (const uint32_t*)(tiles + (buf * 2 + 1) * L::tile) + lane * NW;
+      const uint16_t* ha = (const uint16_t*)pa;
+      const uint16_t* hb = (const uint16_t*)pb;
+      const bool inside = y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx;
+      int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
+      if (inside) {
+        // Pass 1: first strict minimum among valid disparities, as key = total << 8 | k.
+        uint32_t key = 0xffffffffu;
+        int wi = lane;
+        for (int i = 0; i < NW; i++) {
+          const uint32_t wa = pa[wi], wb = pb[wi];
+          const uint32_t bad = prmt(wa, 0, 0xbb99u);  // 0xffff where the cost is invalid
+          const uint32_t tot = ((wa & ~bad) + wb) | bad;
+          const uint32_t k = 2 * wi;
+          key = min(key, min(((tot & 0xffffu) << 8) | k, ((tot >> 8) & 0xffff00u) | (k + 1)));
+          if (++wi == NW) wi = 0;
+        }
+        if ((key >> 8) != 0xffffu) {
+          best = (int)(key & 0xffu);
+          value = (int)(key >> 8);
+          // Pass 2: minimum over valid disparities outside best-1..best+1.
+          uint32_t sec = 0xffffu;
+          wi = lane;
+          for (int i = 0; i < NW; i++) {
+            const uint32_t wa = pa[wi], wb = pb[wi];
+            const uint32_t bad = prmt(wa, 0, 0xbb99u);
+            const uint32_t tot = ((wa & ~bad) + wb) | bad;
+            const int k = 2 * wi;
+            if ((unsigned)(k - best + 1) > 2u) sec = min(sec, tot & 0xffffu);
+            if ((unsigned)(k - best + 2) > 2u) sec = min(sec, tot >> 16);
+            if (++wi == NW) wi = 0;
+          }
+          second = sec == 0xffffu ? INT_MAX : (int)sec;
+          if (best >= 1 && !(ha[best - 1] & 0x8000u)) before = ha[best - 1] + hb[best - 1];
+          if (best + 1 < D && !(ha[best + 1] & 0x8000u)) after = ha[best + 1] + hb[best + 1];
+          flags = (!(ha[0] & 0x8000u) ? 1 : 0) | (!(ha[D - 1] & 0x8000u) ? 2 : 0);
+        }
+      }
+      const int64_t p = (int64_t)y * W + x;
+      select_pixel_record(best, value, second, before, after, flags, D, a.min_disparity,
+                          a.uniqueness, (view ? a.disp[1] : a.disp[0]) + p,
+                          view == 0 && a.reasons ? a.reasons + p : nullptr,
+                          view == 0 && a.boundary ? a.boundary + p : nullptr, counts, view == 0);
+    }
+    __syncwarp();
+  }
+  // Every issued tile was waited for above; after a timed-out wait, give the copy a bounded
+  // second chance to land before the CTA's shared memory is released.
+  for (int j = max(0, it - 2); j < it; j++)
+    wait_bar(&bars[j & 1], (j >> 1) & 1, a.error, a.timeout / 4, 5, false);
   if (a.stats) {
     unsigned long long* dst[6] = {&a.stats->lower_boundary_rejected,
                                   &a.stats->full_interval_pixels, &a.stats->boundary_rejected,
@@ -902,38 +928,47 @@ __global__ void __launch_bounds__(R * 32, 1) sweep_kernel(const SweepArgs a) {
   }
 }
 
-template <int REGS, int NPATH, int K, int RING, int R>
+template <int DP>
+cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
+  using L = WtaLayout<DP>;
+  cudaError_t e =
+      cudaFuncSetAttribute(wta_kernel<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total);
+  if (e != cudaSuccess) return e;
+  const int64_t items = 2LL * a.H * ((a.W + 31) / 32);
+  const int grid = (int)std::min<int64_t>((items + L::warps - 1) / L::warps, sm_count);
+  wta_kernel<DP><<<grid, L::warps * 32, L::total, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int REGS, int NPATH, int K, int R, int MINB>
 cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
-  auto kernel = sweep_kernel<REGS, NPATH, K, RING, R>;
-  const int shared = SweepLayout<REGS, K, RING, R>::total;
+  auto kernel = sweep_kernel<REGS, NPATH, K, R, MINB>;
+  const int shared = SweepLayout<REGS, K, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
   kernel<<<2 * a.nb, R * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
-// Per-register-count configuration: chunk pixels, ring slots, rows per CTA (shared memory fit).
-constexpr int chunk_for(int regs) { return regs >= 8 ? 2 : 4; }
-constexpr int ring_for(int regs) { return regs <= 2 ? 8 : 4; }
-constexpr int rows_for(int regs) { return regs <= 2 ? 16 : 8; }
+// Per-register-count configuration: chunk pixels, rows per CTA, CTAs per SM (shared memory and
+// register fit).
+constexpr int chunk_for(int regs) { return regs >= 6 ? 2 : 4; }
+constexpr int kRows = 8;
+constexpr int minb_for(int regs) { return regs <= 6 ? 2 : 1; }
 
 struct FusedLayout {
   size_t cost, sum, carry, flags, total;
-  int Dp, nb, K, ring, slot, rows;
+  int Dp, nb, slot;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
-    const int regs = Dp / (2 * kLanes);
-    rows = rows_for(regs);
-    nb = (h + rows - 1) / rows;
-    K = chunk_for(regs);
-    ring = ring_for(regs);
+    nb = (h + kRows - 1) / kRows;
     slot = 3 * Dp * 2 + 16;
     size_t n = (size_t)w * h;
     cost = n * Dp;
     sum = n * Dp * 2;
     carry = (size_t)2 * nb * w * kViews * slot;
-    flags = ((size_t)2 * nb + (size_t)h + 8) * sizeof(int);
-    total = 2 * cost + 2 * sum + carry + flags + 4 * 256;
+    flags = ((size_t)2 * nb + 8) * sizeof(int);
+    total = 2 * cost + 4 * sum + carry + flags + 6 * 256;
   }
 };
 
@@ -958,10 +993,12 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   if (!cost_l) return status;
   uint8_t* cost_r = (uint8_t*)ctx.ws->get(kCostR, F.cost, &status);
   if (!cost_r) return status;
-  uint16_t* sum_l = (uint16_t*)ctx.ws->get(kSum, F.sum, &status);
-  if (!sum_l) return status;
-  uint16_t* sum_r = (uint16_t*)ctx.ws->get(kSumR, F.sum, &status);
-  if (!sum_r) return status;
+  uint16_t* sums[4];
+  const int sum_slots[4] = {kSum, kSumR, kSumUp, kSumUpR};
+  for (int i = 0; i < 4; i++) {
+    sums[i] = (uint16_t*)ctx.ws->get(sum_slots[i], F.sum, &status);
+    if (!sums[i]) return status;
+  }
   uint8_t* carry = (uint8_t*)ctx.ws->get(kCarry, F.carry, &status);
   if (!carry) return status;
   int* flags = (int*)ctx.ws->get(kFlags, F.flags, &status);
@@ -1017,40 +1054,31 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.gray[1] = v.gray_r;
   a.tex[0] = v.tex_l;
   a.tex[1] = v.tex_r;
-  a.sum[0] = sum_l;
-  a.sum[1] = sum_r;
-  a.disp[0] = v.disp_l;
-  a.disp[1] = v.disp_r;
+  a.sum[0][0] = sums[0];
+  a.sum[0][1] = sums[1];
+  a.sum[1][0] = sums[2];
+  a.sum[1][1] = sums[3];
   a.carry = carry;
   a.progress = flags;
-  a.row_done = flags + 2 * F.nb;
-  a.ticket = flags + 2 * F.nb + h;
+  a.ticket = flags + 2 * F.nb;
   a.error = a.ticket + 1;
   *error_flag = a.error;
-  a.reasons = v.reasons;
-  a.boundary = v.boundary;
-  a.stats = v.stats;
   a.W = w;
   a.H = h;
   a.D = p.disparities;
   a.nb = F.nb;
-  a.Hp = F.nb * F.rows;
-  a.split = F.rows * ((F.nb + 1) / 2);
+  a.Hp = F.nb * kRows;
   a.p1 = p.p1;
   a.p2 = p.p2;
   a.edge_scale = p.edge_scale;
-  a.min_disparity = p.min_disparity;
-  a.rx = p.window_x / 2;
-  a.ry = p.window_y / 2;
-  a.uniqueness = p.uniqueness;
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
   const int regs = F.Dp / (2 * kLanes);
   const bool eight = p.directions == 8;
   ctx.prof->kernel_begin();
   switch (regs * 2 + (eight ? 1 : 0)) {
-#define CSGM_SWEEP_CASE(R_, NP_)                                                            \
-  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                        \
-    e = launch_sweep<R_, NP_, chunk_for(R_), ring_for(R_), rows_for(R_)>(a, ctx.stream);    \
+#define CSGM_SWEEP_CASE(R_, NP_)                                                             \
+  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                         \
+    e = launch_sweep<R_, NP_, chunk_for(R_), kRows, minb_for(R_)>(a, ctx.stream);           \
     break;
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)
@@ -1065,6 +1093,36 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   }
   if (e != cudaSuccess) return cuda_fail(e, "sweep kernel launch");
   ctx.prof->kernel_end("sweep");
+
+  WtaArgs t{};
+  t.down[0] = sums[0];
+  t.down[1] = sums[1];
+  t.up[0] = sums[2];
+  t.up[1] = sums[3];
+  t.disp[0] = v.disp_l;
+  t.disp[1] = v.disp_r;
+  t.reasons = v.reasons;
+  t.boundary = v.boundary;
+  t.stats = v.stats;
+  t.error = a.error;
+  t.W = w;
+  t.H = h;
+  t.D = p.disparities;
+  t.min_disparity = p.min_disparity;
+  t.rx = p.window_x / 2;
+  t.ry = p.window_y / 2;
+  t.uniqueness = p.uniqueness;
+  t.timeout = a.timeout;
+  ctx.prof->kernel_begin();
+  switch (F.Dp) {
+    case 64: e = launch_wta<64>(t, ctx.sm_count, ctx.stream); break;
+    case 128: e = launch_wta<128>(t, ctx.sm_count, ctx.stream); break;
+    case 192: e = launch_wta<192>(t, ctx.sm_count, ctx.stream); break;
+    case 256: e = launch_wta<256>(t, ctx.sm_count, ctx.stream); break;
+    default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "wta kernel launch");
+  ctx.prof->kernel_end("wta");
   return CSGM_OK;
 }
 
