@@ -127,19 +127,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# Bytes per cell (pixel x disparity of one pair) of the pair-level roofline model: a uint8 cost
+# volume written once and read by both sweeps of both views, and per view a partial aggregate
+# written by one sweep and read by the other: 1 + 2 * (2 + 2 * Sb) = 5 + 4 * Sb.
+def pair_model_bytes_per_cell(prm) -> int:
+    return 5 + 4 * prm.aggregate_bytes
+
+
 def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int):
-    """Algorithmic HBM bytes of one launch of `kernel` (the per-cell figures of the roofline
-    model: uint8 cost volume written once, read once per sweep; the partial aggregate written by
-    one sweep and read by the other).  None for kernels outside the model."""
+    """Algorithmic HBM bytes of one launch of `kernel`, from the bytes each kernel must move per
+    cell (uint8 costs, Sb-byte partial aggregates, both views).  None for per-pixel kernels."""
     cells = w * h * prm.disparities
     sb = prm.aggregate_bytes
     table = {
-        "cost_volume": 1,                 # one view's uint8 cost volume, written once
-        "paths_line": 1 + 2 * sb,         # one direction: cost read + aggregate read-modify-write
-        "winners": 1 + sb,                # cost validity + aggregate read
-        "sweep_down": 2 * (1 + sb),       # both views: cost read + partial aggregate write
-        "sweep_up": 2 * (1 + sb),         # both views: cost read + partial aggregate read
         "cost_pair": 2,                   # both views' uint8 cost volumes, written once
+        "sweep": 4 * (1 + sb),            # 2 streams x 2 views: cost read + partial aggregate write
+        "wta": 4 * sb,                    # 2 views x (down, up) partial aggregates read
+        "cost_volume": 1,                 # general path: one view's uint8 cost volume
+        "paths_line": 1 + 2 * sb,         # general path: cost read + aggregate read-modify-write
+        "winners": 1 + sb,                # general path: cost validity + aggregate read
     }
     if kernel not in table:
         return None
@@ -339,7 +345,10 @@ def run_ours(args):
                         "traffic": read_traffic(args.workload, name),
                         "algorithmic_bytes_per_launch": per_launch,
                         "avg_launch_ms": round(total_ns / count / 1e6, 4),
-                        "share": round(total_ns / max(1, sum(v[1] for v in kernels.values())), 3)}
+                        "share": round(total_ns / max(1, sum(v[1] for v in kernels.values())), 3),
+                        "pair_model_frac": round(
+                            pair_model_bytes_per_cell(prm) * cells / (ms_per_step / 1e3) / 1e9
+                            / peak, 4)}
 
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
