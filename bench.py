@@ -45,6 +45,10 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfg1")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-pairs", type=int, default=0,
+                    help="run this many pairs through GpuSgm.pair and exit (an ncu target)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="with --profile-pairs: use the top ROWS rows of the workload's pair")
     return ap.parse_args()
 
 
@@ -385,8 +389,33 @@ def run_ours(args):
     return 0
 
 
+def run_profile_pairs(args):
+    """Plain pairs through the public API, no timing: the program that ncu captures run."""
+    import numpy as np
+
+    from pose_b200.sgm import GpuSgm
+    from pose_b200.synthetic import make_pair, spec_for
+
+    prm = workload_params(args.workload)
+    spec = spec_for(WORKLOADS[args.workload]["spec"])
+    left, right, _ = make_pair(spec)
+    w, h = spec.width, spec.height
+    if args.rows:
+        h = min(h, args.rows)
+        left = np.ascontiguousarray(left.reshape(-1, w)[:h]).reshape(-1)
+        right = np.ascontiguousarray(right.reshape(-1, w)[:h]).reshape(-1)
+    session = GpuSgm(0)
+    for _ in range(args.profile_pairs):
+        r = session.pair(prm, left, right, w, h)
+    session.close()
+    print(f"ok {w}x{h} {args.workload}: {r.stats.csv()}", flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.profile_pairs:
+        return run_profile_pairs(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
