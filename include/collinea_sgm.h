@@ -244,6 +244,25 @@ int csgm_pair_device(csgm_session* session, const csgm_params* params, const uin
                      int32_t w, int32_t h, float* lr_checked, float* disp_l, float* disp_r,
                      uint8_t* reasons, uint8_t* boundary, csgm_stats* stats, int32_t sync);
 
+/*
+ * Left-right check that allocates nothing; no counterpart in the reference, whose check
+ * (src/main/java/sgm/CensusSgm.java:181-201) always runs inside the matcher.  Same results as the
+ * check inside csgm_pair: lr_checked[p] keeps disp_l[p] where the right view agrees within
+ * lr_threshold, else NaN; reasons[p] (optional) becomes 4 where a pixel is rejected or its match
+ * leaves the window interior; *lr_rejected (optional) receives the rejected count.
+ *   disp_l, disp_r, lr_checked, reasons, lr_rejected : DEVICE pointers on the current device
+ *   stream : cudaStream_t to queue on (NULL = default stream); the call returns after queueing
+ * For callers that cannot let the library allocate device memory: the only scratch is a fixed
+ * array in the library's static device memory, sized for h <= 16384 rows (larger heights are
+ * rejected with CSGM_E_INVALID).  The first call on a device looks the array up; make that first
+ * call before any stream capture.  Calls whose work overlaps in time on one device share the
+ * scratch and must be serialised by the caller.
+ */
+int csgm_lr_check_noalloc(const float* disp_l, const float* disp_r, int32_t w, int32_t h,
+                          int32_t window_x, int32_t window_y, double lr_threshold,
+                          float* lr_checked, uint8_t* reasons, unsigned long long* lr_rejected,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

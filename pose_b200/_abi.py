@@ -160,6 +160,9 @@ SIGNATURES = {
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
          ctypes.POINTER(CsgmStats)],
+    ),    "csgm_lr_check_noalloc": (
+        ctypes.c_int,
+        [_P, _P, _I32, _I32, _I32, _I32, ctypes.c_double, _P, _P, _P, _P],
     ),
 }
 
