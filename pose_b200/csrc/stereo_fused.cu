@@ -95,7 +95,8 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 
 // Bounded waits.  `error` short-circuits every later wait unless `shortcut` is false (the final
 // drain, which must see its copies land).  A wait that runs out stores `code` (the wait site:
-// 1 sweep cost chunk, 2 carry progress, 3 carry chunk, 4 selection tile, 5 drain).
+// 1 sweep cost chunk, 3 carry chunk, 4 selection tile, 5 drain; the sweep's producer warp
+// stores 6 when it made no progress for the limit).
 __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
                                          long long limit, int code, bool shortcut = true) {
   long long start = clock64();
@@ -106,20 +107,6 @@ __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* er
       break;
     }
   }
-}
-
-__device__ __forceinline__ void wait_flag(const int* flag, int target, int* error,
-                                          long long limit) {
-  long long start = clock64();
-  while (*(volatile const int*)flag < target) {
-    if (*(volatile int*)error) break;
-    if (clock64() - start > limit) {
-      atomicExch(error, 2);
-      break;
-    }
-    __nanosleep(64);
-  }
-  __threadfence();  // acquire: later reads see what the producer wrote before its release
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -313,16 +300,19 @@ constexpr int kLanes = 16;  // lanes per view-row
 // Shared-memory layout (byte offsets), compile-time for a kernel instance.
 template <int REGS, int K, int R>
 struct SweepLayout {
-  static constexpr int RING = 4;                           // ring slots between consecutive rows
+  static constexpr int RING = 4;  // ring slots between consecutive rows
+  static constexpr int NB = 4;    // cost chunk slots per row warp
+  static constexpr int CS = 4;    // carry chunk slots
   static constexpr int Dp = 2 * kLanes * REGS;
   static constexpr int slot = 3 * Dp * 2 + 16;             // 3 paths x Dp uint16 + 4 minima
   static constexpr int vslot = kViews * slot;              // both views of one pixel
   static constexpr int lut = 0;                            // 256 x uint32
-  static constexpr int bars = lut + 256 * 4;               // R x 2 + 4 mbarriers
-  static constexpr int cost = (bars + (R * 2 + 4) * 8 + 127) / 128 * 128;
-  static constexpr int ring = cost + R * kViews * 2 * K * Dp;       // cost chunks per warp
-  static constexpr int carry = ring + R * RING * vslot;             // row-to-row rings
-  static constexpr int total = carry + 4 * K * vslot;               // carry chunks (4 in flight)
+  static constexpr int bars = lut + 256 * 4;               // full[R][NB], carry_full[CS]
+  static constexpr int counters = bars + (R * NB + CS) * 8;  // consumed[R], carry, published
+  static constexpr int cost = (counters + (R + 2) * 4 + 127) / 128 * 128;
+  static constexpr int ring = cost + R * NB * kViews * K * Dp;  // cost slots [R][NB][view][K][Dp]
+  static constexpr int carry = ring + R * RING * vslot;          // row-to-row rings
+  static constexpr int total = carry + CS * K * vslot;           // carry chunk slots
 };
 
 // The (P2' - P1) table of StereoCost.pathP2 for every |gray difference|, replicated to u16x2.
@@ -332,30 +322,41 @@ __device__ __forceinline__ uint32_t lut_value(int p1, int p2, int scale, int dif
   return d | (d << 16);
 }
 
+__device__ __forceinline__ int ld_acquire_cta(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cta(int* p, int v) {
+  asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// Barrier among the R row warps only (the producer warp does not take part).
+__device__ __forceinline__ void rows_barrier(int threads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+}
+
 template <int REGS>
 struct PathState {
   uint32_t v[REGS];
   uint32_t m;  // replicated minimum
 };
 
-// Minimum over the 16 lanes of each view-row of two packed uint16 values at once.
-__device__ __forceinline__ uint32_t row_min2(uint32_t packed) {
-#pragma unroll
-  for (int o = kLanes / 2; o > 0; o >>= 1)
-    packed = __vminu2(packed, __shfl_xor_sync(0xffffffffu, packed, o));
-  return packed;
-}
-
 // All paths of one pixel (each lane: its view's 2*REGS disparities), phase by phase so the
-// independent per-path latency chains overlap.
+// independent per-path latency chains overlap.  Disparities >= D carry costs >= 0x8000, so they
+// never win a minimum and never wrap (valid path costs stay below 16384 under the uint16 bound).
 //   prev  predecessor path costs (zeros = no predecessor: the result is then the cost itself)
 //   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1x2 = P1 replicated.
 template <int REGS, int NP>
 __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
                                            const uint32_t (&q)[NP], uint32_t p1x2,
-                                           const uint32_t (&c)[REGS], const uint32_t (&pad)[REGS],
-                                           int sl, PathState<REGS> (&out)[NP]) {
-  uint32_t below[NP], above[NP], mm[NP];
+                                           const uint32_t (&c)[REGS], int sl, int view,
+                                           PathState<REGS> (&out)[NP]) {
+  uint32_t below[NP], above[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
     below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1, kLanes);
@@ -370,26 +371,24 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
     for (int j = 0; j < REGS; j++)
       e[j] = __byte_perm(prev[i].v[j], j + 1 < REGS ? prev[i].v[j + 1] : above[i], 0x5432);
     const uint32_t dn0 = __byte_perm(below[i], prev[i].v[0], 0x5432);
-    mm[i] = 0xffffffffu;
+    uint32_t mm = 0xffffffffu;
 #pragma unroll
     for (int j = 0; j < REGS; j++) {
       const uint32_t dn = j == 0 ? dn0 : e[j - 1];
       const uint32_t m3 = __vimin3_u16x2(dn, e[j], q[i]);
       const uint32_t t = __viaddmin_u16x2(m3, p1x2, prev[i].v[j]);
-      const uint32_t L = (t + c[j] - prev[i].m) | pad[j];
+      const uint32_t L = t + c[j] - prev[i].m;
       out[i].v[j] = L;
-      mm[i] = __vminu2(mm[i], L);
+      mm = __vminu2(mm, L);
     }
-  }
-  // Lane minima of two paths packed into one word, then one butterfly per pair of paths.
-#pragma unroll
-  for (int i = 0; i < NP; i += 2) {
-    const uint32_t lo = __vminu2(mm[i], __byte_perm(mm[i], 0, 0x1032)) & 0xffffu;
-    const uint32_t hi = i + 1 < NP ? __vminu2(mm[i + 1], __byte_perm(mm[i + 1], 0, 0x1032)) & 0xffff0000u
-                                   : 0xffff0000u;
-    const uint32_t r = row_min2(lo | hi);
-    out[i].m = (r & 0xffffu) | (r << 16);
-    if (i + 1 < NP) out[i + 1].m = (r >> 16) | (r & 0xffff0000u);
+    // Row minimum of this view: lane minimum, then one full-warp reduction per view with the
+    // other view's lanes contributing ~0 (a reduction over a half-warp member mask measured more
+    // than twice as slow, a 16-lane butterfly about a quarter slower).
+    const uint32_t lm = __vminu2(mm, __byte_perm(mm, 0, 0x1032)) & 0xffffu;
+    const uint32_t r0 = __reduce_min_sync(0xffffffffu, view == 0 ? lm : 0xffffffffu);
+    const uint32_t r1 = __reduce_min_sync(0xffffffffu, view == 1 ? lm : 0xffffffffu);
+    const uint32_t r = view ? r1 : r0;
+    out[i].m = r | (r << 16);
   }
 }
 
@@ -443,279 +442,342 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// K: pixels per staged chunk (power of two); R: rows (warps) per CTA; MINB: CTAs per SM.
+// One CTA = R row warps + 1 producer warp.
+//  * Row warp w holds image row b*R + w (stream order) of both views and processes stream pixel
+//    xs = step - 2w; the row warps meet at a named barrier once per step.  They only wait on
+//    mbarriers of copies the producer issued ahead of time, and tell the producer through
+//    shared-memory counters (release/acquire) which slots they have finished.
+//  * The producer warp (one lane) bulk-copies cost chunks into each row warp's NB slots, fetches
+//    the previous CTA's carry row chunk by chunk once its progress counter covers it, and
+//    publishes this CTA's own carry progress after the last row warp has written a chunk.
+// K: pixels per chunk (power of two); R: row warps; MINB: CTAs per SM.
 template <int REGS, int NPATH, int K, int R, int MINB>
-__global__ void __launch_bounds__(R * 32, MINB) sweep_kernel(const SweepArgs a) {
+__global__ void __launch_bounds__((R + 1) * 32, MINB) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   using L = SweepLayout<REGS, K, R>;
-  constexpr int Dp = L::Dp;
-  constexpr int RING = L::RING;
+  constexpr int Dp = L::Dp, RING = L::RING, NB = L::NB, CS = L::CS;
   uint32_t* lut = (uint32_t*)(smem + L::lut);
-  uint64_t* bars = (uint64_t*)(smem + L::bars);
+  uint64_t* full = (uint64_t*)(smem + L::bars);  // [R][NB]
+  uint64_t* carry_full = full + R * NB;          // [CS]
+  int* consumed = (int*)(smem + L::counters);    // cost chunks finished, per row warp
+  int* carry_consumed = consumed + R;            // carry chunks no longer needed by row warp 0
+  int* published = consumed + R + 1;             // carry chunks written by row warp R-1
+  uint8_t* carry_buf = smem + L::carry;
   __shared__ int s_ticket;
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int v = lane / kLanes, sl = lane % kLanes;  // view and lane within the view-row
   const int W = a.W, H = a.H;
-  if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
-  if (lane == 0) {
-    for (int i = 0; i < 2; i++) mbar_init(&bars[w * 2 + i], 1);
-    if (w == 0)
-      for (int i = 0; i < 4; i++) mbar_init(&bars[R * 2 + i], 1);
+  if (threadIdx.x == 0) {
+    s_ticket = atomicAdd(a.ticket, 1);
+    for (int i = 0; i < R * NB + CS; i++) mbar_init(&full[i], 1);
+    for (int i = 0; i < R + 2; i++) consumed[i] = 0;
   }
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
 
   const int ticket = s_ticket;
   const int stream = ticket & 1, b = ticket >> 1;
   const bool mirror = stream != 0;
-  const int yp = b * R + w;                   // row in stream coordinates
-  const int y = mirror ? a.Hp - 1 - yp : yp;  // image row
-  const bool exists = y >= 0 && y < H;
+  const bool has_next = b + 1 < a.nb;
   const long long limit = a.timeout;
-  const int steps = W + 2 * (R - 1);
+  const int nchunks = (W + K - 1) / K;
+  auto chunk_n = [&](int c) { return min(K, W - c * K); };
+  auto chunk_first = [&](int c) { return mirror ? W - c * K - chunk_n(c) : c * K; };
+  auto row_of = [&](int r) { return mirror ? a.Hp - 1 - (b * R + r) : b * R + r; };
+  const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
 
-  if (exists) {
-    const bool has_next = b + 1 < a.nb;
-    const int ya = mirror ? y + 1 : y - 1;  // image row of the row above (stream order)
-    const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
-    const bool use_carry = w == 0 && b > 0;  // the row above lives in the previous CTA
-    const int dir = mirror ? -1 : 1;
-    const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
-    const int nchunks = (W + K - 1) / K;
-
-    const uint8_t* cost_v = v ? a.cost[1] : a.cost[0];
-    const uint8_t* gray_v = v ? a.gray[1] : a.gray[0];
-    const uint8_t* tex_v = v ? a.tex[1] : a.tex[0];
-    uint16_t* sum_v = mirror ? (v ? a.sum[1][1] : a.sum[1][0]) : (v ? a.sum[0][1] : a.sum[0][0]);
-    const uint8_t* gray_row = gray_v + (int64_t)y * W + x0;
-    const uint8_t* tex_row = tex_v + (int64_t)y * W + x0;
-    const uint8_t* gray_up = gray_v + (int64_t)(above_exists ? ya : y) * W + x0;
-    uint16_t* sum_mine = sum_v + (int64_t)y * W * Dp;
-    uint8_t* cost_buf = smem + L::cost + w * kViews * 2 * K * Dp;  // [view][2][K][Dp]
-    uint8_t* ring = smem + L::ring + w * RING * L::vslot;
-    const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::vslot;
-    uint8_t* carry_buf = smem + L::carry;
-    uint64_t* cost_bar = &bars[w * 2];
-    uint64_t* carry_bar = &bars[R * 2];
-    uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
-    const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
-    const int* carry_progress = &a.progress[stream * a.nb + b - 1];
-
-    // Chunk c of this row in memory order: image columns [first, first + n).
-    auto chunk_n = [&](int c) { return min(K, W - c * K); };
-    auto chunk_first = [&](int c) { return mirror ? W - c * K - chunk_n(c) : c * K; };
-    auto issue_cost = [&](int c) {
-      if (lane == 0) {
-        fence_proxy_async_shared();
-        const int64_t off = ((int64_t)y * W + chunk_first(c)) * Dp;
+  if (w == R) {
+    // ------------------------------------------------------------------ producer warp
+    if (lane != 0) return;
+    int next[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int y = row_of(r);
+      next[r] = (y >= 0 && y < H) ? 0 : nchunks;  // rows beyond the image get no chunks
+    }
+    int next_carry = b > 0 ? 0 : nchunks;
+    int done_pub = has_next ? 0 : nchunks;
+    const int* prev_progress = &a.progress[stream * a.nb + b - 1];
+    int* my_progress = &a.progress[stream * a.nb + b];
+    long long last = clock64();
+    while (true) {
+      bool pending = false, did = false;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int c = next[r];
+        if (c >= nchunks) continue;
+        pending = true;
+        if (c - ld_acquire_cta(&consumed[r]) >= NB) continue;
+        const int64_t off = ((int64_t)row_of(r) * W + chunk_first(c)) * Dp;
         const uint32_t bytes = (uint32_t)(chunk_n(c) * Dp);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                         smem_u32(&cost_bar[c & 1])),
+        uint64_t* bar = &full[r * NB + c % NB];
+        uint8_t* dst = smem + L::cost + ((r * NB + c % NB) * kViews) * K * Dp;
+        fence_proxy_async_shared();
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
                      "r"(2 * bytes)
                      : "memory");
 #pragma unroll
         for (int vv = 0; vv < kViews; vv++)
           asm volatile(
               "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-              "[%3];" ::"r"(smem_u32(cost_buf + (vv * 2 + (c & 1)) * K * Dp)),
-              "l"(a.cost[vv] + off), "r"(bytes), "r"(smem_u32(&cost_bar[c & 1]))
+              "[%3];" ::"r"(smem_u32(dst + vv * K * Dp)),
+              "l"(a.cost[vv] + off), "r"(bytes), "r"(smem_u32(bar))
               : "memory");
+        next[r] = c + 1;
+        did = true;
       }
-      __syncwarp();  // no lane may spin on the barrier before lane 0 has armed it
-    };
-    // Carry chunks (stream order) of the row above this CTA in a 4-chunk circular buffer.  At
-    // most one chunk is prefetched beyond the last one needed, so the chunk holding pixel xs-1
-    // is never overwritten.
-    int carry_issued = 0, carry_ready = 0;
-    auto carry_issue = [&](bool block) {
-      if (carry_issued >= nchunks || carry_issued >= carry_ready + 2) return;
-      const int need = min(W, carry_issued * K + K);
-      if (!block) {
-        int published = 0;
-        if (lane == 0) published = *(volatile const int*)carry_progress;
-        published = __shfl_sync(0xffffffffu, published, 0);
-        if (published < need) return;
+      if (next_carry < nchunks) {
+        pending = true;
+        const int ch = next_carry;
+        if (ch - ld_acquire_cta(carry_consumed) < CS &&
+            ld_acquire_gpu(prev_progress) >= min(W, (ch + 1) * K)) {
+          fence_proxy_async_global();
+          fence_proxy_async_shared();
+          bulk_load(carry_buf + (ch % CS) * K * L::vslot, carry_in + (int64_t)ch * K * L::vslot,
+                    (uint32_t)(chunk_n(ch) * L::vslot), &carry_full[ch % CS]);
+          next_carry = ch + 1;
+          did = true;
+        }
       }
-      if (lane == 0) {
-        wait_flag(carry_progress, need, a.error, limit);
-        fence_proxy_async_global();
-        fence_proxy_async_shared();
-        bulk_load(carry_buf + (carry_issued & 3) * K * L::vslot,
-                  carry_in + (int64_t)carry_issued * K * L::vslot,
-                  (uint32_t)(chunk_n(carry_issued) * L::vslot), &carry_bar[carry_issued & 3]);
+      if (done_pub < nchunks) {
+        pending = true;
+        const int done = ld_acquire_cta(published);
+        if (done > done_pub) {
+          __threadfence();  // the carry rows the row warps wrote are visible GPU-wide first
+          atomicExch(my_progress, min(W, done * K));
+          done_pub = done;
+          did = true;
+        }
       }
-      // The other lanes block here instead of spinning on a barrier that lane 0 has not armed
-      // yet (a spinning lane could starve lane 0 under independent thread scheduling).
-      __syncwarp();
-      carry_issued++;
-    };
+      if (!pending) break;
+      if (did) {
+        last = clock64();
+      } else {
+        if (*(volatile int*)a.error) break;
+        if (clock64() - last > limit) {
+          atomicExch(a.error, 6);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    // Every copy issued above lands before the CTA's shared memory is released (normally all
+    // have landed already; after an error this bounds the exit).
+    const long long drain = limit / 4;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int y = row_of(r);
+      if (y < 0 || y >= H) continue;
+      for (int c = max(0, next[r] - NB); c < next[r]; c++)
+        wait_bar(&full[r * NB + c % NB], (c / NB) & 1, a.error, drain, 5, false);
+    }
+    if (b > 0)
+      for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
+        wait_bar(&carry_full[ch % CS], (ch / CS) & 1, a.error, drain, 5, false);
+    return;
+  }
 
-    // Per-lane padding mask: disparities >= D stay at 0xffff so they never win a minimum.
-    uint32_t pad[REGS];
+  // -------------------------------------------------------------------- row warps
+  const int v = lane / kLanes, sl = lane % kLanes;  // view and lane within the view-row
+  const int yp = b * R + w;                         // row in stream coordinates
+  const int y = row_of(w);
+  const bool exists = y >= 0 && y < H;
+  const int steps = W + 2 * (R - 1);
+  if (!exists) {
+    // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
+    for (int step = 0; step < steps; step++) rows_barrier(R * 32);
+    return;
+  }
+  const int ya = mirror ? y + 1 : y - 1;  // image row of the row above (stream order)
+  const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
+  const bool use_carry = w == 0 && b > 0;  // the row above lives in the previous CTA
+  const bool from_ring = above_exists && w > 0;
+  const bool from_above = from_ring || use_carry;
+  const bool publish = w == R - 1 && has_next;
+  const int dir = mirror ? -1 : 1;
+  const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
+
+  const uint8_t* gray_v = v ? a.gray[1] : a.gray[0];
+  const uint8_t* tex_v = v ? a.tex[1] : a.tex[0];
+  uint16_t* sum_v = mirror ? (v ? a.sum[1][1] : a.sum[1][0]) : (v ? a.sum[0][1] : a.sum[0][0]);
+  const uint8_t* gray_row = gray_v + (int64_t)y * W + x0;
+  const uint8_t* tex_row = tex_v + (int64_t)y * W + x0;
+  const uint8_t* gray_up = gray_v + (int64_t)(above_exists ? ya : y) * W + x0;
+  uint16_t* sum_mine = sum_v + (int64_t)y * W * Dp;
+  const uint8_t* cost_mine = smem + L::cost + (w * NB * kViews + v) * K * Dp;  // + slot * 2*K*Dp
+  uint8_t* ring = smem + L::ring + w * RING * L::vslot + v * L::slot;
+  const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::vslot + v * L::slot;
+  uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot + v * L::slot;
+  const uint8_t* carry_view = carry_buf + v * L::slot;
+
+  // Costs of disparities >= D are lifted from 512 to 0x8000 (see paths_step).
+  uint32_t padadd[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) {
+    const int k = sl * 2 * REGS + 2 * j;
+    padadd[j] = (k >= a.D ? 0x7e00u : 0u) | (k + 1 >= a.D ? 0x7e000000u : 0u);
+  }
+  const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
+
+  // Per-chunk pixel data, lane sl < K of each view-row <-> pixel c*K + sl of that view:
+  // gray | tex << 8 | gray above << 16 | gray above of the next pixel << 24.
+  auto chunk_pixels = [&](int cc) -> uint32_t {
+    const int xs_l = cc * K + sl;
+    uint32_t d = 0;
+    if (sl < K && xs_l < W) {
+      d = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
+      if (above_exists) {
+        d |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
+        if (xs_l + 1 < W) d |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
+      }
+    }
+    return d;
+  };
+  uint32_t px_cur = chunk_pixels(0);
+  uint32_t px_next = nchunks > 1 ? chunk_pixels(1) : 0u;
+
+  PathState<REGS> horiz;  // (1,0) path in stream coordinates
+  zero_state(horiz);
+  // Penalty-table values and texture flag of the pixel about to be processed.
+  uint32_t lutv[NPATH];
+  bool textured;
+  int g_prev, ga_prev;  // gray of the previous pixel, gray above of the previous pixel
+  {
+    const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes);
+    const int g = pxv & 0xff, ga = (pxv >> 16) & 0xff, gr = pxv >> 24;
+    textured = (pxv >> 8) & 1;
+    lutv[0] = lut[g];  // no left neighbour: the value is unused (zero predecessor)
+    if (NPATH > 1) lutv[1 % NPATH] = lut[abs(g - ga)];
+    if (NPATH > 2) lutv[2 % NPATH] = lut[0];
+    if (NPATH > 3) lutv[3 % NPATH] = lut[abs(g - gr)];
+    g_prev = g;
+    ga_prev = ga;
+  }
+  int off = 0, c = 0, n_c = chunk_n(0), carry_ready = 0, carry_rel = 0;
+
+  for (int step = 0; step < steps; step++) {
+    const int xs = step - 2 * w;
+    if (xs < 0 || xs >= W) {
+      rows_barrier(R * 32);
+      continue;
+    }
+    if (use_carry) {
+      const int need_chunk = min(nchunks - 1, (xs + 1) / K);
+      while (carry_ready <= need_chunk) {
+        wait_bar(&carry_full[carry_ready % CS], (carry_ready / CS) & 1, a.error, limit, 3);
+        carry_ready++;
+      }
+    }
+    if (off == 0) wait_bar(&full[w * NB + c % NB], (c / NB) & 1, a.error, limit, 1);
+    const int slot_off = (c % NB) * kViews * K * Dp;
+    const int pos = mirror ? n_c - 1 - off : off;
+    const int x = x0 + dir * xs;
+    // Predecessor states: ring (row above in this CTA) or carry (row above in the previous CTA).
+    PathState<REGS> prev[NPATH];
+    prev[0] = horiz;
+    const int nbr[3] = {xs, xs - 1, xs + 1};
+#pragma unroll
+    for (int i = 0; i < NPATH - 1; i++) {
+      const int xx = nbr[i];
+      if (from_above && xx >= 0 && xx < W) {
+        const uint8_t* src = from_ring ? ring_up + (xx & (RING - 1)) * L::vslot
+                                       : carry_view + (xx & (CS * K - 1)) * L::vslot;
+        load_state<REGS>(src, i, sl, prev[i + 1]);
+      } else {
+        zero_state(prev[i + 1]);
+      }
+    }
+    // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
+    const uint8_t* cb = cost_mine + slot_off + pos * Dp + sl * 2 * REGS;
+    uint32_t cst[REGS], words[REGS / 2];
+#pragma unroll
+    for (int j = 0; j < REGS; j += 2) {
+      words[j / 2] = ((const uint32_t*)cb)[j / 2];
+      cst[j] = (prmt(words[j / 2], 0, 0x9180u) & 0x027f027fu) + padadd[j];
+      cst[j + 1] = (prmt(words[j / 2], 0, 0xb3a2u) & 0x027f027fu) + padadd[j + 1];
+    }
+    uint32_t q[NPATH];
+#pragma unroll
+    for (int i = 0; i < NPATH; i++) q[i] = prev[i].m + lutv[i];
+    PathState<REGS> out[NPATH];
+    paths_step<REGS, NPATH>(prev, q, p1x2, cst, sl, v, out);
+    // Partial aggregate of this stream's paths; the down stream marks invalid costs 0xffff.
+    uint32_t s[REGS];
 #pragma unroll
     for (int j = 0; j < REGS; j++) {
-      const int k = sl * 2 * REGS + 2 * j;
-      pad[j] = (k >= a.D ? 0xffffu : 0u) | (k + 1 >= a.D ? 0xffff0000u : 0u);
-    }
-    const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
-
-    issue_cost(0);
-    if (use_carry) carry_issue(true);
-
-    PathState<REGS> horiz;  // (1,0) path in stream coordinates
-    zero_state(horiz);
-    int g_left = 0, ga_c = 0;
-    int off = 0, c = 0, n_c = chunk_n(0);
-    // Per-chunk pixel data, lane sl < K of each view-row <-> pixel c*K + sl of that view:
-    // gray | tex << 8 | gray above << 16 | gray above of the next pixel << 24.
-    auto chunk_pixels = [&](int cc) -> uint32_t {
-      const int xs_l = cc * K + sl;
-      uint32_t d = 0;
-      if (sl < K && xs_l < W) {
-        d = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
-        if (above_exists) {
-          d |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
-          if (xs_l + 1 < W) d |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
-        }
-      }
-      return d;
-    };
-    uint32_t px_cur = chunk_pixels(0);
-    uint32_t px_next = nchunks > 1 ? chunk_pixels(1) : 0u;
-
-    // Lock step: warp w handles pixel xs = step - 2w; one CTA barrier per step makes the ring
-    // slots of the row above (pixels xs-1, xs, xs+1, written in earlier steps) visible.
-    for (int step = 0; step < steps; step++) {
-      const int xs = step - 2 * w;
-      if (xs < 0 || xs >= W) {
-        __syncthreads();
-        continue;
-      }
-      if (use_carry) {
-        const int need_chunk = min(nchunks - 1, (xs + 1) / K);
-        while (carry_ready <= need_chunk) {
-          if (carry_issued <= carry_ready) carry_issue(true);
-          wait_bar(&carry_bar[carry_ready & 3], (carry_ready >> 2) & 1, a.error, limit, 3);
-          carry_ready++;
-        }
-        carry_issue(false);
-      }
-      // Cost chunk and the pixel data of the next chunk.
-      if (off == 0) {
-        if (xs > 0) {
-          px_cur = px_next;
-          px_next = c + 1 < nchunks ? chunk_pixels(c + 1) : 0u;
-        }
-        wait_bar(&cost_bar[c & 1], (c >> 1) & 1, a.error, limit, 1);
-        __syncwarp();
-        if (c + 1 < nchunks) issue_cost(c + 1);
-      }
-      const int pos = (v * 2 + (c & 1)) * K + (mirror ? n_c - 1 - off : off);
-      const int x = x0 + dir * xs;
-      // Ring inputs first (their latency overlaps the cost conversion below).
-      PathState<REGS> prev[NPATH];
-      prev[0] = horiz;
-      const int nbr[3] = {xs, xs - 1, xs + 1};
-      const bool from_ring = above_exists && w > 0;
+      uint32_t acc = out[0].v[j];
 #pragma unroll
-      for (int i = 0; i < NPATH - 1; i++) {
-        const int xx = nbr[i];
-        if ((from_ring || use_carry) && xx >= 0 && xx < W) {
-          const uint8_t* src = from_ring ? ring_up + (xx & (RING - 1)) * L::vslot
-                                         : carry_buf + (xx & (4 * K - 1)) * L::vslot;
-          load_state<REGS>(src + v * L::slot, i, sl, prev[i + 1]);
-        } else {
-          zero_state(prev[i + 1]);
-        }
-      }
-      // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512; inv = 0xffff
-      // where the cost is invalid.
-      const uint8_t* cb = cost_buf + pos * Dp + sl * 2 * REGS;
-      uint32_t cst[REGS], inv[REGS];
+      for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
+      s[j] = acc;
+    }
+    if (!mirror) {
 #pragma unroll
       for (int j = 0; j < REGS; j += 2) {
-        const uint32_t word = ((const uint32_t*)cb)[j / 2];
-        cst[j] = prmt(word, 0, 0x9180u) & 0x027f027fu;
-        inv[j] = prmt(word, 0, 0x9988u);
-        if (j + 1 < REGS) {
-          cst[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xb3a2u) & 0x027f027fu;
-          inv[j + 1 < REGS ? j + 1 : 0] = prmt(word, 0, 0xbbaau);
-        }
+        s[j] |= prmt(words[j / 2], 0, 0x9988u);
+        s[j + 1] |= prmt(words[j / 2], 0, 0xbbaau);
       }
-      // Gray values for the edge-aware penalties (stream order), this view's row.
-      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes + off);
-      const int g_cur = pxv & 0xff;
-      const bool textured = (pxv >> 8) & 1;
-      const int ga_l = ga_c;
-      ga_c = (pxv >> 16) & 0xff;
-      const int ga_r = pxv >> 24;
-      const int g_above[3] = {ga_c, ga_l, ga_r};
-      uint32_t q[NPATH];
-      q[0] = horiz.m + lut[abs(g_cur - g_left)];
-#pragma unroll
-      for (int i = 0; i < NPATH - 1; i++) q[i + 1] = prev[i + 1].m + lut[abs(g_cur - g_above[i])];
-      PathState<REGS> out[NPATH];
-      paths_step<REGS, NPATH>(prev, q, p1x2, cst, pad, sl, out);
-      // Partial aggregate of this stream's paths; the down stream marks invalid costs.
-      uint32_t s[REGS];
-#pragma unroll
-      for (int j = 0; j < REGS; j++) {
-        uint32_t acc = out[0].v[j];
-#pragma unroll
-        for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
-        s[j] = mirror ? acc : acc | inv[j];
-      }
-      // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured.
-      uint8_t* out_slot = ring + (xs & (RING - 1)) * L::vslot + v * L::slot;
-#pragma unroll
-      for (int i = 0; i < NPATH - 1; i++) {
-        PathState<REGS> o = out[i + 1];
-        if (!textured) zero_state(o);
-        store_state<REGS>(out_slot, i, sl, o);
-        if (w == R - 1 && has_next)
-          store_state<REGS>(carry_out + (int64_t)xs * L::vslot + v * L::slot, i, sl, o);
-      }
-      horiz = out[0];
-      if (!textured) zero_state(horiz);
-      g_left = g_cur;
-      if (w == R - 1 && has_next && ((xs + 1) % K == 0 || xs == W - 1)) {
-        __syncwarp();
-        if (lane == 0) {
-          __threadfence();
-          atomicExch(&a.progress[stream * a.nb + b], xs + 1);
-        }
-      }
-      uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
-      if (REGS % 4 == 0) {
-#pragma unroll
-        for (int j = 0; j < REGS; j += 4)
-          *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
-                                          s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
-      } else {
-#pragma unroll
-        for (int j = 0; j < REGS; j += 2)
-          *(uint2*)(dst + j) = make_uint2(s[j], s[j + 1 < REGS ? j + 1 : 0]);
-      }
-      if (++off == n_c) {
-        off = 0;
-        c++;
-        if (c < nchunks) n_c = chunk_n(c);
-      }
-      __syncthreads();
     }
-    // Drain: every bulk copy this warp issued has landed before the CTA's shared memory is
-    // released (normally already true; after a timed-out wait this bounds the exit).
-    const long long drain = limit / 4;
-    for (int cc = max(0, nchunks - 2); cc < nchunks; cc++)
-      wait_bar(&cost_bar[cc & 1], (cc >> 1) & 1, a.error, drain, 5, false);
-    if (use_carry)
-      for (int cc = max(0, carry_issued - 4); cc < carry_issued; cc++)
-        if (cc >= carry_ready) wait_bar(&carry_bar[cc & 3], (cc >> 2) & 1, a.error, drain, 5, false);
-  } else {
-    // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
-    for (int step = 0; step < steps; step++) __syncthreads();
+    // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured
+    // (the zeroing only runs in warps that hold an untextured pixel).
+    uint8_t* out_slot = ring + (xs & (RING - 1)) * L::vslot;
+    if (!__all_sync(0xffffffffu, textured)) {
+#pragma unroll
+      for (int i = 0; i < NPATH; i++)
+        if (!textured) zero_state(out[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NPATH - 1; i++) {
+      store_state<REGS>(out_slot, i, sl, out[i + 1]);
+      if (publish) store_state<REGS>(carry_out + (int64_t)xs * L::vslot, i, sl, out[i + 1]);
+    }
+    horiz = out[0];
+    uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
+    if (REGS % 4 == 0) {
+#pragma unroll
+      for (int j = 0; j < REGS; j += 4)
+        *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
+                                        s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < REGS; j += 2)
+        *(uint2*)(dst + j) = make_uint2(s[j], s[j + 1 < REGS ? j + 1 : 0]);
+    }
+    // Next pixel's pixel data, penalty-table values and texture flag (off the critical path).
+    if (off + 1 == n_c) {
+      // End of chunk c: hand the slot back, publish carry progress, move to chunk c+1.
+      __syncwarp();
+      if (lane == 0) {
+        st_release_cta(&consumed[w], c + 1);
+        if (publish) st_release_cta(published, c + 1);
+      }
+      off = 0;
+      c++;
+      if (c < nchunks) {
+        n_c = chunk_n(c);
+        px_cur = px_next;
+        px_next = c + 1 < nchunks ? chunk_pixels(c + 1) : 0u;
+      }
+    } else {
+      off++;
+    }
+    if (xs + 1 < W) {
+      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes + off);
+      const int g = pxv & 0xff, ga = (pxv >> 16) & 0xff, gr = pxv >> 24;
+      textured = (pxv >> 8) & 1;
+      lutv[0] = lut[abs(g - g_prev)];
+      if (NPATH > 1) lutv[1 % NPATH] = lut[abs(g - ga)];
+      if (NPATH > 2) lutv[2 % NPATH] = lut[abs(g - ga_prev)];
+      if (NPATH > 3) lutv[3 % NPATH] = lut[abs(g - gr)];
+      g_prev = g;
+      ga_prev = ga;
+    }
+    if (use_carry && xs / K > carry_rel) {
+      carry_rel = xs / K;  // chunks before the one holding pixel xs are no longer needed
+      __syncwarp();
+      if (lane == 0) st_release_cta(carry_consumed, carry_rel);
+    }
+    rows_barrier(R * 32);
   }
 }
 
@@ -946,22 +1008,22 @@ cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
   const int shared = SweepLayout<REGS, K, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
-  kernel<<<2 * a.nb, R * 32, shared, stream>>>(a);
+  kernel<<<2 * a.nb, (R + 1) * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
-// Per-register-count configuration: chunk pixels, rows per CTA, CTAs per SM (shared memory and
-// register fit).
+// Per-register-count configuration: chunk pixels, rows per CTA (shared-memory fit), CTAs per SM.
 constexpr int chunk_for(int regs) { return regs >= 6 ? 2 : 4; }
-constexpr int kRows = 8;
-constexpr int minb_for(int regs) { return regs <= 6 ? 2 : 1; }
+constexpr int rows_for(int regs) { return regs <= 4 ? 16 : 8; }
+constexpr int minb_for(int) { return 1; }
 
 struct FusedLayout {
   size_t cost, sum, carry, flags, total;
-  int Dp, nb, slot;
+  int Dp, nb, slot, rows;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
-    nb = (h + kRows - 1) / kRows;
+    rows = rows_for(Dp / (2 * kLanes));
+    nb = (h + rows - 1) / rows;
     slot = 3 * Dp * 2 + 16;
     size_t n = (size_t)w * h;
     cost = n * Dp;
@@ -1067,7 +1129,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.H = h;
   a.D = p.disparities;
   a.nb = F.nb;
-  a.Hp = F.nb * kRows;
+  a.Hp = F.nb * F.rows;
   a.p1 = p.p1;
   a.p2 = p.p2;
   a.edge_scale = p.edge_scale;
@@ -1078,7 +1140,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   switch (regs * 2 + (eight ? 1 : 0)) {
 #define CSGM_SWEEP_CASE(R_, NP_)                                                             \
   case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                         \
-    e = launch_sweep<R_, NP_, chunk_for(R_), kRows, minb_for(R_)>(a, ctx.stream);           \
+    e = launch_sweep<R_, NP_, chunk_for(R_), rows_for(R_), minb_for(R_)>(a, ctx.stream);     \
     break;
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)
