@@ -180,6 +180,24 @@ def measured_peak_gbs():
 
 
 # ---------------------------------------------------------------------------------------------
+# Multi-GPU: one process per GPU, every rank matches its own pair (replicas, weak scaling).
+def max_over_ranks(seconds: float, dist, device) -> float:
+    """The slowest rank's time: a job of replicas finishes when its last rank does."""
+    if dist is None:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(cells_per_pair: int, steps: int, world: int, seconds: float) -> float:
+    """Whole-job Gcells/s: every rank processed `steps` pairs in at most `seconds`."""
+    return cells_per_pair * steps * world / seconds / 1e9
+
+
+# ---------------------------------------------------------------------------------------------
 def cpu_baseline(prm, left, right, w, h, rows: int, threads: int):
     """The oracle on a bounded band of the workload (full width, `rows` rows)."""
     import numpy as np
@@ -301,12 +319,10 @@ def run_ours(args):
     kernels = session.kernel_times(reset=True)
     device_s = prof["kernel_ns"] / 1e9
     launches = int(prof["launches"])
+    device_s = max_over_ranks(device_s, dist, f"cuda:{local}")
     if dist:
-        t = torch.tensor([device_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        device_s = float(t.item())
         dist.barrier()
-    value = cells * args.steps * world / device_s / 1e9
+    value = replica_throughput(cells, args.steps, world, device_s)
     ms_per_step = device_s / args.steps * 1e3
 
     # End to end through csgm_pair with pinned host buffers.
@@ -328,12 +344,8 @@ def run_ours(args):
     e0 = time.perf_counter()
     for _ in range(args.steps):
         step_host()
-    e2e_s = time.perf_counter() - e0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = cells * args.steps * world / e2e_s / 1e9
+    e2e_s = max_over_ranks(time.perf_counter() - e0, dist, f"cuda:{local}")
+    e2e_value = replica_throughput(cells, args.steps, world, e2e_s)
 
     # Roofline of the dominant kernel (largest share of device time in the timed region).
     roofline = None
