@@ -33,6 +33,8 @@
 //  * CTAs take tickets in launch order; a CTA only waits on lower tickets, so the schedule cannot
 //    deadlock even when not every CTA is resident.
 #include <climits>
+#include <cstdlib>
+#include <type_traits>
 
 #include "stereo_fused.h"
 #include "stereo_kernels.h"
@@ -53,18 +55,6 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                : "memory");
-}
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
-                                          uint64_t* bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
 }
 
 __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
@@ -99,12 +89,16 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 // stores 6 when it made no progress for the limit).
 __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
                                          long long limit, int code, bool shortcut = true) {
-  long long start = clock64();
-  while (!mbar_test(bar, parity)) {
-    if (shortcut && *(volatile int*)error) break;
-    if (clock64() - start > limit) {
-      atomicExch(error, code);
-      break;
+  if (mbar_test(bar, parity)) return;  // the common case: the copy has landed
+  const long long start = clock64();
+  for (unsigned spin = 1;; spin++) {
+    if (mbar_test(bar, parity)) return;
+    if ((spin & 15) == 0) {  // the error flag and the clock only every 16th probe
+      if (shortcut && *(volatile int*)error) return;
+      if (clock64() - start > limit) {
+        atomicExch(error, code);
+        return;
+      }
     }
   }
 }
@@ -281,46 +275,82 @@ __global__ void cost_pair_kernel(CostPairArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Per-pixel penalty records (StereoCost.pathP2, StereoCost.java:44-48), one per stream and pixel
+// in stream order (row yp, pixel xs).  Word i belongs to the stream's path i - (1,0), (0,1),
+// (1,1), (-1,1) in stream coordinates - and holds pathP2 - P1 of the left view in bits 0-14 and
+// of the right view in bits 16-30.  Bits 15 / 31 of word 0 flag a textured left / right pixel.
+// A path without a predecessor gets P2 - P1 (its state is zero, so the value is never used).
+struct PenaltyArgs {
+  const uint8_t* gray[2];
+  const uint8_t* tex[2];
+  uint4* out;  // [2 streams][H][W]
+  int W, H, p1, p2, edge_scale;
+};
+
+__global__ void penalty_kernel(const PenaltyArgs a) {
+  const int xs = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yp = blockIdx.y, s = blockIdx.z;
+  const int W = a.W, H = a.H;
+  if (xs >= W) return;
+  const int step = s ? -1 : 1;  // image offset of one stream step, in x and in y
+  const int x = s ? W - 1 - xs : xs, y = s ? H - 1 - yp : yp;
+  const int px[4] = {x - step, x, x - step, x + step};
+  const int py[4] = {y, y - step, y - step, y - step};
+  uint32_t word[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int v = 0; v < 2; v++) {
+    const uint8_t* g = a.gray[v];
+    const int center = g[(int64_t)y * W + x];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      int value = a.p2;
+      if (px[i] >= 0 && px[i] < W && py[i] >= 0 && py[i] < H)
+        value = path_p2(a.p1, a.p2, a.edge_scale, center, g[(int64_t)py[i] * W + px[i]]);
+      word[i] |= (uint32_t)(value - a.p1) << (16 * v);
+    }
+    if (a.tex[v][(int64_t)y * W + x]) word[0] |= 0x8000u << (16 * v);
+  }
+  a.out[((int64_t)s * H + yp) * W + xs] = make_uint4(word[0], word[1], word[2], word[3]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Aggregation sweep.  Both views of one image row live in one warp: every 32-bit register holds
+// one disparity of the left view (low half) and the same disparity of the right view (high
+// half), lane l owning disparities l*REGS .. l*REGS+REGS-1.  The d-1 / d+1 neighbours of a
+// register are therefore the neighbouring registers (one shuffle per lane edge), and every
+// packed DPX min / add serves both views at once.
 struct SweepArgs {
-  const uint8_t* cost[2];  // [H][W][Dp] per view
-  const uint8_t* gray[2];  // matching-view image per view
-  const uint8_t* tex[2];   // matching-view texture per view
-  uint16_t* sum[2][2];     // [stream][view] partial aggregate [H][W][Dp]
-  uint8_t* carry;          // [2 streams][nb][W][2 views][slot] bytes
-  int* progress;           // [2][nb]
+  const uint8_t* cost[2];  // [H][W][Dp] per view, image order; 0x80 = invalid (512)
+  const uint4* pen;        // [2 streams][H][W] penalty records, stream order
+  uint32_t* sum[2];        // per stream: partial aggregate [H][W][Dp], left | right << 16
+  uint8_t* carry;          // [2 streams][nb][W][vslot] last-row states of each row block
+  int* progress;           // [2][nb] carry pixels published per row block
   int* ticket;
   int* error;
-  int W, H, D, nb, Hp, p1, p2, edge_scale;
+  int W, H, D, nb, p1;
   long long timeout;
 };
 
-constexpr int kViews = 2;   // views per warp
-constexpr int kLanes = 16;  // lanes per view-row
-
-// Shared-memory layout (byte offsets), compile-time for a kernel instance.
-template <int REGS, int K, int R>
+// Shared-memory layout (byte offsets) of one sweep CTA.
+template <int REGS, int NPATH, int K, int R>
 struct SweepLayout {
-  static constexpr int RING = 4;  // ring slots between consecutive rows
-  static constexpr int NB = 4;    // cost chunk slots per row warp
-  static constexpr int CS = 4;    // carry chunk slots
-  static constexpr int Dp = 2 * kLanes * REGS;
-  static constexpr int slot = 3 * Dp * 2 + 16;             // 3 paths x Dp uint16 + 4 minima
-  static constexpr int vslot = kViews * slot;              // both views of one pixel
-  static constexpr int lut = 0;                            // 256 x uint32
-  static constexpr int bars = lut + 256 * 4;               // full[R][NB], carry_full[CS]
-  static constexpr int counters = bars + (R * NB + CS) * 8;  // consumed[R], carry, published
-  static constexpr int cost = (counters + (R + 2) * 4 + 127) / 128 * 128;
-  static constexpr int ring = cost + R * NB * kViews * K * Dp;  // cost slots [R][NB][view][K][Dp]
-  static constexpr int carry = ring + R * RING * vslot;          // row-to-row rings
-  static constexpr int total = carry + CS * K * vslot;           // carry chunk slots
+  static constexpr int Dp = 32 * REGS;
+  static constexpr int NV = NPATH - 1;  // paths whose predecessor lies in the row above
+  static constexpr int RING = 4;        // ring slots between consecutive row warps
+  static constexpr int NB = 4;          // cost chunk slots per row warp
+  static constexpr int CS = 4;          // carry chunk slots
+  // One pixel's vertical path states: NV x Dp u16x2, then the NV packed minima.
+  static constexpr int vslot = NV * Dp * 4 + 16;
+  // One cost chunk: K x Dp cost bytes of the left view, of the right view, K penalty records.
+  static constexpr int cslot = K * (2 * Dp + 16);
+  static constexpr int bars = 0;                            // cost_full[R][NB], carry_full[CS]
+  static constexpr int counters = bars + (R * NB + CS) * 8;  // carry_consumed, published
+  static constexpr int cost = (counters + 16 + 127) / 128 * 128;
+  static constexpr int ring = cost + R * NB * cslot;
+  static constexpr int carry = ring + R * RING * vslot;
+  static constexpr int zero = carry + CS * K * vslot;  // a pixel slot of zeros
+  static constexpr int total = zero + vslot;
 };
-
-// The (P2' - P1) table of StereoCost.pathP2 for every |gray difference|, replicated to u16x2.
-__device__ __forceinline__ uint32_t lut_value(int p1, int p2, int scale, int diff) {
-  int v = scale == 0 ? p2 : max(p1 + 1, (int)(((long long)p2 * scale) / (scale + diff)));
-  uint32_t d = (uint32_t)(v - p1);
-  return d | (d << 16);
-}
 
 __device__ __forceinline__ int ld_acquire_cta(const int* p) {
   int v;
@@ -330,110 +360,82 @@ __device__ __forceinline__ int ld_acquire_cta(const int* p) {
 __device__ __forceinline__ void st_release_cta(int* p, int v) {
   asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
 }
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
   int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
 // Barrier among the R row warps only (the producer warp does not take part).
 __device__ __forceinline__ void rows_barrier(int threads) {
   asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
 }
-
-template <int REGS>
-struct PathState {
-  uint32_t v[REGS];
-  uint32_t m;  // replicated minimum
-};
-
-// All paths of one pixel (each lane: its view's 2*REGS disparities), phase by phase so the
-// independent per-path latency chains overlap.  Disparities >= D carry costs >= 0x8000, so they
-// never win a minimum and never wrap (valid path costs stay below 16384 under the uint16 bound).
-//   prev  predecessor path costs (zeros = no predecessor: the result is then the cost itself)
-//   q     min(prev) + P2' - P1 (replicated), c the pixel's costs, p1x2 = P1 replicated.
-template <int REGS, int NP>
-__device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
-                                           const uint32_t (&q)[NP], uint32_t p1x2,
-                                           const uint32_t (&c)[REGS], int sl, int view,
-                                           PathState<REGS> (&out)[NP]) {
-  uint32_t below[NP], above[NP];
-#pragma unroll
-  for (int i = 0; i < NP; i++) {
-    below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1, kLanes);
-    above[i] = __shfl_down_sync(0xffffffffu, prev[i].v[0], 1, kLanes);
-  }
-#pragma unroll
-  for (int i = 0; i < NP; i++) {
-    if (sl == 0) below[i] = 0xffffffffu;
-    if (sl == kLanes - 1) above[i] = 0xffffffffu;
-    uint32_t e[REGS];
-#pragma unroll
-    for (int j = 0; j < REGS; j++)
-      e[j] = __byte_perm(prev[i].v[j], j + 1 < REGS ? prev[i].v[j + 1] : above[i], 0x5432);
-    const uint32_t dn0 = __byte_perm(below[i], prev[i].v[0], 0x5432);
-    uint32_t mm = 0xffffffffu;
-#pragma unroll
-    for (int j = 0; j < REGS; j++) {
-      const uint32_t dn = j == 0 ? dn0 : e[j - 1];
-      const uint32_t m3 = __vimin3_u16x2(dn, e[j], q[i]);
-      const uint32_t t = __viaddmin_u16x2(m3, p1x2, prev[i].v[j]);
-      const uint32_t L = t + c[j] - prev[i].m;
-      out[i].v[j] = L;
-      mm = __vminu2(mm, L);
-    }
-    // Row minimum of this view: lane minimum, then one full-warp reduction per view with the
-    // other view's lanes contributing ~0 (a reduction over a half-warp member mask measured more
-    // than twice as slow, a 16-lane butterfly about a quarter slower).
-    const uint32_t lm = __vminu2(mm, __byte_perm(mm, 0, 0x1032)) & 0xffffu;
-    const uint32_t r0 = __reduce_min_sync(0xffffffffu, view == 0 ? lm : 0xffffffffu);
-    const uint32_t r1 = __reduce_min_sync(0xffffffffu, view == 1 ? lm : 0xffffffffu);
-    const uint32_t r = view ? r1 : r0;
-    out[i].m = r | (r << 16);
-  }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 
+// REGS consecutive 32-bit words at a 8-byte aligned address (16-byte aligned when REGS % 4 == 0).
 template <int REGS>
-__device__ __forceinline__ void load_state(const uint8_t* slot, int path, int sl,
-                                           PathState<REGS>& s) {
-  constexpr int Dp = 2 * kLanes * REGS;
-  const uint32_t* src = (const uint32_t*)(slot + 2 * (path * Dp + sl * 2 * REGS));
-  if (REGS % 4 == 0) {
+__device__ __forceinline__ void load_words(const void* p, uint32_t (&v)[REGS]) {
+  if constexpr (REGS % 4 == 0) {
 #pragma unroll
     for (int j = 0; j < REGS; j += 4) {
-      const uint4 v = *(const uint4*)(src + j);
-      s.v[j] = v.x;
-      s.v[j + 1 < REGS ? j + 1 : 0] = v.y;
-      s.v[j + 2 < REGS ? j + 2 : 0] = v.z;
-      s.v[j + 3 < REGS ? j + 3 : 0] = v.w;
+      const uint4 t = ((const uint4*)p)[j / 4];
+      v[j] = t.x;
+      v[j + 1] = t.y;
+      v[j + 2] = t.z;
+      v[j + 3] = t.w;
     }
   } else {
 #pragma unroll
     for (int j = 0; j < REGS; j += 2) {
-      const uint2 v = *(const uint2*)(src + j);
-      s.v[j] = v.x;
-      s.v[j + 1 < REGS ? j + 1 : 0] = v.y;
+      const uint2 t = ((const uint2*)p)[j / 2];
+      v[j] = t.x;
+      v[j + 1] = t.y;
     }
   }
-  s.m = ((const uint32_t*)(slot + 6 * Dp))[path];
+}
+template <int REGS>
+__device__ __forceinline__ void store_words(void* p, const uint32_t (&v)[REGS]) {
+  if constexpr (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4)
+      ((uint4*)p)[j / 4] = make_uint4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 2) ((uint2*)p)[j / 2] = make_uint2(v[j], v[j + 1]);
+  }
+}
+// Streaming global store of a partial aggregate (not re-read before the selection kernel).
+template <int REGS>
+__device__ __forceinline__ void store_words_cs(uint32_t* p, const uint32_t (&v)[REGS]) {
+  if constexpr (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4)
+      __stcs((uint4*)p + j / 4, make_uint4(v[j], v[j + 1], v[j + 2], v[j + 3]));
+  } else {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 2) __stcs((uint2*)p + j / 2, make_uint2(v[j], v[j + 1]));
+  }
 }
 
 template <int REGS>
-__device__ __forceinline__ void store_state(uint8_t* slot, int path, int sl,
-                                            const PathState<REGS>& s) {
-  constexpr int Dp = 2 * kLanes * REGS;
-  uint32_t* dst = (uint32_t*)(slot + 2 * (path * Dp + sl * 2 * REGS));
-  if (REGS % 4 == 0) {
-#pragma unroll
-    for (int j = 0; j < REGS; j += 4)
-      *(uint4*)(dst + j) = make_uint4(s.v[j], s.v[j + 1 < REGS ? j + 1 : 0],
-                                      s.v[j + 2 < REGS ? j + 2 : 0], s.v[j + 3 < REGS ? j + 3 : 0]);
-  } else {
-#pragma unroll
-    for (int j = 0; j < REGS; j += 2)
-      *(uint2*)(dst + j) = make_uint2(s.v[j], s.v[j + 1 < REGS ? j + 1 : 0]);
-  }
-  if (sl == 0) ((uint32_t*)(slot + 6 * Dp))[path] = s.m;
-}
+struct PathState {
+  uint32_t v[REGS];
+  uint32_t m;  // packed row minima (left | right << 16)
+};
 
 template <int REGS>
 __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
@@ -442,372 +444,401 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// One CTA = R row warps + 1 producer warp.
-//  * Row warp w holds image row b*R + w (stream order) of both views and processes stream pixel
-//    xs = step - 2w; the row warps meet at a named barrier once per step.  They only wait on
-//    mbarriers of copies the producer issued ahead of time, and tell the producer through
-//    shared-memory counters (release/acquire) which slots they have finished.
-//  * The producer warp (one lane) bulk-copies cost chunks into each row warp's NB slots, fetches
-//    the previous CTA's carry row chunk by chunk once its progress counter covers it, and
-//    publishes this CTA's own carry progress after the last row warp has written a chunk.
-// K: pixels per chunk (power of two); R: row warps; MINB: CTAs per SM.
-template <int REGS, int NPATH, int K, int R, int MINB>
-__global__ void __launch_bounds__((R + 1) * 32, MINB) sweep_kernel(const SweepArgs a) {
+// Path `path` of one pixel slot (vslot layout) for this lane.
+template <int REGS, int NV>
+__device__ __forceinline__ void load_path(const uint8_t* pixel, int path, int lane,
+                                          PathState<REGS>& s) {
+  load_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, s.v);
+  s.m = ((const uint32_t*)(pixel + NV * 32 * REGS * 4))[path];
+}
+template <int REGS, int NV>
+__device__ __forceinline__ void store_path(uint8_t* pixel, int path, int lane,
+                                           const PathState<REGS>& s) {
+  store_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, s.v);
+  if (lane == 0) ((uint32_t*)(pixel + NV * 32 * REGS * 4))[path] = s.m;
+}
+
+// This lane's costs of both views as packed u16 pairs: byte j of each view widened, 0x80 -> 512,
+// and pad[j] ORed in (disparities >= D are lifted to 0x1200 so they never win a minimum).
+template <int REGS>
+__device__ __forceinline__ void widen_costs(const uint8_t* c0, const uint8_t* c1,
+                                            const uint32_t (&pad)[REGS], uint32_t (&c)[REGS]) {
+  constexpr int NW = (REGS + 3) / 4;
+  uint32_t a[NW], b[NW];
+  if constexpr (REGS == 2) {
+    a[0] = *(const uint16_t*)c0;
+    b[0] = *(const uint16_t*)c1;
+  } else if constexpr (REGS == 4) {
+    a[0] = *(const uint32_t*)c0;
+    b[0] = *(const uint32_t*)c1;
+  } else if constexpr (REGS == 6) {
+    const uint16_t* h0 = (const uint16_t*)c0;
+    const uint16_t* h1 = (const uint16_t*)c1;
+    a[0] = (uint32_t)h0[0] | ((uint32_t)h0[1] << 16);
+    a[1] = h0[2];
+    b[0] = (uint32_t)h1[0] | ((uint32_t)h1[1] << 16);
+    b[1] = h1[2];
+  } else {
+    const uint2 t0 = *(const uint2*)c0, t1 = *(const uint2*)c1;
+    a[0] = t0.x;
+    a[1] = t0.y;
+    b[0] = t1.x;
+    b[1] = t1.y;
+  }
+#pragma unroll
+  for (int j = 0; j < REGS; j++) {
+    const uint32_t i = j % 4;
+    // byte i of a, its sign, byte i of b, its sign
+    const uint32_t sel = i | ((i | 8) << 4) | ((4 + i) << 8) | (((4 + i) | 8) << 12);
+    c[j] = (prmt(a[j / 4], b[j / 4], sel) & 0x027f027fu) | pad[j];
+  }
+}
+
+// Lane minimum of REGS packed pairs.
+template <int REGS>
+__device__ __forceinline__ uint32_t lane_min(const uint32_t (&v)[REGS]) {
+  uint32_t m = v[0];
+  int j = 1;
+#pragma unroll
+  for (; j + 1 < REGS; j += 2) m = __vimin3_u16x2(m, v[j], v[j + 1]);
+  if (j < REGS) m = __vminu2(m, v[j]);
+  return m;
+}
+
+// One pixel of every path of the stream (CensusSgm.java:436-457 for both views at once):
+//   L(k) = C(k) + min(Lp(k), Lp(k-1) + P1, Lp(k+1) + P1, minLp + P2') - minLp,
+// q = minLp + P2' - P1 (packed), with the row minimum of the new state for the next pixel.
+// A zero predecessor state (no predecessor, or an untextured one) gives L = C.
+template <int REGS, int NP>
+__device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
+                                           const uint32_t (&q)[NP], uint32_t p1x2,
+                                           const uint32_t (&c)[REGS], uint32_t lo_edge,
+                                           uint32_t hi_edge, PathState<REGS> (&out)[NP]) {
+  uint32_t below[NP], above[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    below[i] = __shfl_up_sync(0xffffffffu, prev[i].v[REGS - 1], 1) | lo_edge;
+    above[i] = __shfl_down_sync(0xffffffffu, prev[i].v[0], 1) | hi_edge;
+  }
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+#pragma unroll
+    for (int j = 0; j < REGS; j++) {
+      const uint32_t dn = j == 0 ? below[i] : prev[i].v[j - 1];
+      const uint32_t up = j == REGS - 1 ? above[i] : prev[i].v[j + 1];
+      const uint32_t t =
+          __viaddmin_u16x2(__vimin3_u16x2(dn, up, q[i]), p1x2, prev[i].v[j]);
+      out[i].v[j] = t + c[j] - prev[i].m;  // t >= minLp in both halves: no borrow
+    }
+    const uint32_t mm = lane_min<REGS>(out[i].v);
+    const uint32_t r0 = __reduce_min_sync(0xffffffffu, mm & 0xffffu);
+    const uint32_t r1 = __reduce_min_sync(0xffffffffu, mm >> 16);
+    out[i].m = __byte_perm(r0, r1, 0x5410);
+  }
+}
+
+// One CTA = R row warps + 1 producer warp, one row block of one stream.
+//  * "down" (stream 0) runs rows top to bottom and pixels left to right and owns the paths whose
+//    predecessor lies above or to the left: (1,0), (0,1), (1,1), (-1,1); "up" (stream 1) is the
+//    same code on the image mirrored in x and y and owns the four opposite paths.
+//  * Row warp w holds stream row b*R + w of both views and processes stream pixel xs at step
+//    xs + 2w; the row warps meet at a named barrier once per step.  The vertical path states of
+//    a pixel reach the next row through a shared-memory ring; the (1,0) state stays in registers.
+//  * Each row warp bulk-copies its own cost chunks (both views + penalty records) NB chunks
+//    ahead; the last row warp also stores its vertical states as the block's carry row.
+//  * The producer warp fetches the previous block's carry row chunk by chunk once its progress
+//    counter covers the chunk, and publishes this block's carry progress (a GPU-scope fence off
+//    the row warps' critical path).
+//  * CTAs take tickets in launch order and only wait on lower tickets, so the schedule cannot
+//    deadlock even when not every CTA is resident.
+template <int REGS, int NPATH, int K, int R>
+__global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using L = SweepLayout<REGS, K, R>;
-  constexpr int Dp = L::Dp, RING = L::RING, NB = L::NB, CS = L::CS;
-  uint32_t* lut = (uint32_t*)(smem + L::lut);
-  uint64_t* full = (uint64_t*)(smem + L::bars);  // [R][NB]
-  uint64_t* carry_full = full + R * NB;          // [CS]
-  int* consumed = (int*)(smem + L::counters);    // cost chunks finished, per row warp
-  int* carry_consumed = consumed + R;            // carry chunks no longer needed by row warp 0
-  int* published = consumed + R + 1;             // carry chunks written by row warp R-1
+  using L = SweepLayout<REGS, NPATH, K, R>;
+  constexpr int Dp = L::Dp, NV = L::NV, RING = L::RING, NB = L::NB, CS = L::CS;
+  uint64_t* full = (uint64_t*)(smem + L::bars);     // [R][NB]
+  uint64_t* carry_full = full + R * NB;             // [CS]
+  int* carry_consumed = (int*)(smem + L::counters);  // carry chunks row warp 0 no longer needs
+  int* published = carry_consumed + 1;              // carry chunks row warp R-1 has written
   uint8_t* carry_buf = smem + L::carry;
   __shared__ int s_ticket;
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int W = a.W, H = a.H;
   if (threadIdx.x == 0) {
     s_ticket = atomicAdd(a.ticket, 1);
     for (int i = 0; i < R * NB + CS; i++) mbar_init(&full[i], 1);
-    for (int i = 0; i < R + 2; i++) consumed[i] = 0;
+    *carry_consumed = 0;
+    *published = 0;
   }
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_value(a.p1, a.p2, a.edge_scale, i);
+  for (int i = threadIdx.x; i < L::vslot / 4; i += blockDim.x) ((uint32_t*)(smem + L::zero))[i] = 0;
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
 
   const int ticket = s_ticket;
   const int stream = ticket & 1, b = ticket >> 1;
   const bool mirror = stream != 0;
+  const int W = a.W, H = a.H;
   const bool has_next = b + 1 < a.nb;
   const long long limit = a.timeout;
+  int* const err = a.error;
   const int nchunks = (W + K - 1) / K;
   auto chunk_n = [&](int c) { return min(K, W - c * K); };
-  auto chunk_first = [&](int c) { return mirror ? W - c * K - chunk_n(c) : c * K; };
-  auto row_of = [&](int r) { return mirror ? a.Hp - 1 - (b * R + r) : b * R + r; };
-  const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
 
   if (w == R) {
     // ------------------------------------------------------------------ producer warp
     if (lane != 0) return;
-    int next[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int y = row_of(r);
-      next[r] = (y >= 0 && y < H) ? 0 : nchunks;  // rows beyond the image get no chunks
-    }
     int next_carry = b > 0 ? 0 : nchunks;
     int done_pub = has_next ? 0 : nchunks;
     const int* prev_progress = &a.progress[stream * a.nb + b - 1];
     int* my_progress = &a.progress[stream * a.nb + b];
+    const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
     long long last = clock64();
-    while (true) {
-      bool pending = false, did = false;
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        const int c = next[r];
-        if (c >= nchunks) continue;
-        pending = true;
-        if (c - ld_acquire_cta(&consumed[r]) >= NB) continue;
-        const int64_t off = ((int64_t)row_of(r) * W + chunk_first(c)) * Dp;
-        const uint32_t bytes = (uint32_t)(chunk_n(c) * Dp);
-        uint64_t* bar = &full[r * NB + c % NB];
-        uint8_t* dst = smem + L::cost + ((r * NB + c % NB) * kViews) * K * Dp;
-        fence_proxy_async_shared();
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                     "r"(2 * bytes)
-                     : "memory");
-#pragma unroll
-        for (int vv = 0; vv < kViews; vv++)
-          asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-              "[%3];" ::"r"(smem_u32(dst + vv * K * Dp)),
-              "l"(a.cost[vv] + off), "r"(bytes), "r"(smem_u32(bar))
-              : "memory");
-        next[r] = c + 1;
-        did = true;
-      }
+    int prev_seen = 0;  // last progress value read from the previous block
+    while (next_carry < nchunks || done_pub < nchunks) {
+      bool did = false;
       if (next_carry < nchunks) {
-        pending = true;
         const int ch = next_carry;
         if (ch - ld_acquire_cta(carry_consumed) < CS &&
-            ld_acquire_gpu(prev_progress) >= min(W, (ch + 1) * K)) {
+            (prev_seen >= min(W, (ch + 1) * K) ||
+             (prev_seen = ld_relaxed_gpu(prev_progress)) >= min(W, (ch + 1) * K))) {
+          fence_acq_rel_gpu();  // the carry data behind the observed progress is visible
           fence_proxy_async_global();
           fence_proxy_async_shared();
-          bulk_load(carry_buf + (ch % CS) * K * L::vslot, carry_in + (int64_t)ch * K * L::vslot,
-                    (uint32_t)(chunk_n(ch) * L::vslot), &carry_full[ch % CS]);
+          uint64_t* bar = &carry_full[ch % CS];
+          const uint32_t bytes = (uint32_t)(chunk_n(ch) * L::vslot);
+          mbar_expect_tx(bar, bytes);
+          bulk_copy(carry_buf + (ch % CS) * K * L::vslot, carry_in + (int64_t)ch * K * L::vslot,
+                    bytes, bar);
           next_carry = ch + 1;
           did = true;
         }
       }
       if (done_pub < nchunks) {
-        pending = true;
         const int done = ld_acquire_cta(published);
         if (done > done_pub) {
-          __threadfence();  // the carry rows the row warps wrote are visible GPU-wide first
+          __threadfence();  // the carry rows the row warp wrote are visible GPU-wide first
           atomicExch(my_progress, min(W, done * K));
           done_pub = done;
           did = true;
         }
       }
-      if (!pending) break;
       if (did) {
         last = clock64();
       } else {
-        if (*(volatile int*)a.error) break;
+        if (*(volatile int*)err) break;
         if (clock64() - last > limit) {
-          atomicExch(a.error, 6);
+          atomicExch(err, 6);
           break;
         }
-        __nanosleep(32);
+        __nanosleep(128);  // a chunk takes K steps of several hundred cycles each
       }
     }
-    // Every copy issued above lands before the CTA's shared memory is released (normally all
-    // have landed already; after an error this bounds the exit).
-    const long long drain = limit / 4;
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int y = row_of(r);
-      if (y < 0 || y >= H) continue;
-      for (int c = max(0, next[r] - NB); c < next[r]; c++)
-        wait_bar(&full[r * NB + c % NB], (c / NB) & 1, a.error, drain, 5, false);
-    }
+    // Every issued carry copy lands before the CTA's shared memory is released.
     if (b > 0)
       for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
-        wait_bar(&carry_full[ch % CS], (ch / CS) & 1, a.error, drain, 5, false);
+        wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, limit / 4, 5, false);
     return;
   }
 
   // -------------------------------------------------------------------- row warps
-  const int v = lane / kLanes, sl = lane % kLanes;  // view and lane within the view-row
-  const int yp = b * R + w;                         // row in stream coordinates
-  const int y = row_of(w);
-  const bool exists = y >= 0 && y < H;
-  const int steps = W + 2 * (R - 1);
-  if (!exists) {
+  const int yp = b * R + w;  // row in stream order
+  if (yp >= H) {
     // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
-    for (int step = 0; step < steps; step++) rows_barrier(R * 32);
+    for (int step = 0; step < W + 2 * (R - 1); step++) rows_barrier(R * 32);
     return;
   }
-  const int ya = mirror ? y + 1 : y - 1;  // image row of the row above (stream order)
-  const bool above_exists = yp >= 1 && ya >= 0 && ya < H;
+  const int y = mirror ? H - 1 - yp : yp;
   const bool use_carry = w == 0 && b > 0;  // the row above lives in the previous CTA
-  const bool from_ring = above_exists && w > 0;
-  const bool from_above = from_ring || use_carry;
   const bool publish = w == R - 1 && has_next;
-  const int dir = mirror ? -1 : 1;
-  const int x0 = mirror ? W - 1 : 0;       // image column of stream pixel 0
+  uint8_t* my_slots = smem + L::cost + w * NB * L::cslot;
+  uint64_t* my_full = full + w * NB;
+  uint8_t* ring_mine = smem + L::ring + w * RING * L::vslot;
+  const uint8_t* zero = smem + L::zero;
+  // Predecessor row: the ring of the warp above, the carry buffer, or (first image row) the zero
+  // slot for every pixel.
+  const uint8_t* up_base = yp == 0     ? zero
+                           : use_carry ? carry_buf
+                                       : smem + L::ring + (w - 1) * RING * L::vslot;
+  const int up_mask = yp == 0 ? 0 : use_carry ? CS * K - 1 : RING - 1;
+  uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
+  const uint8_t* cost_row0 = a.cost[0] + (int64_t)y * W * Dp;
+  const uint8_t* cost_row1 = a.cost[1] + (int64_t)y * W * Dp;
+  const uint4* pen_row = a.pen + ((int64_t)stream * H + yp) * W;
+  // Partial aggregate of stream pixel xs: sum_px + xs * sum_step (this lane's words).
+  uint32_t* sum_px = (stream ? a.sum[1] : a.sum[0]) + ((int64_t)y * W + (mirror ? W - 1 : 0)) * Dp + lane * REGS;
+  const int64_t sum_step = mirror ? -(int64_t)Dp : (int64_t)Dp;
+  // Cost bytes of chunk pixel `off` sit at slot + cost_first + off * cost_step (image order).
+  const int cost_first_full = (mirror ? (K - 1) * Dp : 0) + lane * REGS;
+  const int cost_step = mirror ? -Dp : Dp;
 
-  const uint8_t* gray_v = v ? a.gray[1] : a.gray[0];
-  const uint8_t* tex_v = v ? a.tex[1] : a.tex[0];
-  uint16_t* sum_v = mirror ? (v ? a.sum[1][1] : a.sum[1][0]) : (v ? a.sum[0][1] : a.sum[0][0]);
-  const uint8_t* gray_row = gray_v + (int64_t)y * W + x0;
-  const uint8_t* tex_row = tex_v + (int64_t)y * W + x0;
-  const uint8_t* gray_up = gray_v + (int64_t)(above_exists ? ya : y) * W + x0;
-  uint16_t* sum_mine = sum_v + (int64_t)y * W * Dp;
-  const uint8_t* cost_mine = smem + L::cost + (w * NB * kViews + v) * K * Dp;  // + slot * 2*K*Dp
-  uint8_t* ring = smem + L::ring + w * RING * L::vslot + v * L::slot;
-  const uint8_t* ring_up = smem + L::ring + (w - 1) * RING * L::vslot + v * L::slot;
-  uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot + v * L::slot;
-  const uint8_t* carry_view = carry_buf + v * L::slot;
-
-  // Costs of disparities >= D are lifted from 512 to 0x8000 (see paths_step).
-  uint32_t padadd[REGS];
-#pragma unroll
-  for (int j = 0; j < REGS; j++) {
-    const int k = sl * 2 * REGS + 2 * j;
-    padadd[j] = (k >= a.D ? 0x7e00u : 0u) | (k + 1 >= a.D ? 0x7e000000u : 0u);
-  }
-  const uint32_t p1x2 = (uint32_t)a.p1 | ((uint32_t)a.p1 << 16);
-
-  // Per-chunk pixel data, lane sl < K of each view-row <-> pixel c*K + sl of that view:
-  // gray | tex << 8 | gray above << 16 | gray above of the next pixel << 24.
-  auto chunk_pixels = [&](int cc) -> uint32_t {
-    const int xs_l = cc * K + sl;
-    uint32_t d = 0;
-    if (sl < K && xs_l < W) {
-      d = (uint32_t)__ldg(gray_row + dir * xs_l) | ((uint32_t)(__ldg(tex_row + dir * xs_l) != 0) << 8);
-      if (above_exists) {
-        d |= (uint32_t)__ldg(gray_up + dir * xs_l) << 16;
-        if (xs_l + 1 < W) d |= (uint32_t)__ldg(gray_up + dir * (xs_l + 1)) << 24;
-      }
-    }
-    return d;
+  auto issue_chunk = [&](int c) {  // lane 0
+    const int n = chunk_n(c);
+    const int first = mirror ? W - c * K - n : c * K;  // image column of the chunk's first byte
+    uint8_t* dst = my_slots + (c % NB) * L::cslot;
+    uint64_t* bar = &my_full[c % NB];
+    const uint32_t cb = (uint32_t)(n * Dp);
+    fence_proxy_async_shared();
+    mbar_expect_tx(bar, 2 * cb + 16u * n);
+    bulk_copy(dst, cost_row0 + (int64_t)first * Dp, cb, bar);
+    bulk_copy(dst + K * Dp, cost_row1 + (int64_t)first * Dp, cb, bar);
+    bulk_copy(dst + 2 * K * Dp, pen_row + c * K, 16u * n, bar);
   };
-  uint32_t px_cur = chunk_pixels(0);
-  uint32_t px_next = nchunks > 1 ? chunk_pixels(1) : 0u;
+  int issued = min(NB, nchunks);
+  if (lane == 0)
+    for (int c = 0; c < issued; c++) issue_chunk(c);
+  __syncwarp();
 
-  PathState<REGS> horiz;  // (1,0) path in stream coordinates
+  const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
+  const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
+  uint32_t pad[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
+  const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
+  PathState<REGS> horiz;  // (1,0) in stream coordinates
   zero_state(horiz);
-  // Penalty-table values and texture flag of the pixel about to be processed.
-  uint32_t lutv[NPATH];
-  bool textured;
-  int g_prev, ga_prev;  // gray of the previous pixel, gray above of the previous pixel
-  {
-    const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes);
-    const int g = pxv & 0xff, ga = (pxv >> 16) & 0xff, gr = pxv >> 24;
-    textured = (pxv >> 8) & 1;
-    lutv[0] = lut[g];  // no left neighbour: the value is unused (zero predecessor)
-    if (NPATH > 1) lutv[1 % NPATH] = lut[abs(g - ga)];
-    if (NPATH > 2) lutv[2 % NPATH] = lut[0];
-    if (NPATH > 3) lutv[3 % NPATH] = lut[abs(g - gr)];
-    g_prev = g;
-    ga_prev = ga;
-  }
-  int off = 0, c = 0, n_c = chunk_n(0), carry_ready = 0, carry_rel = 0;
+  int carry_ready = 0;
 
-  for (int step = 0; step < steps; step++) {
-    const int xs = step - 2 * w;
-    if (xs < 0 || xs >= W) {
-      rows_barrier(R * 32);
-      continue;
-    }
-    if (use_carry) {
-      const int need_chunk = min(nchunks - 1, (xs + 1) / K);
-      while (carry_ready <= need_chunk) {
-        wait_bar(&carry_full[carry_ready % CS], (carry_ready / CS) & 1, a.error, limit, 3);
+  // Idle steps before this row starts (the 2-pixel lag behind the row above).
+  for (int step = 0; step < 2 * w; step++) rows_barrier(R * 32);
+
+  // The sweep of one row.  CARRY_IN: the row above is the previous block's carry row (waited for
+  // chunk by chunk); PUBLISH: this row's vertical states are also stored as this block's carry.
+  auto sweep_row = [&](auto carry_tag, auto publish_tag) {
+    constexpr bool CARRY_IN = decltype(carry_tag)::value;
+    constexpr bool PUBLISH = decltype(publish_tag)::value;
+    auto wait_carry = [&](int need) {
+      need = min(need, nchunks - 1);
+      while (carry_ready <= need) {
+        wait_bar(&carry_full[carry_ready % CS], (carry_ready / CS) & 1, err, limit, 3);
         carry_ready++;
       }
-    }
-    if (off == 0) wait_bar(&full[w * NB + c % NB], (c / NB) & 1, a.error, limit, 1);
-    const int slot_off = (c % NB) * kViews * K * Dp;
-    const int pos = mirror ? n_c - 1 - off : off;
-    const int x = x0 + dir * xs;
-    // Predecessor states: ring (row above in this CTA) or carry (row above in the previous CTA).
-    PathState<REGS> prev[NPATH];
-    prev[0] = horiz;
-    const int nbr[3] = {xs, xs - 1, xs + 1};
-#pragma unroll
-    for (int i = 0; i < NPATH - 1; i++) {
-      const int xx = nbr[i];
-      if (from_above && xx >= 0 && xx < W) {
-        const uint8_t* src = from_ring ? ring_up + (xx & (RING - 1)) * L::vslot
-                                       : carry_view + (xx & (CS * K - 1)) * L::vslot;
-        load_state<REGS>(src, i, sl, prev[i + 1]);
-      } else {
-        zero_state(prev[i + 1]);
+    };
+    // One pixel: xs (stream column), off (index in the chunk), costs at cb, penalties at pb.
+    auto pixel = [&](int xs, int off, const uint8_t* cb, const uint4* pb) {
+      uint32_t cst[REGS];
+      widen_costs<REGS>(cb, cb + K * Dp, pad, cst);
+      const uint4 pw = *pb;
+      PathState<REGS> prev[NPATH];
+      prev[0] = horiz;
+      load_path<REGS, NV>(up_base + (xs & up_mask) * L::vslot, 0, lane, prev[1]);
+      if constexpr (NPATH > 2) {
+        const uint8_t* pd = xs > 0 ? up_base + ((xs - 1) & up_mask) * L::vslot : zero;
+        const uint8_t* pa = xs + 1 < W ? up_base + ((xs + 1) & up_mask) * L::vslot : zero;
+        load_path<REGS, NV>(pd, 1, lane, prev[2]);
+        load_path<REGS, NV>(pa, 2, lane, prev[3]);
       }
-    }
-    // Costs: 2*REGS bytes per lane -> REGS packed uint16 pairs, 0x80 -> 512.
-    const uint8_t* cb = cost_mine + slot_off + pos * Dp + sl * 2 * REGS;
-    uint32_t cst[REGS], words[REGS / 2];
-#pragma unroll
-    for (int j = 0; j < REGS; j += 2) {
-      words[j / 2] = ((const uint32_t*)cb)[j / 2];
-      cst[j] = (prmt(words[j / 2], 0, 0x9180u) & 0x027f027fu) + padadd[j];
-      cst[j + 1] = (prmt(words[j / 2], 0, 0xb3a2u) & 0x027f027fu) + padadd[j + 1];
-    }
-    uint32_t q[NPATH];
-#pragma unroll
-    for (int i = 0; i < NPATH; i++) q[i] = prev[i].m + lutv[i];
-    PathState<REGS> out[NPATH];
-    paths_step<REGS, NPATH>(prev, q, p1x2, cst, sl, v, out);
-    // Partial aggregate of this stream's paths; the down stream marks invalid costs 0xffff.
-    uint32_t s[REGS];
-#pragma unroll
-    for (int j = 0; j < REGS; j++) {
-      uint32_t acc = out[0].v[j];
-#pragma unroll
-      for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
-      s[j] = acc;
-    }
-    if (!mirror) {
-#pragma unroll
-      for (int j = 0; j < REGS; j += 2) {
-        s[j] |= prmt(words[j / 2], 0, 0x9988u);
-        s[j + 1] |= prmt(words[j / 2], 0, 0xbbaau);
+      uint32_t q[NPATH];
+      q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
+      q[1] = prev[1].m + pw.y;
+      if constexpr (NPATH > 2) {
+        q[2] = prev[2].m + pw.z;
+        q[3] = prev[3].m + pw.w;
       }
-    }
-    // Outputs for the row below: the three vertical paths, zeros if this pixel is untextured
-    // (the zeroing only runs in warps that hold an untextured pixel).
-    uint8_t* out_slot = ring + (xs & (RING - 1)) * L::vslot;
-    if (!__all_sync(0xffffffffu, textured)) {
+      PathState<REGS> out[NPATH];
+      paths_step<REGS, NPATH>(prev, q, p1x2, cst, lo_edge, hi_edge, out);
+      // Partial aggregate of this stream's paths.
+      uint32_t s[REGS];
 #pragma unroll
-      for (int i = 0; i < NPATH; i++)
-        if (!textured) zero_state(out[i]);
-    }
+      for (int j = 0; j < REGS; j++) {
+        uint32_t acc = out[0].v[j];
 #pragma unroll
-    for (int i = 0; i < NPATH - 1; i++) {
-      store_state<REGS>(out_slot, i, sl, out[i + 1]);
-      if (publish) store_state<REGS>(carry_out + (int64_t)xs * L::vslot, i, sl, out[i + 1]);
-    }
-    horiz = out[0];
-    uint32_t* dst = (uint32_t*)(sum_mine + (int64_t)x * Dp + sl * 2 * REGS);
-    if (REGS % 4 == 0) {
+        for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
+        s[j] = acc;
+      }
+      store_words_cs<REGS>(sum_px + xs * sum_step, s);
+      // Successors of an untextured pixel start afresh (CensusSgm.java:432-433): they see zeros.
+      const uint32_t keep = prmt(pw.x, 0, 0xbb99u);
+      if (keep != 0xffffffffu) {
 #pragma unroll
-      for (int j = 0; j < REGS; j += 4)
-        *(uint4*)(dst + j) = make_uint4(s[j], s[j + 1 < REGS ? j + 1 : 0],
-                                        s[j + 2 < REGS ? j + 2 : 0], s[j + 3 < REGS ? j + 3 : 0]);
-    } else {
+        for (int i = 0; i < NPATH; i++) {
 #pragma unroll
-      for (int j = 0; j < REGS; j += 2)
-        *(uint2*)(dst + j) = make_uint2(s[j], s[j + 1 < REGS ? j + 1 : 0]);
-    }
-    // Next pixel's pixel data, penalty-table values and texture flag (off the critical path).
-    if (off + 1 == n_c) {
-      // End of chunk c: hand the slot back, publish carry progress, move to chunk c+1.
+          for (int j = 0; j < REGS; j++) out[i].v[j] &= keep;
+          out[i].m &= keep;
+        }
+      }
+      uint8_t* o = ring_mine + (xs & (RING - 1)) * L::vslot;
+#pragma unroll
+      for (int i = 0; i < NV; i++) store_path<REGS, NV>(o, i, lane, out[i + 1]);
+      if constexpr (PUBLISH) {
+        uint8_t* g = carry_out + (int64_t)xs * L::vslot;
+#pragma unroll
+        for (int i = 0; i < NV; i++) store_path<REGS, NV>(g, i, lane, out[i + 1]);
+      }
+      horiz = out[0];
+      (void)off;
+    };
+    // End of chunk c: refill its slot NB chunks ahead, report carry progress / release.
+    auto end_chunk = [&](int c) {
       __syncwarp();
       if (lane == 0) {
-        st_release_cta(&consumed[w], c + 1);
-        if (publish) st_release_cta(published, c + 1);
+        if (c + NB < nchunks) issue_chunk(c + NB);
+        if constexpr (PUBLISH) st_release_cta(published, c + 1);
+        if constexpr (CARRY_IN) st_release_cta(carry_consumed, c);
       }
-      off = 0;
-      c++;
-      if (c < nchunks) {
-        n_c = chunk_n(c);
-        px_cur = px_next;
-        px_next = c + 1 < nchunks ? chunk_pixels(c + 1) : 0u;
-      }
-    } else {
-      off++;
-    }
-    if (xs + 1 < W) {
-      const uint32_t pxv = __shfl_sync(0xffffffffu, px_cur, v * kLanes + off);
-      const int g = pxv & 0xff, ga = (pxv >> 16) & 0xff, gr = pxv >> 24;
-      textured = (pxv >> 8) & 1;
-      lutv[0] = lut[abs(g - g_prev)];
-      if (NPATH > 1) lutv[1 % NPATH] = lut[abs(g - ga)];
-      if (NPATH > 2) lutv[2 % NPATH] = lut[abs(g - ga_prev)];
-      if (NPATH > 3) lutv[3 % NPATH] = lut[abs(g - gr)];
-      g_prev = g;
-      ga_prev = ga;
-    }
-    if (use_carry && xs / K > carry_rel) {
-      carry_rel = xs / K;  // chunks before the one holding pixel xs are no longer needed
       __syncwarp();
-      if (lane == 0) st_release_cta(carry_consumed, carry_rel);
+      if (c + NB < nchunks) issued = c + NB + 1;
+    };
+    const int full_chunks = W / K;
+    for (int c = 0; c < full_chunks; c++) {
+      wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
+      if constexpr (CARRY_IN) wait_carry(c);
+      const uint8_t* slot = my_slots + (c % NB) * L::cslot;
+      const uint4* pens = (const uint4*)(slot + 2 * K * Dp);
+#pragma unroll
+      for (int off = 0; off < K; off++) {
+        if constexpr (CARRY_IN) {
+          if (off == K - 1) wait_carry(c + 1);
+        }
+        pixel(c * K + off, off, slot + cost_first_full + off * cost_step, pens + off);
+        rows_barrier(R * 32);
+      }
+      end_chunk(c);
     }
-    rows_barrier(R * 32);
-  }
+    if (full_chunks < nchunks) {
+      // Partial last chunk.
+      const int c = full_chunks, n = W - c * K;
+      wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
+      if constexpr (CARRY_IN) wait_carry(c);
+      const uint8_t* slot = my_slots + (c % NB) * L::cslot;
+      const uint4* pens = (const uint4*)(slot + 2 * K * Dp);
+      const int first = (mirror ? (n - 1) * Dp : 0) + lane * REGS;
+      for (int off = 0; off < n; off++) {
+        pixel(c * K + off, off, slot + first + off * cost_step, pens + off);
+        rows_barrier(R * 32);
+      }
+      end_chunk(c);
+    }
+  };
+  if (use_carry)
+    sweep_row(std::true_type{}, std::false_type{});
+  else if (publish)
+    sweep_row(std::false_type{}, std::true_type{});
+  else
+    sweep_row(std::false_type{}, std::false_type{});
+
+  // Idle steps after this row finished (the rows below are still running).
+  for (int step = 0; step < 2 * (R - 1 - w); step++) rows_barrier(R * 32);
+  // After an expired wait, give outstanding chunk copies a bounded chance to land before exit.
+  for (int cc = max(0, issued - NB); cc < issued; cc++)
+    wait_bar(&my_full[cc % NB], (cc / NB) & 1, err, limit / 4, 5, false);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Winner-take-all, uniqueness and sub-pixel selection of both views (CensusSgm.java:460-515).
-// A warp owns a tile of 32 consecutive pixels of one row of one view; lane 0 bulk-copies the
-// tile's two partial aggregates (down, up) into shared memory (double-buffered across tiles) and
-// every lane then selects one pixel.  Lane t reads its pixel's words starting at word t, so the
-// 32 lanes hit 32 different banks although the pixels are Dp words apart.
+// One warp per pixel: lane l adds the two streams' partial aggregates of its REGS disparities
+// (both views packed), the first strict minimum and the second minimum outside best-1..best+1
+// are warp reductions of (total << 8 | k) keys, and lane v then selects view v.  A total of at
+// least `invalid` (directions x 512) marks a cell whose cost is invalid: every valid total is
+// smaller because each valid path cost is at most bits + P2 < 512.
 struct WtaArgs {
-  const uint16_t* down[2];  // per view; 0xffff = invalid cost
-  const uint16_t* up[2];
+  const uint32_t* down;  // [H][W][Dp] left | right << 16
+  const uint32_t* up;
   float* disp[2];
   uint8_t* reasons;    // left view only
   uint8_t* boundary;   // left view only
   DeviceStats* stats;  // left view only
-  int* error;
-  int W, H, D, min_disparity, rx, ry;
+  int W, H, D, min_disparity, rx, ry, invalid;
   double uniqueness;
-  long long timeout;
-};
-
-template <int DP>
-struct WtaLayout {
-  static constexpr int warps = DP <= 64 ? 8 : DP <= 128 ? 6 : DP <= 192 ? 4 : 3;
-  static constexpr int tile = 32 * DP * 2;             // bytes of one stream's tile
-  static constexpr int per_warp = 2 * 2 * tile;        // 2 buffers x (down, up)
-  static constexpr int bars = 0;                        // warps x 2 mbarriers
-  static constexpr int tiles = 128;
-  static constexpr int total = tiles + warps * per_warp;
 };
 
 // Selection of one pixel from its winners record (CensusSgm.java:471-513).
@@ -864,119 +895,70 @@ __device__ __forceinline__ void select_pixel_record(int best, int value, int sec
   *out = result;
 }
 
-template <int DP>
-__global__ void __launch_bounds__(WtaLayout<DP>::warps * 32) wta_kernel(const WtaArgs a) {
-  extern __shared__ __align__(128) uint8_t smem[];
-  using L = WtaLayout<DP>;
-  constexpr int NW = DP / 2;  // 32-bit words per pixel and stream
+constexpr int kWtaWarps = 8;
+
+template <int REGS>
+__global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
+  constexpr int Dp = 32 * REGS;
+  __shared__ __align__(16) uint32_t stage[kWtaWarps][Dp];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t* bars = (uint64_t*)(smem + L::bars) + warp * 2;
-  uint8_t* tiles = smem + L::tiles + warp * L::per_warp;
-  if (lane == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-  }
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  __syncwarp();
-
-  const int W = a.W, H = a.H, D = a.D;
-  const int per_row = (W + 31) / 32;
-  const int64_t items = 2LL * H * per_row;  // (view, row, tile)
-  const int64_t stride = (int64_t)gridDim.x * L::warps;
-  int64_t item = (int64_t)blockIdx.x * L::warps + warp;
-  auto decode = [&](int64_t it, int& view, int& y, int& x0) {
-    view = (int)(it / ((int64_t)H * per_row));
-    const int64_t r = it - (int64_t)view * H * per_row;
-    y = (int)(r / per_row);
-    x0 = (int)(r - (int64_t)y * per_row) * 32;
-  };
-  auto issue = [&](int64_t it, int buf) {
-    if (lane == 0) {
-      int view, y, x0;
-      decode(it, view, y, x0);
-      const uint32_t bytes = (uint32_t)(min(32, W - x0) * DP * 2);
-      const int64_t off = ((int64_t)y * W + x0) * DP;
-      fence_proxy_async_shared();
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                       smem_u32(&bars[buf])),
-                   "r"(2 * bytes)
-                   : "memory");
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-          "[%3];" ::"r"(smem_u32(tiles + (buf * 2) * L::tile)),
-          "l"((view ? a.down[1] : a.down[0]) + off), "r"(bytes), "r"(smem_u32(&bars[buf]))
-          : "memory");
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-          "[%3];" ::"r"(smem_u32(tiles + (buf * 2 + 1) * L::tile)),
-          "l"((view ? a.up[1] : a.up[0]) + off), "r"(bytes), "r"(smem_u32(&bars[buf]))
-          : "memory");
-    }
-    __syncwarp();  // no lane may spin on the barrier before lane 0 has armed it
-  };
-
+  const uint16_t* t16 = (const uint16_t*)stage[warp] + lane;  // view `lane` of k at t16[2k]
+  const int W = a.W, H = a.H, D = a.D, invalid = a.invalid;
+  const int64_t n = (int64_t)W * H;
+  const int64_t stride = (int64_t)gridDim.x * kWtaWarps;
   unsigned counts[6] = {0, 0, 0, 0, 0, 0};
-  int it = 0;
-  if (item < items) issue(item, 0);
-  for (; item < items; item += stride, it++) {
-    const int buf = it & 1;
-    if (item + stride < items) issue(item + stride, buf ^ 1);
-    wait_bar(&bars[buf], (it >> 1) & 1, a.error, a.timeout, 4);
-    int view, y, x0;
-    decode(item, view, y, x0);
-    const int x = x0 + lane;
-    if (x < W) {
-      const uint32_t* pa = (const uint32_t*)(tiles + (buf * 2) * L::tile) + lane * NW;
-      const uint32_t* pb = (const uint32_t*)(tiles + (buf * 2 + 1) * L::tile) + lane * NW;
-      const uint16_t* ha = (const uint16_t*)pa;
-      const uint16_t* hb = (const uint16_t*)pb;
-      const bool inside = y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx;
-      int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
-      if (inside) {
-        // Pass 1: first strict minimum among valid disparities, as key = total << 8 | k.
-        uint32_t key = 0xffffffffu;
-        int wi = lane;
-        for (int i = 0; i < NW; i++) {
-          const uint32_t wa = pa[wi], wb = pb[wi];
-          const uint32_t bad = prmt(wa, 0, 0xbb99u);  // 0xffff where the cost is invalid
-          const uint32_t tot = ((wa & ~bad) + wb) | bad;
-          const uint32_t k = 2 * wi;
-          key = min(key, min(((tot & 0xffffu) << 8) | k, ((tot >> 8) & 0xffff00u) | (k + 1)));
-          if (++wi == NW) wi = 0;
-        }
-        if ((key >> 8) != 0xffffu) {
+  for (int64_t p = (int64_t)blockIdx.x * kWtaWarps + warp; p < n; p += stride) {
+    const int y = (int)(p / W), x = (int)(p - (int64_t)y * W);
+    int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
+    if (y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx) {
+      uint32_t d[REGS], u[REGS], tot[REGS];
+      load_words<REGS>(a.down + p * Dp + lane * REGS, d);
+      load_words<REGS>(a.up + p * Dp + lane * REGS, u);
+#pragma unroll
+      for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j];
+      // Pass 1: first strict minimum, as key = total << 8 | k.
+      uint32_t k0 = 0xffffffffu, k1 = 0xffffffffu;
+#pragma unroll
+      for (int j = 0; j < REGS; j++) {
+        const uint32_t k = lane * REGS + j;
+        k0 = min(k0, ((tot[j] << 8) & 0xffff00u) | k);
+        k1 = min(k1, ((tot[j] >> 8) & 0xffff00u) | k);
+      }
+      k0 = __reduce_min_sync(0xffffffffu, k0);
+      k1 = __reduce_min_sync(0xffffffffu, k1);
+      // Pass 2: minimum outside best-1..best+1.
+      const int b0 = (int)(k0 & 0xffu), b1 = (int)(k1 & 0xffu);
+      uint32_t s0 = 0xffffu, s1 = 0xffffu;
+#pragma unroll
+      for (int j = 0; j < REGS; j++) {
+        const int k = lane * REGS + j;
+        if ((unsigned)(k - b0 + 1) > 2u) s0 = min(s0, tot[j] & 0xffffu);
+        if ((unsigned)(k - b1 + 1) > 2u) s1 = min(s1, tot[j] >> 16);
+      }
+      s0 = __reduce_min_sync(0xffffffffu, s0);
+      s1 = __reduce_min_sync(0xffffffffu, s1);
+      store_words<REGS>(stage[warp] + lane * REGS, tot);
+      __syncwarp();
+      if (lane < 2) {
+        const uint32_t key = lane ? k1 : k0;
+        if ((int)(key >> 8) < invalid) {
           best = (int)(key & 0xffu);
           value = (int)(key >> 8);
-          // Pass 2: minimum over valid disparities outside best-1..best+1.
-          uint32_t sec = 0xffffu;
-          wi = lane;
-          for (int i = 0; i < NW; i++) {
-            const uint32_t wa = pa[wi], wb = pb[wi];
-            const uint32_t bad = prmt(wa, 0, 0xbb99u);
-            const uint32_t tot = ((wa & ~bad) + wb) | bad;
-            const int k = 2 * wi;
-            if ((unsigned)(k - best + 1) > 2u) sec = min(sec, tot & 0xffffu);
-            if ((unsigned)(k - best + 2) > 2u) sec = min(sec, tot >> 16);
-            if (++wi == NW) wi = 0;
-          }
-          second = sec == 0xffffu ? INT_MAX : (int)sec;
-          if (best >= 1 && !(ha[best - 1] & 0x8000u)) before = ha[best - 1] + hb[best - 1];
-          if (best + 1 < D && !(ha[best + 1] & 0x8000u)) after = ha[best + 1] + hb[best + 1];
-          flags = (!(ha[0] & 0x8000u) ? 1 : 0) | (!(ha[D - 1] & 0x8000u) ? 2 : 0);
+          const int sec = (int)(lane ? s1 : s0);
+          second = sec < invalid ? sec : INT_MAX;
+          if (best >= 1 && t16[2 * (best - 1)] < invalid) before = t16[2 * (best - 1)];
+          if (best + 1 < D && t16[2 * (best + 1)] < invalid) after = t16[2 * (best + 1)];
+          flags = (t16[0] < invalid ? 1 : 0) | (t16[2 * (D - 1)] < invalid ? 2 : 0);
         }
       }
-      const int64_t p = (int64_t)y * W + x;
-      select_pixel_record(best, value, second, before, after, flags, D, a.min_disparity,
-                          a.uniqueness, (view ? a.disp[1] : a.disp[0]) + p,
-                          view == 0 && a.reasons ? a.reasons + p : nullptr,
-                          view == 0 && a.boundary ? a.boundary + p : nullptr, counts, view == 0);
+      __syncwarp();
     }
-    __syncwarp();
+    if (lane < 2)
+      select_pixel_record(best, value, second, before, after, flags, D, a.min_disparity,
+                          a.uniqueness, (lane ? a.disp[1] : a.disp[0]) + p,
+                          lane == 0 && a.reasons ? a.reasons + p : nullptr,
+                          lane == 0 && a.boundary ? a.boundary + p : nullptr, counts, lane == 0);
   }
-  // Every issued tile was waited for above; after a timed-out wait, give the copy a bounded
-  // second chance to land before the CTA's shared memory is released.
-  for (int j = max(0, it - 2); j < it; j++)
-    wait_bar(&bars[j & 1], (j >> 1) & 1, a.error, a.timeout / 4, 5, false);
   if (a.stats) {
     unsigned long long* dst[6] = {&a.stats->lower_boundary_rejected,
                                   &a.stats->full_interval_pixels, &a.stats->boundary_rejected,
@@ -990,47 +972,55 @@ __global__ void __launch_bounds__(WtaLayout<DP>::warps * 32) wta_kernel(const Wt
   }
 }
 
-template <int DP>
+template <int REGS>
 cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
-  using L = WtaLayout<DP>;
-  cudaError_t e =
-      cudaFuncSetAttribute(wta_kernel<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total);
-  if (e != cudaSuccess) return e;
-  const int64_t items = 2LL * a.H * ((a.W + 31) / 32);
-  const int grid = (int)std::min<int64_t>((items + L::warps - 1) / L::warps, sm_count);
-  wta_kernel<DP><<<grid, L::warps * 32, L::total, stream>>>(a);
+  const int64_t n = (int64_t)a.W * a.H;
+  const int grid = (int)std::min<int64_t>((n + kWtaWarps - 1) / kWtaWarps, (int64_t)sm_count * 8);
+  wta_kernel<REGS><<<grid, kWtaWarps * 32, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
-template <int REGS, int NPATH, int K, int R, int MINB>
+template <int REGS, int NPATH, int K, int R>
 cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
-  auto kernel = sweep_kernel<REGS, NPATH, K, R, MINB>;
-  const int shared = SweepLayout<REGS, K, R>::total;
+  auto kernel = sweep_kernel<REGS, NPATH, K, R>;
+  const int shared = SweepLayout<REGS, NPATH, K, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
   kernel<<<2 * a.nb, (R + 1) * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
-// Per-register-count configuration: chunk pixels, rows per CTA (shared-memory fit), CTAs per SM.
-constexpr int chunk_for(int regs) { return regs >= 6 ? 2 : 4; }
-constexpr int rows_for(int regs) { return regs <= 4 ? 16 : 8; }
-constexpr int minb_for(int) { return 1; }
+// Rows per sweep CTA: few enough that the rows of a block (all busy at once) spread over SMs,
+// many enough that the carry hand-off between blocks stays rare.
+constexpr int kChunk = 4;
+constexpr int rows_default(int regs) { return regs >= 8 ? 4 : 8; }
+
+// Rows per sweep CTA: the default, or CSGM_SWEEP_ROWS (4 or 8) for tuning runs.
+int rows_for(int regs) {
+  static const int forced = [] {
+    const char* e = getenv("CSGM_SWEEP_ROWS");
+    const int v = e ? atoi(e) : 0;
+    return v == 4 || v == 8 ? v : 0;
+  }();
+  return forced ? forced : rows_default(regs);
+}
 
 struct FusedLayout {
-  size_t cost, sum, carry, flags, total;
-  int Dp, nb, slot, rows;
+  size_t cost, sum, pen, carry, flags, total;
+  int Dp, nb, vslot, rows;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
-    rows = rows_for(Dp / (2 * kLanes));
+    rows = rows_for(Dp / 32);
     nb = (h + rows - 1) / rows;
-    slot = 3 * Dp * 2 + 16;
+    const int nv = p.directions == 8 ? 3 : 1;
+    vslot = nv * Dp * 4 + 16;
     size_t n = (size_t)w * h;
     cost = n * Dp;
-    sum = n * Dp * 2;
-    carry = (size_t)2 * nb * w * kViews * slot;
+    sum = n * Dp * 4;
+    pen = 2 * n * 16;
+    carry = (size_t)2 * nb * w * vslot;
     flags = ((size_t)2 * nb + 8) * sizeof(int);
-    total = 2 * cost + 4 * sum + carry + flags + 6 * 256;
+    total = 2 * cost + 2 * sum + pen + carry + flags + 6 * 256;
   }
 };
 
@@ -1039,7 +1029,10 @@ struct FusedLayout {
 bool fused_supported(const csgm_params& p) {
   if (p.disparities > 256 || p.aggregate_bytes != 2) return false;
   if (p.directions != 4 && p.directions != 8) return false;
-  if (512 + 2 * (int64_t)p.p2 + p.p1 > 65535) return false;
+  // Valid path costs stay below 512 (cost <= bits, penalty <= P2), which is what lets the
+  // selection tell invalid cells by their totals.
+  const int bits = p.window_x * p.window_y - 1;
+  if (bits > 127 || p.p2 + bits >= 512) return false;
   return true;
 }
 
@@ -1050,17 +1043,18 @@ size_t fused_workspace_bytes(const csgm_params& p, int w, int h) {
 int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h,
                     int** error_flag) {
   int status = CSGM_OK;
+  if (h > 65535) return fail(CSGM_E_UNSUPPORTED, "fused path: image taller than 65535 rows");
   FusedLayout F(p, w, h);
   uint8_t* cost_l = (uint8_t*)ctx.ws->get(kCostL, F.cost, &status);
   if (!cost_l) return status;
   uint8_t* cost_r = (uint8_t*)ctx.ws->get(kCostR, F.cost, &status);
   if (!cost_r) return status;
-  uint16_t* sums[4];
-  const int sum_slots[4] = {kSum, kSumR, kSumUp, kSumUpR};
-  for (int i = 0; i < 4; i++) {
-    sums[i] = (uint16_t*)ctx.ws->get(sum_slots[i], F.sum, &status);
-    if (!sums[i]) return status;
-  }
+  uint32_t* sum_down = (uint32_t*)ctx.ws->get(kSum, F.sum, &status);
+  if (!sum_down) return status;
+  uint32_t* sum_up = (uint32_t*)ctx.ws->get(kSumUp, F.sum, &status);
+  if (!sum_up) return status;
+  uint4* pen = (uint4*)ctx.ws->get(kPen, F.pen, &status);
+  if (!pen) return status;
   uint8_t* carry = (uint8_t*)ctx.ws->get(kCarry, F.carry, &status);
   if (!carry) return status;
   int* flags = (int*)ctx.ws->get(kFlags, F.flags, &status);
@@ -1106,20 +1100,24 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     if (le != cudaSuccess) return cuda_fail(le, "cost kernel launch");
     ctx.prof->kernel_end("cost_pair");
   }
+  {
+    PenaltyArgs pa{{v.gray_l, v.gray_r}, {v.tex_l, v.tex_r}, pen, w, h, p.p1, p.p2,
+                   p.edge_scale};
+    ctx.prof->kernel_begin();
+    penalty_kernel<<<dim3((w + 127) / 128, h, 2), 128, 0, ctx.stream>>>(pa);
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return cuda_fail(le, "penalty kernel launch");
+    ctx.prof->kernel_end("penalty");
+  }
   cudaError_t e = cudaMemsetAsync(flags, 0, F.flags, ctx.stream);
   if (e != cudaSuccess) return cuda_fail(e, "flag clear");
 
   SweepArgs a{};
   a.cost[0] = cost_l;
   a.cost[1] = cost_r;
-  a.gray[0] = v.gray_l;
-  a.gray[1] = v.gray_r;
-  a.tex[0] = v.tex_l;
-  a.tex[1] = v.tex_r;
-  a.sum[0][0] = sums[0];
-  a.sum[0][1] = sums[1];
-  a.sum[1][0] = sums[2];
-  a.sum[1][1] = sums[3];
+  a.pen = pen;
+  a.sum[0] = sum_down;
+  a.sum[1] = sum_up;
   a.carry = carry;
   a.progress = flags;
   a.ticket = flags + 2 * F.nb;
@@ -1129,18 +1127,18 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.H = h;
   a.D = p.disparities;
   a.nb = F.nb;
-  a.Hp = F.nb * F.rows;
   a.p1 = p.p1;
-  a.p2 = p.p2;
-  a.edge_scale = p.edge_scale;
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
-  const int regs = F.Dp / (2 * kLanes);
+  const int regs = F.Dp / 32;
   const bool eight = p.directions == 8;
   ctx.prof->kernel_begin();
-  switch (regs * 2 + (eight ? 1 : 0)) {
-#define CSGM_SWEEP_CASE(R_, NP_)                                                             \
-  case R_ * 2 + (NP_ == 4 ? 1 : 0):                                                         \
-    e = launch_sweep<R_, NP_, chunk_for(R_), rows_for(R_), minb_for(R_)>(a, ctx.stream);     \
+  switch (regs * 4 + (eight ? 2 : 0) + (F.rows == 8 ? 1 : 0)) {
+#define CSGM_SWEEP_CASE(R_, NP_)                                                       \
+  case R_ * 4 + (NP_ == 4 ? 2 : 0):                                                   \
+    e = launch_sweep<R_, NP_, kChunk, 4>(a, ctx.stream);                              \
+    break;                                                                             \
+  case R_ * 4 + (NP_ == 4 ? 2 : 0) + 1:                                               \
+    e = launch_sweep<R_, NP_, kChunk, 8>(a, ctx.stream);                              \
     break;
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)
@@ -1157,30 +1155,27 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   ctx.prof->kernel_end("sweep");
 
   WtaArgs t{};
-  t.down[0] = sums[0];
-  t.down[1] = sums[1];
-  t.up[0] = sums[2];
-  t.up[1] = sums[3];
+  t.down = sum_down;
+  t.up = sum_up;
   t.disp[0] = v.disp_l;
   t.disp[1] = v.disp_r;
   t.reasons = v.reasons;
   t.boundary = v.boundary;
   t.stats = v.stats;
-  t.error = a.error;
   t.W = w;
   t.H = h;
   t.D = p.disparities;
   t.min_disparity = p.min_disparity;
   t.rx = p.window_x / 2;
   t.ry = p.window_y / 2;
+  t.invalid = 512 * p.directions;
   t.uniqueness = p.uniqueness;
-  t.timeout = a.timeout;
   ctx.prof->kernel_begin();
-  switch (F.Dp) {
-    case 64: e = launch_wta<64>(t, ctx.sm_count, ctx.stream); break;
-    case 128: e = launch_wta<128>(t, ctx.sm_count, ctx.stream); break;
-    case 192: e = launch_wta<192>(t, ctx.sm_count, ctx.stream); break;
-    case 256: e = launch_wta<256>(t, ctx.sm_count, ctx.stream); break;
+  switch (regs) {
+    case 2: e = launch_wta<2>(t, ctx.sm_count, ctx.stream); break;
+    case 4: e = launch_wta<4>(t, ctx.sm_count, ctx.stream); break;
+    case 6: e = launch_wta<6>(t, ctx.sm_count, ctx.stream); break;
+    case 8: e = launch_wta<8>(t, ctx.sm_count, ctx.stream); break;
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
   if (e != cudaSuccess) return cuda_fail(e, "wta kernel launch");
