@@ -105,132 +105,196 @@ __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* er
 
 // ---------------------------------------------------------------------------------------------
 // Cost volumes of both views (uint8, 0x80 = invalid), StereoCost.value semantics
-// (StereoCost.java:50-90) with CensusSgm.java:405-420 validity.  A CTA handles a segment of
-// kCostSeg pixels of one row of one view: the segment's descriptors, textures and grays (with the
-// disparity range of the target view) are staged in shared memory; one thread computes one
-// pixel's Dp costs into a per-warp staging tile that the warp then writes out as coalesced
-// 16-byte stores.  ZNCC (FP64 window sums) stays on the general per-cell path.
+// (StereoCost.java:50-90) with CensusSgm.java:405-420 validity.  A CTA item is a segment of
+// kCostSeg pixels of one row of one view.  The segment's descriptors and the target view's
+// descriptors over the disparity span are staged in shared memory, each target with a validity
+// byte (inside [r, w-r) and textured) and, for the blended modes, its gray value or packed
+// central-difference gradient.  Thread t computes pixel t % kCostSeg for a slice of disparity
+// groups (consecutive threads read consecutive targets: no bank conflicts) into a padded tile
+// that the CTA then writes out as coalesced 16-byte stores.  The blended modes divide by
+// 1000 * cap through an exact 64-bit reciprocal (floor(n * ceil(2^64 / d) / 2^64) == n / d for
+// n, d < 2^32).  ZNCC (FP64 window sums) stays on the general per-cell path.
 struct CostPairArgs {
   CostArgs view[2];  // per view: a = matching image, b = target image, reverse 0/1
   uint8_t* out[2];
   int Dp;
+  unsigned long long recip;  // ceil(2^64 / (1000 * cap)) of the blended modes
 };
 
-constexpr int kCostSeg = 128;  // pixels per CTA segment (4 warps x 32 pixels)
+constexpr int kCostSeg = 64;       // pixels per CTA item
+constexpr int kCostThreads = 256;  // 4 threads per pixel
 
-__global__ void __launch_bounds__(kCostSeg) cost_rows_kernel(CostPairArgs a) {
+template <int DP>
+struct CostLayout {
+  static constexpr int pitch = DP + 16;                   // tile row pitch (bank spread)
+  static constexpr int tile = 0;                          // [kCostSeg][pitch] cost bytes
+  static constexpr int da = tile + kCostSeg * pitch;       // [2][kCostSeg] u64
+  static constexpr int span = kCostSeg + DP;               // staged targets (>= seg + DP - 1)
+  static constexpr int db = da + 2 * kCostSeg * 8;         // [2][span] u64
+  static constexpr int aux = db + 2 * span * 8;            // [span] u32 gray / gradient of targets
+  static constexpr int valid = aux + span * 4;             // [span] u8
+  static constexpr int inside = valid + span;              // [kCostSeg] u8
+  static constexpr int aaux = inside + kCostSeg;           // [kCostSeg] u32 of the segment pixels
+  static constexpr int total = (aaux + kCostSeg * 4 + 15) / 16 * 16;
+};
+
+// Packed central-difference gradient (dx | dy << 16, each as int16) of pixel (x, y).
+__device__ __forceinline__ uint32_t gradient_of(const uint8_t* g, int w, int h, int x, int y) {
+  if (x < 1 || x >= w - 1 || y < 1 || y >= h - 1) return 0;
+  const int64_t p = (int64_t)y * w + x;
+  const int dx = (int)g[p + 1] - (int)g[p - 1];
+  const int dy = (int)g[p + w] - (int)g[p - w];
+  return (uint32_t)(dx & 0xffff) | ((uint32_t)dy << 16);
+}
+
+template <int DP, int MODE, int WORDS>
+__global__ void __launch_bounds__(kCostThreads) cost_rows_kernel(const CostPairArgs a) {
   extern __shared__ __align__(16) uint8_t csm[];
-  const CostArgs& c = a.view[blockIdx.y];
-  uint8_t* out = a.out[blockIdx.y];
-  const int w = c.w, h = c.h, D = c.D, Dp = a.Dp, words = c.words;
-  const int rx = c.wx / 2, ry = c.wy / 2;
+  using L = CostLayout<DP>;
+  constexpr int G = DP / 16;              // 16-disparity groups per pixel
+  constexpr int TPP = kCostThreads / kCostSeg;  // threads per pixel
+  uint8_t* tile = csm + L::tile;
+  uint64_t* da = (uint64_t*)(csm + L::da);
+  uint64_t* db = (uint64_t*)(csm + L::db);
+  uint32_t* aux = (uint32_t*)(csm + L::aux);
+  uint8_t* valid = csm + L::valid;
+  uint8_t* inside = csm + L::inside;
+  uint32_t* aaux = (uint32_t*)(csm + L::aaux);
+  const int w = a.view[0].w, h = a.view[0].h, D = a.view[0].D, mind = a.view[0].min_disparity;
+  const int rx = a.view[0].wx / 2, ry = a.view[0].wy / 2;
   const int segs = (w + kCostSeg - 1) / kCostSeg;
-  // Target columns of a segment [x0, x0+seg): left view q = x - d, right view q = x + d.
-  const int span = kCostSeg + D;  // staged target pixels
-  uint64_t* da = (uint64_t*)csm;                       // [words][kCostSeg]
-  uint64_t* db = da + 2 * kCostSeg;                    // [words][span]
-  uint8_t* stage = (uint8_t*)(db + 2 * span);          // [4 warps][32][Dp]
-  uint8_t* ta = stage + 4 * 32 * Dp;                   // [kCostSeg]
-  uint8_t* tb = ta + kCostSeg;                         // [span]
-  uint8_t* ga = tb + span;                             // [3][kCostSeg + 2] rows y-1..y+1, x0-1..
-  uint8_t* gb = ga + 3 * (kCostSeg + 2);               // [3][span + 2]
   const int64_t n = (int64_t)w * h;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t item = blockIdx.x; item < (int64_t)h * segs; item += gridDim.x) {
-    const int y = (int)(item / segs), x0 = (int)(item % segs) * kCostSeg;
-    const int qlo = c.reverse ? x0 + c.min_disparity : x0 - c.min_disparity - (D - 1);
+  const int64_t items = 2LL * h * segs;
+  for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const int view = (int)(item / ((int64_t)h * segs));
+    const int rest = (int)(item - (int64_t)view * h * segs);
+    const int y = rest / segs, x0 = (rest % segs) * kCostSeg;
+    const CostArgs& c = view ? a.view[1] : a.view[0];
+    uint8_t* out = view ? a.out[1] : a.out[0];
+    // Target pixel of (x0 + i, k): qlo + i + DP - 1 - k (left view), qlo + i + k (right view).
+    const int qlo = view ? x0 + mind : x0 - mind - (DP - 1);
     const bool row_inside = y >= ry && y < h - ry;
-    __syncthreads();
-    // Stage the segment.
-    for (int i = threadIdx.x; i < kCostSeg; i += blockDim.x) {
+    const int64_t row = (int64_t)y * w;
+    __syncthreads();  // the previous item's tile has been written out
+    for (int i = threadIdx.x; i < kCostSeg; i += kCostThreads) {
       const int x = x0 + i;
       const bool ok = x < w;
-      const int64_t p = (int64_t)y * w + x;
-      for (int j = 0; j < words; j++) da[j * kCostSeg + i] = ok ? c.desc_a[j * n + p] : 0;
-      ta[i] = ok ? c.tex_a[p] : 0;
+#pragma unroll
+      for (int j = 0; j < WORDS; j++) da[j * kCostSeg + i] = ok ? c.desc_a[j * n + row + x] : 0;
+      inside[i] = ok && row_inside && x >= rx && x < w - rx && c.tex_a[row + x];
+      if (MODE == CSGM_COST_AD_CENSUS) aaux[i] = ok ? c.gray_a[row + x] : 0;
+      if (MODE == CSGM_COST_CENSUS_GRADIENT) aaux[i] = ok ? gradient_of(c.gray_a, w, h, x, y) : 0;
     }
-    for (int i = threadIdx.x; i < span; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kCostSeg + DP - 1; i += kCostThreads) {
       const int q = qlo + i;
-      const bool ok = q >= 0 && q < w;
-      const int64_t p = (int64_t)y * w + q;
-      for (int j = 0; j < words; j++) db[j * span + i] = ok ? c.desc_b[j * n + p] : 0;
-      tb[i] = ok ? c.tex_b[p] : 0;
+      const bool ok = q >= rx && q < w - rx;
+#pragma unroll
+      for (int j = 0; j < WORDS; j++) db[j * L::span + i] = ok ? c.desc_b[j * n + row + q] : 0;
+      valid[i] = ok && c.tex_b[row + q] ? 0xff : 0;
+      if (MODE == CSGM_COST_AD_CENSUS) aux[i] = ok ? c.gray_b[row + q] : 0;
+      if (MODE == CSGM_COST_CENSUS_GRADIENT) aux[i] = ok ? gradient_of(c.gray_b, w, h, q, y) : 0;
     }
-    if (c.mode == CSGM_COST_AD_CENSUS || c.mode == CSGM_COST_CENSUS_GRADIENT) {
-      for (int i = threadIdx.x; i < 3 * (kCostSeg + 2); i += blockDim.x) {
-        const int r = i / (kCostSeg + 2), x = x0 - 1 + i % (kCostSeg + 2), yy = y - 1 + r;
-        ga[i] = (yy >= 0 && yy < h && x >= 0 && x < w) ? c.gray_a[(int64_t)yy * w + x] : 0;
-      }
-      for (int i = threadIdx.x; i < 3 * (span + 2); i += blockDim.x) {
-        const int r = i / (span + 2), x = qlo - 1 + i % (span + 2), yy = y - 1 + r;
-        gb[i] = (yy >= 0 && yy < h && x >= 0 && x < w) ? c.gray_b[(int64_t)yy * w + x] : 0;
+    __syncthreads();
+    {
+      const int i = threadIdx.x % kCostSeg;
+      const bool in = inside[i];
+      const uint64_t a0 = da[i], a1 = WORDS > 1 ? da[kCostSeg + i] : 0;
+      const uint32_t av = aaux[i];
+      const int cap = MODE == CSGM_COST_AD_CENSUS ? c.ad_cap : c.grad_cap;
+      const uint32_t wh = (uint32_t)(c.weight * cap), wd = (uint32_t)((1000 - c.weight) * c.bits);
+      const uint32_t half = (uint32_t)(1000 * cap / 2);
+      for (int g = threadIdx.x / kCostSeg; g < G; g += TPP) {
+        uint32_t word[4] = {0x80808080u, 0x80808080u, 0x80808080u, 0x80808080u};
+        if (in) {
+#pragma unroll
+          for (int m = 0; m < 4; m++) {
+            uint32_t v[4];
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+              const int k = g * 16 + m * 4 + b;
+              const int qi = view ? i + k : i + DP - 1 - k;  // inside the staged span
+              uint32_t ham = __popcll(a0 ^ db[qi]);
+              if (WORDS > 1) ham += __popcll(a1 ^ db[L::span + qi]);
+              uint32_t cost = ham;
+              if (MODE != CSGM_COST_CENSUS) {
+                uint32_t diff;
+                if (MODE == CSGM_COST_AD_CENSUS) {
+                  diff = (uint32_t)abs((int)av - (int)aux[qi]);
+                } else {
+                  const uint32_t d2 = __vabsdiffs2(av, aux[qi]);
+                  diff = (d2 & 0xffffu) + (d2 >> 16);
+                }
+                const uint32_t num = wh * ham + wd * min(diff, (uint32_t)cap) + half;
+                cost = (uint32_t)__umul64hi((unsigned long long)num, a.recip);
+              }
+              // valid[] is 0x00 / 0xff: cost where the target is valid, 0x80 elsewhere.
+              const uint32_t keep = (uint32_t)(int32_t)(int8_t)valid[qi];
+              v[b] = (cost & keep) | (0x80u & ~keep);
+            }
+            word[m] = __byte_perm(__byte_perm(v[0], v[1], 0x0040), __byte_perm(v[2], v[3], 0x0040),
+                                  0x5410);
+          }
+          if (g * 16 + 16 > D) {  // disparities >= D are invalid
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+#pragma unroll
+              for (int b = 0; b < 4; b++)
+                if (g * 16 + m * 4 + b >= D) word[m] = (word[m] & ~(0xffu << (8 * b))) | (0x80u << (8 * b));
+          }
+        }
+        *(uint4*)(tile + i * L::pitch + g * 16) = make_uint4(word[0], word[1], word[2], word[3]);
       }
     }
     __syncthreads();
-    // One pixel per thread.
-    const int xi = threadIdx.x, x = x0 + xi;
-    uint8_t* mine = stage + (warp * 32 + lane) * Dp;
-    const bool inside = x < w && row_inside && x >= rx && x < w - rx && ta[xi];
-    const int ax = inside && c.mode == CSGM_COST_CENSUS_GRADIENT
-                       ? (int)ga[(kCostSeg + 2) + xi + 2] - (int)ga[(kCostSeg + 2) + xi] : 0;
-    const int ay = inside && c.mode == CSGM_COST_CENSUS_GRADIENT
-                       ? (int)ga[2 * (kCostSeg + 2) + xi + 1] - (int)ga[xi + 1] : 0;
-    const int gav = inside ? (int)ga[(kCostSeg + 2) + xi + 1] : 0;
-    const int denominator = 1000 * (c.mode == CSGM_COST_AD_CENSUS ? c.ad_cap : c.grad_cap);
-    for (int k0 = 0; k0 < Dp; k0 += 4) {
-      uint32_t packed = 0;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = k0 + j;
-        int value = 0x80;
-        if (inside && k < D) {
-          const long long disparity = (long long)c.min_disparity + k;
-          const long long target = (long long)x + (c.reverse ? disparity : -disparity);
-          if (target >= rx && target < w - rx) {
-            const int qi = (int)(target - qlo);
-            if (tb[qi]) {
-              int ham = __popcll(da[xi] ^ db[qi]);
-              if (words > 1) ham += __popcll(da[kCostSeg + xi] ^ db[span + qi]);
-              value = ham;
-              if (c.mode == CSGM_COST_AD_CENSUS || c.mode == CSGM_COST_CENSUS_GRADIENT) {
-                int difference, cap;
-                if (c.mode == CSGM_COST_AD_CENSUS) {
-                  difference = abs(gav - (int)gb[(span + 2) + qi + 1]);
-                  cap = c.ad_cap;
-                } else {
-                  const int bx = (int)gb[(span + 2) + qi + 2] - (int)gb[(span + 2) + qi];
-                  const int by = (int)gb[2 * (span + 2) + qi + 1] - (int)gb[qi + 1];
-                  difference = abs(ax - bx) + abs(ay - by);
-                  cap = c.grad_cap;
-                }
-                value = (c.weight * ham * cap + (1000 - c.weight) * min(difference, cap) * c.bits +
-                         denominator / 2) /
-                        denominator;
-              }
-            }
-          }
-        }
-        packed |= (uint32_t)value << (8 * j);
-      }
-      *(uint32_t*)(mine + k0) = packed;
+    // Coalesced write-out: the segment's pixels are contiguous in the volume.
+    const int npx = min(kCostSeg, w - x0);
+    uint8_t* dst = out + (row + x0) * DP;
+    for (int t = threadIdx.x; t < npx * G; t += kCostThreads) {
+      const int i = t / G, g = t % G;
+      __stcs((uint4*)(dst + (int64_t)i * DP + g * 16), *(const uint4*)(tile + i * L::pitch + g * 16));
     }
-    __syncwarp();
-    // Coalesced write-out of the warp's 32 pixels (contiguous in memory).
-    const int wx0 = x0 + warp * 32;
-    const int npx = max(0, min(32, w - wx0));
-    const int64_t base = ((int64_t)y * w + wx0) * Dp;
-    const uint8_t* tile = stage + warp * 32 * Dp;
-    for (int b = lane * 16; b < npx * Dp; b += 32 * 16)
-      *(uint4*)(out + base + b) = *(const uint4*)(tile + b);
   }
 }
 
-size_t cost_rows_shared(int D, int Dp) {
-  const int span = kCostSeg + D;
-  return 2 * kCostSeg * 8 + 2 * (size_t)span * 8 + 4 * 32 * (size_t)Dp + kCostSeg + span +
-         3 * (kCostSeg + 2) + 3 * ((size_t)span + 2) + 16;
+template <int DP, int MODE, int WORDS>
+cudaError_t launch_cost_rows_t(const CostPairArgs& a, int sm_count, cudaStream_t stream) {
+  using L = CostLayout<DP>;
+  auto kernel = cost_rows_kernel<DP, MODE, WORDS>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total);
+  if (e != cudaSuccess) return e;
+  const int64_t items = 2LL * a.view[0].h * ((a.view[0].w + kCostSeg - 1) / kCostSeg);
+  const int grid = (int)std::min<int64_t>(items, (int64_t)sm_count * 8);
+  kernel<<<grid, kCostThreads, L::total, stream>>>(a);
+  return cudaGetLastError();
 }
 
+template <int DP>
+cudaError_t launch_cost_rows_dp(const CostPairArgs& a, int sm_count, cudaStream_t stream) {
+  const int mode = a.view[0].mode, words = a.view[0].words;
+  if (mode == CSGM_COST_CENSUS)
+    return words > 1 ? launch_cost_rows_t<DP, CSGM_COST_CENSUS, 2>(a, sm_count, stream)
+                     : launch_cost_rows_t<DP, CSGM_COST_CENSUS, 1>(a, sm_count, stream);
+  if (mode == CSGM_COST_AD_CENSUS)
+    return words > 1 ? launch_cost_rows_t<DP, CSGM_COST_AD_CENSUS, 2>(a, sm_count, stream)
+                     : launch_cost_rows_t<DP, CSGM_COST_AD_CENSUS, 1>(a, sm_count, stream);
+  return words > 1 ? launch_cost_rows_t<DP, CSGM_COST_CENSUS_GRADIENT, 2>(a, sm_count, stream)
+                   : launch_cost_rows_t<DP, CSGM_COST_CENSUS_GRADIENT, 1>(a, sm_count, stream);
+}
+
+cudaError_t launch_cost_rows(const CostPairArgs& a, int sm_count, cudaStream_t stream) {
+  switch (a.Dp) {
+    case 64: return launch_cost_rows_dp<64>(a, sm_count, stream);
+    case 128: return launch_cost_rows_dp<128>(a, sm_count, stream);
+    case 192: return launch_cost_rows_dp<192>(a, sm_count, stream);
+    case 256: return launch_cost_rows_dp<256>(a, sm_count, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ceil(2^64 / d) for 2 <= d < 2^32.
+unsigned long long reciprocal64(unsigned long long d) { return ~0ull / d + 1; }
+
+// ---------------------------------------------------------------------------------------------
 // ZNCC and other fallbacks: one warp per pixel, lanes own contiguous disparity groups.
 __global__ void cost_pair_kernel(CostPairArgs a) {
   const CostArgs& c = a.view[blockIdx.y];
@@ -907,15 +971,24 @@ __global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
   const int64_t n = (int64_t)W * H;
   const int64_t stride = (int64_t)gridDim.x * kWtaWarps;
   unsigned counts[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t p = (int64_t)blockIdx.x * kWtaWarps + warp; p < n; p += stride) {
+  // Software pipeline: the next pixel's aggregates are in flight while this one is selected.
+  uint32_t d[REGS], u[REGS];
+  int64_t p = (int64_t)blockIdx.x * kWtaWarps + warp;
+  if (p < n) {
+    load_words<REGS>(a.down + p * Dp + lane * REGS, d);
+    load_words<REGS>(a.up + p * Dp + lane * REGS, u);
+  }
+  for (; p < n; p += stride) {
     const int y = (int)(p / W), x = (int)(p - (int64_t)y * W);
+    uint32_t tot[REGS];
+#pragma unroll
+    for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j];
+    if (p + stride < n) {
+      load_words<REGS>(a.down + (p + stride) * Dp + lane * REGS, d);
+      load_words<REGS>(a.up + (p + stride) * Dp + lane * REGS, u);
+    }
     int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
     if (y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx) {
-      uint32_t d[REGS], u[REGS], tot[REGS];
-      load_words<REGS>(a.down + p * Dp + lane * REGS, d);
-      load_words<REGS>(a.up + p * Dp + lane * REGS, u);
-#pragma unroll
-      for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j];
       // Pass 1: first strict minimum, as key = total << 8 | k.
       uint32_t k0 = 0xffffffffu, k1 = 0xffffffffu;
 #pragma unroll
@@ -1087,15 +1160,9 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
       cost_pair_kernel<<<dim3(grid, 2), 256, 0, ctx.stream>>>(ca);
       le = cudaGetLastError();
     } else {
-      const size_t shared = cost_rows_shared(p.disparities, F.Dp);
-      le = cudaFuncSetAttribute(cost_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)shared);
-      if (le == cudaSuccess) {
-        const int64_t items = (int64_t)h * ((w + kCostSeg - 1) / kCostSeg);
-        const int grid = (int)std::min<int64_t>(items, (int64_t)ctx.sm_count * 16);
-        cost_rows_kernel<<<dim3(grid, 2), kCostSeg, shared, ctx.stream>>>(ca);
-        le = cudaGetLastError();
-      }
+      const int cap = p.cost_mode == CSGM_COST_AD_CENSUS ? p.ad_truncation : p.gradient_truncation;
+      ca.recip = p.cost_mode == CSGM_COST_CENSUS ? 0 : reciprocal64(1000ull * (unsigned)cap);
+      le = launch_cost_rows(ca, ctx.sm_count, ctx.stream);
     }
     if (le != cudaSuccess) return cuda_fail(le, "cost kernel launch");
     ctx.prof->kernel_end("cost_pair");

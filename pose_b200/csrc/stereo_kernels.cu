@@ -18,33 +18,50 @@ namespace csgm {
 
 // ---------------------------------------------------------------------------------------------
 // Census descriptors and texture masks (CensusSgm.java:523-555), both images in one launch.
-// blockIdx.z selects the image.  Border pixels get zero descriptors and are untextured.
-__global__ void census_texture_kernel(CensusArgs args) {
+// blockIdx.z selects the image.  A 32x8 block stages its pixels plus the window apron in shared
+// memory; border pixels get zero descriptors and are untextured.
+constexpr int kCensusBx = 32, kCensusBy = 8, kCensusMaxR = 5;
+
+// RX, RY: window radii (compile time, so every bit position is a constant).
+template <int RX, int RY>
+__global__ void __launch_bounds__(kCensusBx * kCensusBy) census_texture_kernel(CensusArgs args) {
+  constexpr int TW = kCensusBx + 2 * RX, TH = kCensusBy + 2 * RY;
+  __shared__ uint8_t tile[TH][TW];
   const CensusImage& im = args.image[blockIdx.z];
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
-  int w = args.w, h = args.h;
+  const int w = args.w, h = args.h;
+  const int bx0 = blockIdx.x * kCensusBx, by0 = blockIdx.y * kCensusBy;
+  for (int i = threadIdx.y * kCensusBx + threadIdx.x; i < TW * TH; i += kCensusBx * kCensusBy) {
+    const int ty = i / TW, tx = i % TW;
+    const int gx = bx0 - RX + tx, gy = by0 - RY + ty;
+    tile[ty][tx] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? im.img[(int64_t)gy * w + gx] : 0;
+  }
+  __syncthreads();
+  const int x = bx0 + threadIdx.x, y = by0 + threadIdx.y;
   if (x >= w || y >= h) return;
-  int rx = args.wx / 2, ry = args.wy / 2;
-  int64_t n = (int64_t)w * h, p = (int64_t)y * w + x;
+  const int64_t n = (int64_t)w * h, p = (int64_t)y * w + x;
   uint64_t w0 = 0, w1 = 0;
   uint8_t textured = 0;
-  if (x >= rx && x < w - rx && y >= ry && y < h - ry) {
-    int center = im.img[p], bit = 0, low = 255, high = 0;
-    for (int yy = -ry; yy <= ry; yy++) {
-      const uint8_t* row = im.img + (int64_t)(y + yy) * w + x;
-      for (int xx = -rx; xx <= rx; xx++) {
-        int v = row[xx];
+  if (x >= RX && x < w - RX && y >= RY && y < h - RY) {
+    const uint8_t* c = &tile[threadIdx.y + RY][threadIdx.x + RX];
+    const int center = *c;
+    int low = 255, high = 0;
+#pragma unroll
+    for (int yy = -RY; yy <= RY; yy++) {
+#pragma unroll
+      for (int xx = -RX; xx <= RX; xx++) {
+        const int v = c[yy * TW + xx];
         low = min(low, v);
         high = max(high, v);
-        if (xx == 0 && yy == 0) continue;
-        if (v < center) {
-          if (bit < 64)
-            w0 |= 1ull << bit;
-          else
-            w1 |= 1ull << (bit - 64);
-        }
-        bit++;
+        // Row-major bit index over the window, skipping the centre (CensusSgm.java:545-552).
+        const int idx = (yy + RY) * (2 * RX + 1) + (xx + RX);
+        const int center_idx = RY * (2 * RX + 1) + RX;
+        if (idx == center_idx) continue;
+        const int bit = idx < center_idx ? idx : idx - 1;
+        const uint64_t set = v < center ? 1ull : 0ull;
+        if (bit < 64)
+          w0 |= set << bit;
+        else
+          w1 |= set << (bit - 64);
       }
     }
     textured = high - low >= 4 && (im.valid == nullptr || im.valid[p] != 0);
@@ -283,8 +300,24 @@ static int grid_for(int64_t work, int threads, int max_blocks) {
 }
 
 cudaError_t launch_census_texture(const CensusArgs& a, int images, cudaStream_t stream) {
-  dim3 block(32, 8), grid((a.w + 31) / 32, (a.h + 7) / 8, images);
-  census_texture_kernel<<<grid, block, 0, stream>>>(a);
+  dim3 block(kCensusBx, kCensusBy);
+  dim3 grid((a.w + kCensusBx - 1) / kCensusBx, (a.h + kCensusBy - 1) / kCensusBy, images);
+  const int rx = a.wx / 2, ry = a.wy / 2;
+  if (rx < 1 || rx > kCensusMaxR || ry < 1 || ry > kCensusMaxR) return cudaErrorInvalidValue;
+  using Kernel = void (*)(CensusArgs);
+  // [rx - 1][ry - 1]
+  static const Kernel table[5][5] = {
+      {census_texture_kernel<1, 1>, census_texture_kernel<1, 2>, census_texture_kernel<1, 3>,
+       census_texture_kernel<1, 4>, census_texture_kernel<1, 5>},
+      {census_texture_kernel<2, 1>, census_texture_kernel<2, 2>, census_texture_kernel<2, 3>,
+       census_texture_kernel<2, 4>, census_texture_kernel<2, 5>},
+      {census_texture_kernel<3, 1>, census_texture_kernel<3, 2>, census_texture_kernel<3, 3>,
+       census_texture_kernel<3, 4>, census_texture_kernel<3, 5>},
+      {census_texture_kernel<4, 1>, census_texture_kernel<4, 2>, census_texture_kernel<4, 3>,
+       census_texture_kernel<4, 4>, census_texture_kernel<4, 5>},
+      {census_texture_kernel<5, 1>, census_texture_kernel<5, 2>, census_texture_kernel<5, 3>,
+       census_texture_kernel<5, 4>, census_texture_kernel<5, 5>}};
+  table[rx - 1][ry - 1]<<<grid, block, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
