@@ -68,6 +68,18 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-suspending probe of an mbarrier phase.
+__device__ __forceinline__ bool mbar_probe(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
@@ -87,9 +99,10 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 // drain, which must see its copies land).  A wait that runs out stores `code` (the wait site:
 // 1 sweep cost chunk, 3 carry chunk, 4 selection tile, 5 drain; the sweep's producer warp
 // stores 6 when it made no progress for the limit).
+__device__ __forceinline__ bool mbar_probe(uint64_t* bar, uint32_t parity);
 __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
                                          long long limit, int code, bool shortcut = true) {
-  if (mbar_test(bar, parity)) return;  // the common case: the copy has landed
+  if (mbar_probe(bar, parity)) return;  // the common case: the copy has landed
   const long long start = clock64();
   for (unsigned spin = 1;; spin++) {
     if (mbar_test(bar, parity)) return;
@@ -403,8 +416,9 @@ struct SweepLayout {
   static constexpr int RING = 4;        // ring slots between consecutive row warps
   static constexpr int NB = 4;          // cost chunk slots per row warp
   static constexpr int CS = 4;          // carry chunk slots
-  // One pixel's vertical path states: NV x Dp u16x2, then the NV packed minima.
-  static constexpr int vslot = NV * Dp * 4 + 16;
+  // One pixel's vertical path states, normalised (L - min L, so the successor needs no
+  // minimum): NV x Dp u16x2.
+  static constexpr int vslot = NV * Dp * 4;
   // One cost chunk: K x Dp cost bytes of the left view, of the right view, K penalty records.
   static constexpr int cslot = K * (2 * Dp + 16);
   static constexpr int bars = 0;                            // cost_full[R][NB], carry_full[CS]
@@ -508,18 +522,21 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// Path `path` of one pixel slot (vslot layout) for this lane.
-template <int REGS, int NV>
+// Path `path` of one pixel slot (vslot layout) for this lane: a normalised state (minimum 0).
+template <int REGS>
 __device__ __forceinline__ void load_path(const uint8_t* pixel, int path, int lane,
                                           PathState<REGS>& s) {
   load_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, s.v);
-  s.m = ((const uint32_t*)(pixel + NV * 32 * REGS * 4))[path];
+  s.m = 0;
 }
-template <int REGS, int NV>
+// Stores L - min L of state s (no borrow: every half is at least its minimum), ANDed with keep.
+template <int REGS>
 __device__ __forceinline__ void store_path(uint8_t* pixel, int path, int lane,
-                                           const PathState<REGS>& s) {
-  store_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, s.v);
-  if (lane == 0) ((uint32_t*)(pixel + NV * 32 * REGS * 4))[path] = s.m;
+                                           const PathState<REGS>& s, uint32_t keep) {
+  uint32_t d[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) d[j] = (s.v[j] - s.m) & keep;
+  store_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, d);
 }
 
 // This lane's costs of both views as packed u16 pairs: byte j of each view widened, 0x80 -> 512,
@@ -601,7 +618,7 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
   }
 }
 
-// One CTA = R row warps + 1 producer warp, one row block of one stream.
+// One CTA = R row warps + a carry-in warp + a publisher warp, one row block of one stream.
 //  * "down" (stream 0) runs rows top to bottom and pixels left to right and owns the paths whose
 //    predecessor lies above or to the left: (1,0), (0,1), (1,1), (-1,1); "up" (stream 1) is the
 //    same code on the image mirrored in x and y and owns the four opposite paths.
@@ -610,13 +627,13 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
 //    a pixel reach the next row through a shared-memory ring; the (1,0) state stays in registers.
 //  * Each row warp bulk-copies its own cost chunks (both views + penalty records) NB chunks
 //    ahead; the last row warp also stores its vertical states as the block's carry row.
-//  * The producer warp fetches the previous block's carry row chunk by chunk once its progress
-//    counter covers the chunk, and publishes this block's carry progress (a GPU-scope fence off
-//    the row warps' critical path).
+//  * The carry-in warp fetches the previous block's carry row chunk by chunk once its progress
+//    counter covers the chunk; the publisher warp advances this block's progress counter after a
+//    GPU-scope fence (both off the row warps' critical path).
 //  * CTAs take tickets in launch order and only wait on lower tickets, so the schedule cannot
 //    deadlock even when not every CTA is resident.
 template <int REGS, int NPATH, int K, int R>
-__global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) {
+__global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   using L = SweepLayout<REGS, NPATH, K, R>;
   constexpr int Dp = L::Dp, NV = L::NV, RING = L::RING, NB = L::NB, CS = L::CS;
@@ -649,44 +666,31 @@ __global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) 
   auto chunk_n = [&](int c) { return min(K, W - c * K); };
 
   if (w == R) {
-    // ------------------------------------------------------------------ producer warp
-    if (lane != 0) return;
-    int next_carry = b > 0 ? 0 : nchunks;
-    int done_pub = has_next ? 0 : nchunks;
+    // --------------------------------------------------------------- carry-in warp
+    // Copies the previous block's carry row into the carry ring as soon as its progress counter
+    // covers a chunk, every covered chunk at once.
+    if (lane != 0 || b == 0) return;
     const int* prev_progress = &a.progress[stream * a.nb + b - 1];
-    int* my_progress = &a.progress[stream * a.nb + b];
     const uint8_t* carry_in = a.carry + (int64_t)(stream * a.nb + b - 1) * W * L::vslot;
+    int next_carry = 0, prev_seen = 0;
     long long last = clock64();
-    int prev_seen = 0;  // last progress value read from the previous block
-    while (next_carry < nchunks || done_pub < nchunks) {
-      bool did = false;
-      if (next_carry < nchunks) {
-        const int ch = next_carry;
-        if (ch - ld_acquire_cta(carry_consumed) < CS &&
-            (prev_seen >= min(W, (ch + 1) * K) ||
-             (prev_seen = ld_relaxed_gpu(prev_progress)) >= min(W, (ch + 1) * K))) {
-          fence_acq_rel_gpu();  // the carry data behind the observed progress is visible
-          fence_proxy_async_global();
-          fence_proxy_async_shared();
+    while (next_carry < nchunks) {
+      const int room = ld_acquire_cta(carry_consumed) + CS;  // chunks below this fit the ring
+      if (next_carry < room && prev_seen < min(W, (next_carry + 1) * K))
+        prev_seen = ld_relaxed_gpu(prev_progress);
+      const int avail = min(min(room, nchunks), prev_seen >= W ? nchunks : prev_seen / K);
+      if (next_carry < avail) {
+        fence_acq_rel_gpu();  // the carry data behind the observed progress is visible
+        fence_proxy_async_global();
+        fence_proxy_async_shared();
+        for (; next_carry < avail; next_carry++) {
+          const int ch = next_carry;
           uint64_t* bar = &carry_full[ch % CS];
           const uint32_t bytes = (uint32_t)(chunk_n(ch) * L::vslot);
           mbar_expect_tx(bar, bytes);
           bulk_copy(carry_buf + (ch % CS) * K * L::vslot, carry_in + (int64_t)ch * K * L::vslot,
                     bytes, bar);
-          next_carry = ch + 1;
-          did = true;
         }
-      }
-      if (done_pub < nchunks) {
-        const int done = ld_acquire_cta(published);
-        if (done > done_pub) {
-          __threadfence();  // the carry rows the row warp wrote are visible GPU-wide first
-          atomicExch(my_progress, min(W, done * K));
-          done_pub = done;
-          did = true;
-        }
-      }
-      if (did) {
         last = clock64();
       } else {
         if (*(volatile int*)err) break;
@@ -694,13 +698,38 @@ __global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) 
           atomicExch(err, 6);
           break;
         }
-        __nanosleep(128);  // a chunk takes K steps of several hundred cycles each
+        __nanosleep(32);
       }
     }
     // Every issued carry copy lands before the CTA's shared memory is released.
-    if (b > 0)
-      for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
-        wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, limit / 4, 5, false);
+    for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
+      wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, limit / 4, 5, false);
+    return;
+  }
+  if (w == R + 1) {
+    // --------------------------------------------------------------- publisher warp
+    // Makes the carry chunks the last row warp has written visible GPU-wide, then advances this
+    // block's progress counter (the fence stays off the row warps' critical path).
+    if (lane != 0 || !has_next) return;
+    int* my_progress = &a.progress[stream * a.nb + b];
+    int done_pub = 0;
+    long long last = clock64();
+    while (done_pub < nchunks) {
+      const int done = ld_acquire_cta(published);
+      if (done > done_pub) {
+        __threadfence();
+        atomicExch(my_progress, min(W, done * K));
+        done_pub = done;
+        last = clock64();
+      } else {
+        if (*(volatile int*)err) break;
+        if (clock64() - last > limit) {
+          atomicExch(err, 6);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
     return;
   }
 
@@ -784,19 +813,19 @@ __global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) 
       const uint4 pw = *pb;
       PathState<REGS> prev[NPATH];
       prev[0] = horiz;
-      load_path<REGS, NV>(up_base + (xs & up_mask) * L::vslot, 0, lane, prev[1]);
+      load_path<REGS>(up_base + (xs & up_mask) * L::vslot, 0, lane, prev[1]);
       if constexpr (NPATH > 2) {
         const uint8_t* pd = xs > 0 ? up_base + ((xs - 1) & up_mask) * L::vslot : zero;
         const uint8_t* pa = xs + 1 < W ? up_base + ((xs + 1) & up_mask) * L::vslot : zero;
-        load_path<REGS, NV>(pd, 1, lane, prev[2]);
-        load_path<REGS, NV>(pa, 2, lane, prev[3]);
+        load_path<REGS>(pd, 1, lane, prev[2]);
+        load_path<REGS>(pa, 2, lane, prev[3]);
       }
       uint32_t q[NPATH];
       q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
-      q[1] = prev[1].m + pw.y;
+      q[1] = pw.y;  // normalised predecessors: minimum 0
       if constexpr (NPATH > 2) {
-        q[2] = prev[2].m + pw.z;
-        q[3] = prev[3].m + pw.w;
+        q[2] = pw.z;
+        q[3] = pw.w;
       }
       PathState<REGS> out[NPATH];
       paths_step<REGS, NPATH>(prev, q, p1x2, cst, lo_edge, hi_edge, out);
@@ -812,21 +841,18 @@ __global__ void __launch_bounds__((R + 1) * 32) sweep_kernel(const SweepArgs a) 
       store_words_cs<REGS>(sum_px + xs * sum_step, s);
       // Successors of an untextured pixel start afresh (CensusSgm.java:432-433): they see zeros.
       const uint32_t keep = prmt(pw.x, 0, 0xbb99u);
-      if (keep != 0xffffffffu) {
-#pragma unroll
-        for (int i = 0; i < NPATH; i++) {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) out[i].v[j] &= keep;
-          out[i].m &= keep;
-        }
-      }
       uint8_t* o = ring_mine + (xs & (RING - 1)) * L::vslot;
 #pragma unroll
-      for (int i = 0; i < NV; i++) store_path<REGS, NV>(o, i, lane, out[i + 1]);
+      for (int i = 0; i < NV; i++) store_path<REGS>(o, i, lane, out[i + 1], keep);
       if constexpr (PUBLISH) {
         uint8_t* g = carry_out + (int64_t)xs * L::vslot;
 #pragma unroll
-        for (int i = 0; i < NV; i++) store_path<REGS, NV>(g, i, lane, out[i + 1]);
+        for (int i = 0; i < NV; i++) store_path<REGS>(g, i, lane, out[i + 1], keep);
+      }
+      if (keep != 0xffffffffu) {
+#pragma unroll
+        for (int j = 0; j < REGS; j++) out[0].v[j] &= keep;
+        out[0].m &= keep;
       }
       horiz = out[0];
       (void)off;
@@ -1056,10 +1082,12 @@ cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
 template <int REGS, int NPATH, int K, int R>
 cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
   auto kernel = sweep_kernel<REGS, NPATH, K, R>;
-  const int shared = SweepLayout<REGS, NPATH, K, R>::total;
+  // At least 116 KB so that one CTA holds an SM alone: two row blocks on one SM halve each
+  // other's step rate, while a later block never needs an SM before an earlier one finishes.
+  const int shared = std::max(SweepLayout<REGS, NPATH, K, R>::total, 116 * 1024);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
-  kernel<<<2 * a.nb, (R + 1) * 32, shared, stream>>>(a);
+  kernel<<<2 * a.nb, (R + 2) * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -1086,7 +1114,7 @@ struct FusedLayout {
     rows = rows_for(Dp / 32);
     nb = (h + rows - 1) / rows;
     const int nv = p.directions == 8 ? 3 : 1;
-    vslot = nv * Dp * 4 + 16;
+    vslot = nv * Dp * 4;
     size_t n = (size_t)w * h;
     cost = n * Dp;
     sum = n * Dp * 4;
