@@ -415,7 +415,7 @@ struct SweepLayout {
   static constexpr int NV = NPATH - 1;  // paths whose predecessor lies in the row above
   static constexpr int RING = 4;        // ring slots between consecutive row warps
   static constexpr int NB = 4;          // cost chunk slots per row warp
-  static constexpr int CS = 4;          // carry chunk slots
+  static constexpr int CS = 16 / K;     // carry chunk slots (16 pixels)
   // One pixel's vertical path states, normalised (L - min L, so the successor needs no
   // minimum): NV x Dp u16x2.
   static constexpr int vslot = NV * Dp * 4;
@@ -1093,7 +1093,7 @@ cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
 
 // Rows per sweep CTA: few enough that the rows of a block (all busy at once) spread over SMs,
 // many enough that the carry hand-off between blocks stays rare.
-constexpr int kChunk = 4;
+constexpr int kChunk = 2;  // pixels per cost chunk and per carry publication
 constexpr int rows_default(int regs) { return regs >= 8 ? 4 : 8; }
 
 // Rows per sweep CTA: the default, or CSGM_SWEEP_ROWS (4 or 8) for tuning runs.
