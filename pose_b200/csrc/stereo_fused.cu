@@ -509,6 +509,67 @@ __device__ __forceinline__ void store_words_cs(uint32_t* p, const uint32_t (&v)[
   }
 }
 
+// Shared-memory loads and stores through 32-bit shared-window addresses (volatile, so they keep
+// their order relative to the barriers and mbarrier waits around them).
+__device__ __forceinline__ uint32_t lds_u16(uint32_t a) {
+  unsigned short v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint2 lds_v2(uint32_t a) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint4 lds_v4(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts_v2(uint32_t a, uint32_t x, uint32_t y) {
+  asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(a), "r"(x), "r"(y));
+}
+__device__ __forceinline__ void sts_v4(uint32_t a, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(x), "r"(y), "r"(z), "r"(w));
+}
+template <int REGS>
+__device__ __forceinline__ void lds_words(uint32_t a, uint32_t (&v)[REGS]) {
+  if constexpr (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4) {
+      const uint4 t = lds_v4(a + 4 * j);
+      v[j] = t.x;
+      v[j + 1] = t.y;
+      v[j + 2] = t.z;
+      v[j + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 2) {
+      const uint2 t = lds_v2(a + 4 * j);
+      v[j] = t.x;
+      v[j + 1] = t.y;
+    }
+  }
+}
+template <int REGS>
+__device__ __forceinline__ void sts_words(uint32_t a, const uint32_t (&v)[REGS]) {
+  if constexpr (REGS % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 4) sts_v4(a + 4 * j, v[j], v[j + 1], v[j + 2], v[j + 3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < REGS; j += 2) sts_v2(a + 4 * j, v[j], v[j + 1]);
+  }
+}
+
 template <int REGS>
 struct PathState {
   uint32_t v[REGS];
@@ -522,45 +583,41 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// Path `path` of one pixel slot (vslot layout) for this lane: a normalised state (minimum 0).
+// Path `path` of one pixel slot (vslot layout) for this lane (`lane_slot` = the pixel slot's
+// shared address plus this lane's offset): a normalised state (minimum 0).
 template <int REGS>
-__device__ __forceinline__ void load_path(const uint8_t* pixel, int path, int lane,
-                                          PathState<REGS>& s) {
-  load_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, s.v);
+__device__ __forceinline__ void load_path(uint32_t lane_slot, int path, PathState<REGS>& s) {
+  lds_words<REGS>(lane_slot + path * (32 * REGS * 4), s.v);
   s.m = 0;
 }
-// Stores L - min L of state s (no borrow: every half is at least its minimum), ANDed with keep.
+// L - min L of state s (no borrow: every half is at least its minimum), ANDed with keep.
 template <int REGS>
-__device__ __forceinline__ void store_path(uint8_t* pixel, int path, int lane,
-                                           const PathState<REGS>& s, uint32_t keep) {
-  uint32_t d[REGS];
+__device__ __forceinline__ void normalise(const PathState<REGS>& s, uint32_t keep,
+                                          uint32_t (&d)[REGS]) {
 #pragma unroll
   for (int j = 0; j < REGS; j++) d[j] = (s.v[j] - s.m) & keep;
-  store_words<REGS>(pixel + path * (32 * REGS * 4) + lane * REGS * 4, d);
 }
 
 // This lane's costs of both views as packed u16 pairs: byte j of each view widened, 0x80 -> 512,
 // and pad[j] ORed in (disparities >= D are lifted to 0x1200 so they never win a minimum).
 template <int REGS>
-__device__ __forceinline__ void widen_costs(const uint8_t* c0, const uint8_t* c1,
-                                            const uint32_t (&pad)[REGS], uint32_t (&c)[REGS]) {
+__device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint32_t (&pad)[REGS],
+                                            uint32_t (&c)[REGS]) {
   constexpr int NW = (REGS + 3) / 4;
   uint32_t a[NW], b[NW];
   if constexpr (REGS == 2) {
-    a[0] = *(const uint16_t*)c0;
-    b[0] = *(const uint16_t*)c1;
+    a[0] = lds_u16(c0);
+    b[0] = lds_u16(c1);
   } else if constexpr (REGS == 4) {
-    a[0] = *(const uint32_t*)c0;
-    b[0] = *(const uint32_t*)c1;
+    a[0] = lds_u32(c0);
+    b[0] = lds_u32(c1);
   } else if constexpr (REGS == 6) {
-    const uint16_t* h0 = (const uint16_t*)c0;
-    const uint16_t* h1 = (const uint16_t*)c1;
-    a[0] = (uint32_t)h0[0] | ((uint32_t)h0[1] << 16);
-    a[1] = h0[2];
-    b[0] = (uint32_t)h1[0] | ((uint32_t)h1[1] << 16);
-    b[1] = h1[2];
+    a[0] = lds_u16(c0) | (lds_u16(c0 + 2) << 16);
+    a[1] = lds_u16(c0 + 4);
+    b[0] = lds_u16(c1) | (lds_u16(c1 + 2) << 16);
+    b[1] = lds_u16(c1 + 4);
   } else {
-    const uint2 t0 = *(const uint2*)c0, t1 = *(const uint2*)c1;
+    const uint2 t0 = lds_v2(c0), t1 = lds_v2(c1);
     a[0] = t0.x;
     a[1] = t0.y;
     b[0] = t1.x;
@@ -745,24 +802,31 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   const bool publish = w == R - 1 && has_next;
   uint8_t* my_slots = smem + L::cost + w * NB * L::cslot;
   uint64_t* my_full = full + w * NB;
-  uint8_t* ring_mine = smem + L::ring + w * RING * L::vslot;
-  const uint8_t* zero = smem + L::zero;
+  // Shared-window addresses (32-bit), this lane's offset inside a pixel slot folded in.
+  const uint32_t sm0 = smem_u32(smem);
+  const uint32_t lane_off = lane * REGS * 4;
+  const uint32_t slots_a = sm0 + L::cost + w * NB * L::cslot;
+  const uint32_t ring_a = sm0 + L::ring + w * RING * L::vslot + lane_off;
+  const uint32_t zero_a = sm0 + L::zero + lane_off;
   // Predecessor row: the ring of the warp above, the carry buffer, or (first image row) the zero
   // slot for every pixel.
-  const uint8_t* up_base = yp == 0     ? zero
-                           : use_carry ? carry_buf
-                                       : smem + L::ring + (w - 1) * RING * L::vslot;
+  const uint32_t up_a = (yp == 0     ? sm0 + L::zero
+                         : use_carry ? sm0 + L::carry
+                                     : sm0 + L::ring + (w - 1) * RING * L::vslot) +
+                        lane_off;
   const int up_mask = yp == 0 ? 0 : use_carry ? CS * K - 1 : RING - 1;
   uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
   const uint8_t* cost_row0 = a.cost[0] + (int64_t)y * W * Dp;
   const uint8_t* cost_row1 = a.cost[1] + (int64_t)y * W * Dp;
   const uint4* pen_row = a.pen + ((int64_t)stream * H + yp) * W;
-  // Partial aggregate of stream pixel xs: sum_px + xs * sum_step (this lane's words).
-  uint32_t* sum_px = (stream ? a.sum[1] : a.sum[0]) + ((int64_t)y * W + (mirror ? W - 1 : 0)) * Dp + lane * REGS;
-  const int64_t sum_step = mirror ? -(int64_t)Dp : (int64_t)Dp;
+  // Partial aggregate of the current stream pixel (this lane's words), advanced by sum_step.
+  uint32_t* sum_ptr = (stream ? a.sum[1] : a.sum[0]) + ((int64_t)y * W + (mirror ? W - 1 : 0)) * Dp +
+                      lane * REGS;
+  const int sum_step = mirror ? -Dp : Dp;
   // Cost bytes of chunk pixel `off` sit at slot + cost_first + off * cost_step (image order).
   const int cost_first_full = (mirror ? (K - 1) * Dp : 0) + lane * REGS;
   const int cost_step = mirror ? -Dp : Dp;
+  uint8_t* carry_ptr = carry_out + lane_off;  // this row's carry slot of the current pixel
 
   auto issue_chunk = [&](int c) {  // lane 0
     const int n = chunk_n(c);
@@ -806,19 +870,20 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
         carry_ready++;
       }
     };
-    // One pixel: xs (stream column), off (index in the chunk), costs at cb, penalties at pb.
-    auto pixel = [&](int xs, int off, const uint8_t* cb, const uint4* pb) {
+    // One pixel: xs (stream column); cb = shared address of this lane's left-view cost bytes,
+    // pb = shared address of the pixel's penalty record.
+    auto pixel = [&](int xs, uint32_t cb, uint32_t pb) {
       uint32_t cst[REGS];
       widen_costs<REGS>(cb, cb + K * Dp, pad, cst);
-      const uint4 pw = *pb;
+      const uint4 pw = lds_v4(pb);
       PathState<REGS> prev[NPATH];
       prev[0] = horiz;
-      load_path<REGS>(up_base + (xs & up_mask) * L::vslot, 0, lane, prev[1]);
+      load_path<REGS>(up_a + (xs & up_mask) * L::vslot, 0, prev[1]);
       if constexpr (NPATH > 2) {
-        const uint8_t* pd = xs > 0 ? up_base + ((xs - 1) & up_mask) * L::vslot : zero;
-        const uint8_t* pa = xs + 1 < W ? up_base + ((xs + 1) & up_mask) * L::vslot : zero;
-        load_path<REGS>(pd, 1, lane, prev[2]);
-        load_path<REGS>(pa, 2, lane, prev[3]);
+        const uint32_t pd = xs > 0 ? up_a + ((xs - 1) & up_mask) * L::vslot : zero_a;
+        const uint32_t pa = xs + 1 < W ? up_a + ((xs + 1) & up_mask) * L::vslot : zero_a;
+        load_path<REGS>(pd, 1, prev[2]);
+        load_path<REGS>(pa, 2, prev[3]);
       }
       uint32_t q[NPATH];
       q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
@@ -838,24 +903,35 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
         for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
         s[j] = acc;
       }
-      store_words_cs<REGS>(sum_px + xs * sum_step, s);
-      // Successors of an untextured pixel start afresh (CensusSgm.java:432-433): they see zeros.
+      store_words_cs<REGS>(sum_ptr, s);
+      sum_ptr += sum_step;
+      // The row below gets normalised states; successors of an untextured pixel start afresh
+      // (CensusSgm.java:432-433): they see zeros.
       const uint32_t keep = prmt(pw.x, 0, 0xbb99u);
-      uint8_t* o = ring_mine + (xs & (RING - 1)) * L::vslot;
+      const uint32_t o = ring_a + (xs & (RING - 1)) * L::vslot;
+      if (keep == 0xffffffffu) {
 #pragma unroll
-      for (int i = 0; i < NV; i++) store_path<REGS>(o, i, lane, out[i + 1], keep);
-      if constexpr (PUBLISH) {
-        uint8_t* g = carry_out + (int64_t)xs * L::vslot;
+        for (int i = 0; i < NV; i++) {
+          uint32_t d[REGS];
 #pragma unroll
-        for (int i = 0; i < NV; i++) store_path<REGS>(g, i, lane, out[i + 1], keep);
-      }
-      if (keep != 0xffffffffu) {
+          for (int j = 0; j < REGS; j++) d[j] = out[i + 1].v[j] - out[i + 1].m;
+          sts_words<REGS>(o + i * (Dp * 4), d);
+          if constexpr (PUBLISH) store_words<REGS>(carry_ptr + i * (Dp * 4), d);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+          uint32_t d[REGS];
+          normalise<REGS>(out[i + 1], keep, d);
+          sts_words<REGS>(o + i * (Dp * 4), d);
+          if constexpr (PUBLISH) store_words<REGS>(carry_ptr + i * (Dp * 4), d);
+        }
 #pragma unroll
         for (int j = 0; j < REGS; j++) out[0].v[j] &= keep;
         out[0].m &= keep;
       }
+      if constexpr (PUBLISH) carry_ptr += L::vslot;
       horiz = out[0];
-      (void)off;
     };
     // End of chunk c: refill its slot NB chunks ahead, report carry progress / release.
     auto end_chunk = [&](int c) {
@@ -872,14 +948,13 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
     for (int c = 0; c < full_chunks; c++) {
       wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
       if constexpr (CARRY_IN) wait_carry(c);
-      const uint8_t* slot = my_slots + (c % NB) * L::cslot;
-      const uint4* pens = (const uint4*)(slot + 2 * K * Dp);
+      const uint32_t slot = slots_a + (c % NB) * L::cslot;
 #pragma unroll
       for (int off = 0; off < K; off++) {
         if constexpr (CARRY_IN) {
           if (off == K - 1) wait_carry(c + 1);
         }
-        pixel(c * K + off, off, slot + cost_first_full + off * cost_step, pens + off);
+        pixel(c * K + off, slot + cost_first_full + off * cost_step, slot + 2 * K * Dp + 16 * off);
         rows_barrier(R * 32);
       }
       end_chunk(c);
@@ -889,11 +964,10 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
       const int c = full_chunks, n = W - c * K;
       wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
       if constexpr (CARRY_IN) wait_carry(c);
-      const uint8_t* slot = my_slots + (c % NB) * L::cslot;
-      const uint4* pens = (const uint4*)(slot + 2 * K * Dp);
+      const uint32_t slot = slots_a + (c % NB) * L::cslot;
       const int first = (mirror ? (n - 1) * Dp : 0) + lane * REGS;
       for (int off = 0; off < n; off++) {
-        pixel(c * K + off, off, slot + first + off * cost_step, pens + off);
+        pixel(c * K + off, slot + first + off * cost_step, slot + 2 * K * Dp + 16 * off);
         rows_barrier(R * 32);
       }
       end_chunk(c);
