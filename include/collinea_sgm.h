@@ -245,6 +245,46 @@ int csgm_pair_device(csgm_session* session, const csgm_params* params, const uin
                      uint8_t* reasons, uint8_t* boundary, csgm_stats* stats, int32_t sync);
 
 /*
+ * Batched and served pairs.  No counterpart in the reference, which matches one pair per call and
+ * keeps one session per Java thread (src/main/java/sgm/GpuSgm.java:22,163-303); every result is
+ * bit-identical to csgm_pair on the same inputs.
+ *
+ * csgm_batch_configure: gives the session `slots` pair slots (1..64), each with its own CUDA stream
+ * and a device workspace that stays resident between pairs, and a device-memory budget for all
+ * of them (0 = 70% of device memory).  Fails with CSGM_E_BUSY while requests are in flight.
+ */
+int csgm_batch_configure(csgm_session* session, int32_t slots, int64_t budget_bytes);
+
+/*
+ * Queues one pair (arguments as csgm_pair) on a free slot and returns at once with *request set.
+ * Host buffers must stay valid until csgm_batch_poll reports the request finished; pinned host
+ * memory lets uploads and downloads overlap other pairs' kernels.  Admission: the workspace bytes
+ * of the pairs in flight (cost volumes and aggregates, W*H*D based, plus images and outputs) and
+ * this pair's must fit the budget, and a slot must be free; otherwise CSGM_E_BUSY and nothing is
+ * queued (submit again after a poll).  CSGM_E_NOMEM: the pair alone exceeds the budget.
+ */
+int csgm_batch_submit(csgm_session* session, const csgm_params* params, const uint8_t* left,
+                      const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
+                      int32_t w, int32_t h, float* lr_checked, float* disp_l, float* disp_r,
+                      uint8_t* reasons, uint8_t* boundary, int64_t* request);
+
+/*
+ * Collects a request: CSGM_OK once its outputs are in the caller's buffers (stats as csgm_pair),
+ * CSGM_E_BUSY while it is still running (wait == 0), or the pair's own error status.  Waiting does
+ * not hold the session lock: other threads may submit meanwhile.
+ */
+int csgm_batch_poll(csgm_session* session, int64_t request, int32_t wait, csgm_stats* stats);
+
+/* Requests in flight, bytes admitted for them, bytes of resident slot workspaces. */
+int csgm_batch_status(csgm_session* session, int32_t* in_flight, int64_t* reserved_bytes,
+                      int64_t* resident_bytes);
+
+/* Page-locked host memory (cudaMallocHost) for batch inputs and outputs; csgm_host_free releases
+ * it.  No counterpart in the reference (its FFM arenas are pageable). */
+int csgm_host_alloc(int64_t bytes, void** ptr);
+void csgm_host_free(void* ptr);
+
+/*
  * Left-right check that allocates nothing; no counterpart in the reference, whose check
  * (src/main/java/sgm/CensusSgm.java:181-201) always runs inside the matcher.  Same results as the
  * check inside csgm_pair: lr_checked[p] keeps disp_l[p] where the right view agrees within

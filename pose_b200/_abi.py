@@ -160,10 +160,24 @@ SIGNATURES = {
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
          ctypes.POINTER(CsgmStats)],
-    ),    "csgm_lr_check_noalloc": (
+    ),
+    "csgm_lr_check_noalloc": (
         ctypes.c_int,
         [_P, _P, _I32, _I32, _I32, _I32, ctypes.c_double, _P, _P, _P, _P],
     ),
+    "csgm_batch_configure": (ctypes.c_int, [_P, _I32, _I64]),
+    "csgm_batch_submit": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
+         ctypes.POINTER(_I64)],
+    ),
+    "csgm_batch_poll": (ctypes.c_int, [_P, _I64, _I32, ctypes.POINTER(CsgmStats)]),
+    "csgm_batch_status": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+    ),
+    "csgm_host_alloc": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),
+    "csgm_host_free": (None, [_P]),
 }
 
 

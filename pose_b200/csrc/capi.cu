@@ -50,7 +50,10 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return b.ptr;
   if (b.ptr) {
-    cudaFree(b.ptr);
+    if (async_stream)
+      cudaFreeAsync(b.ptr, async_stream);
+    else
+      cudaFree(b.ptr);
     allocated -= b.bytes;
     b.ptr = nullptr;
     b.bytes = 0;
@@ -60,7 +63,7 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
                    (allocated + bytes) / 1048576.0, budget / 1048576.0);
     return nullptr;
   }
-  cudaError_t e = cudaMalloc(&b.ptr, bytes);
+  cudaError_t e = async_stream ? cudaMallocAsync(&b.ptr, bytes, async_stream) : cudaMalloc(&b.ptr, bytes);
   if (e != cudaSuccess) {
     *status = cuda_fail(e, "GPU buffer allocation");
     b.ptr = nullptr;
@@ -74,7 +77,10 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
 void Workspace::release_all() {
   for (auto& b : buffers)
     if (b.ptr) {
-      cudaFree(b.ptr);
+      if (async_stream)
+        cudaFreeAsync(b.ptr, async_stream);
+      else
+        cudaFree(b.ptr);
       b.ptr = nullptr;
       b.bytes = 0;
     }
@@ -138,17 +144,6 @@ Profiler::~Profiler() {
 }
 
 }  // namespace csgm
-
-struct csgm_session {
-  int device = 0;
-  int sm_count = 0;
-  size_t memory = 0;
-  cudaStream_t stream = nullptr;
-  std::mutex lock;
-  csgm::Workspace workspace;
-  csgm::Profiler profiler;
-  csgm_profile profile{};
-};
 
 using namespace csgm;
 
@@ -286,6 +281,7 @@ void csgm_session_close(csgm_session* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
+  release_batch_slots(s);
   s->workspace.release_all();
   cudaStreamDestroy(s->stream);
   delete s;  // destroys the profiler's events on the current device

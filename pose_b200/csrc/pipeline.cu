@@ -77,7 +77,7 @@ static int run_view_general(Context& ctx, const csgm_params& p, const uint64_t* 
   return CSGM_OK;
 }
 
-static void copy_stats(const DeviceStats& d, csgm_stats* out, bool add) {
+void copy_stats(const DeviceStats& d, csgm_stats* out, bool add) {
   if (!add) memset(out, 0, sizeof *out);
   out->lower_boundary_rejected += (int64_t)d.lower_boundary_rejected;
   out->full_interval_pixels += (int64_t)d.full_interval_pixels;
@@ -191,12 +191,22 @@ int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, con
                         reasons, boundary, stats, sync, true);
 }
 
-int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
-                  const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
-                  float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
-                  uint8_t* boundary, csgm_stats* stats) {
+// Uploads, device pipeline and downloads of a pair with host buffers, queued on ctx.stream.
+// pinned_stats (may be null) receives the selection counters; *host_d2h_stats says whether it was
+// queued.  Returns before the GPU has finished.
+static int queue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left,
+                           const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
+                           int w, int h, float* lr_checked, float* disp_l, float* disp_r,
+                           uint8_t* reasons, uint8_t* boundary, DeviceStats* stats_dst,
+                           cudaEvent_t* timing /* [4] or null */) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
+  // Reserve the pipeline's own buffers before the upload so a budget failure costs no copies.
+  int64_t needed = (int64_t)pair_workspace_bytes(p, w, h, true);
+  if ((size_t)needed > ctx.ws->budget)
+    return fail(CSGM_E_NOMEM,
+                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
+                needed / 1048576.0, ctx.ws->budget / 1048576.0);
   WS(d_left, uint8_t, kImgL, n);
   WS(d_right, uint8_t, kImgR, n);
   uint8_t *d_vl = nullptr, *d_vr = nullptr;
@@ -219,33 +229,18 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
     WS(b, uint8_t, kBoundary, n);
     d_boundary = b;
   }
-  // Reserve the pipeline's own buffers before the upload so a budget failure costs no copies.
-  int64_t needed = (int64_t)pair_workspace_bytes(p, w, h, true);
-  if ((size_t)needed > ctx.ws->budget)
-    return fail(CSGM_E_NOMEM,
-                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
-                needed / 1048576.0, ctx.ws->budget / 1048576.0);
-  cudaEvent_t u0 = nullptr, u1 = nullptr, d0 = nullptr, d1 = nullptr;
-  bool timed = ctx.prof->level >= 1;
-  ctx.prof->begin_call(ctx.stream);
-  if (timed) {
-    u0 = ctx.prof->event();
-    u1 = ctx.prof->event();
-    d0 = ctx.prof->event();
-    d1 = ctx.prof->event();
-    CK(cudaEventRecord(u0, ctx.stream), "event record");
-  }
+  if (timing) CK(cudaEventRecord(timing[0], ctx.stream), "event record");
   CK(cudaMemcpyAsync(d_left, left, n, cudaMemcpyHostToDevice, ctx.stream), "image upload");
   CK(cudaMemcpyAsync(d_right, right, n, cudaMemcpyHostToDevice, ctx.stream), "image upload");
   if (valid_l) {
     CK(cudaMemcpyAsync(d_vl, valid_l, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
     CK(cudaMemcpyAsync(d_vr, valid_r, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
   }
-  if (timed) CK(cudaEventRecord(u1, ctx.stream), "event record");
+  if (timing) CK(cudaEventRecord(timing[1], ctx.stream), "event record");
   status = pair_on_device(ctx, p, d_left, d_right, d_vl, d_vr, w, h, d_checked, d_dl, d_dr,
                           d_reasons, d_boundary, nullptr, false, false);
   if (status) return status;
-  if (timed) CK(cudaEventRecord(d0, ctx.stream), "event record");
+  if (timing) CK(cudaEventRecord(timing[2], ctx.stream), "event record");
   CK(cudaMemcpyAsync(lr_checked, d_checked, n * 4, cudaMemcpyDeviceToHost, ctx.stream),
      "disparity readback");
   if (disp_l)
@@ -256,18 +251,43 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
     CK(cudaMemcpyAsync(reasons, d_reasons, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
   if (boundary)
     CK(cudaMemcpyAsync(boundary, d_boundary, n, cudaMemcpyDeviceToHost, ctx.stream), "readback");
-  DeviceStats host{};
   WS(dstats, DeviceStats, kStats, sizeof(DeviceStats));
-  CK(cudaMemcpyAsync(&host, dstats, sizeof host, cudaMemcpyDeviceToHost, ctx.stream),
+  CK(cudaMemcpyAsync(stats_dst, dstats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, ctx.stream),
      "stats readback");
-  if (timed) CK(cudaEventRecord(d1, ctx.stream), "event record");
+  if (timing) CK(cudaEventRecord(timing[3], ctx.stream), "event record");
+  return CSGM_OK;
+}
+
+int enqueue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left,
+                      const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r, int w,
+                      int h, float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                      uint8_t* boundary, DeviceStats* host_stats) {
+  ctx.prof->begin_call(ctx.stream);
+  return queue_pair_host(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
+                         reasons, boundary, host_stats, nullptr);
+}
+
+int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
+                  const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
+                  float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                  uint8_t* boundary, csgm_stats* stats) {
+  size_t n = (size_t)w * h;
+  bool timed = ctx.prof->level >= 1;
+  ctx.prof->begin_call(ctx.stream);
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (timed)
+    for (auto& e : ev) e = ctx.prof->event();
+  DeviceStats host{};
+  int status = queue_pair_host(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
+                               disp_r, reasons, boundary, &host, timed ? ev : nullptr);
+  if (status) return status;
   CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
   if (host.pad) return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host.pad);
   if (stats) copy_stats(host, stats, false);
   if (timed) {
-    ctx.profile->upload_ns += (int64_t)(elapsed_ms(u0, u1) * 1e6);
-    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(u1, d0) * 1e6);
-    ctx.profile->download_ns += (int64_t)(elapsed_ms(d0, d1) * 1e6);
+    ctx.profile->upload_ns += (int64_t)(elapsed_ms(ev[0], ev[1]) * 1e6);
+    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(ev[1], ev[2]) * 1e6);
+    ctx.profile->download_ns += (int64_t)(elapsed_ms(ev[2], ev[3]) * 1e6);
     ctx.profile->uploaded_bytes += (int64_t)(valid_l ? 4 * n : 2 * n);
     ctx.profile->downloaded_bytes += (int64_t)(n * 4 * (1 + (disp_l != 0) + (disp_r != 0)) +
                                                (reasons ? n : 0) + (boundary ? n : 0));

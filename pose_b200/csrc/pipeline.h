@@ -5,9 +5,11 @@
 
 #include <cstdint>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "collinea_sgm.h"
+#include "sgm_device.cuh"
 
 namespace csgm {
 
@@ -30,6 +32,9 @@ struct Workspace {
   Buffer buffers[kSlotCount];
   size_t allocated = 0;
   size_t budget = 0;
+  // When set, buffers are allocated and freed stream-ordered on this stream (no device-wide
+  // synchronisation while other streams' kernels run).
+  cudaStream_t async_stream = nullptr;
   void* get(int slot, size_t bytes, int* status);
   void release_all();
 };
@@ -66,6 +71,20 @@ struct Context {
   Workspace* ws;
   Profiler* prof;
   csgm_profile* profile;
+  // One sweep CTA per SM (a lone pair runs fastest so); batched pairs share SMs instead.
+  bool exclusive_sweep = true;
+};
+
+// One batch slot: a pair in flight with its own stream and resident workspace.
+struct BatchSlot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  Workspace ws;
+  Profiler prof;
+  csgm_profile profile{};
+  DeviceStats* host_stats = nullptr;  // pinned
+  int64_t id = 0;                     // request in flight, 0 = free
+  size_t reserved = 0;                // bytes admitted for it
 };
 
 // Bytes of device workspace a pair needs (host_inputs: include the upload/download staging).
@@ -87,4 +106,34 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
                    float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
                    csgm_stats* stats);
 
+// Adds (add) or copies device selection counters into the ABI's stats record.
+void copy_stats(const DeviceStats& d, csgm_stats* out, bool add);
+
+// Queues a pair with host buffers on ctx.stream without waiting: uploads, the device pipeline,
+// downloads, and the selection counters into *host_stats (pinned).  The caller synchronises.
+int enqueue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left,
+                      const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r, int w,
+                      int h, float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                      uint8_t* boundary, DeviceStats* host_stats);
+
 }  // namespace csgm
+
+namespace csgm {
+struct BatchSlot;
+void release_batch_slots(csgm_session* s);
+}  // namespace csgm
+
+struct csgm_session {
+  int device = 0;
+  int sm_count = 0;
+  size_t memory = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex lock;
+  csgm::Workspace workspace;
+  csgm::Profiler profiler;
+  csgm_profile profile{};
+  // Batched / served pairs (batch.cu).
+  std::vector<csgm::BatchSlot> slots;
+  size_t batch_budget = 0;
+  int64_t next_request = 1;
+};

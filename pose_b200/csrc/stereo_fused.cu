@@ -1154,11 +1154,13 @@ cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
 }
 
 template <int REGS, int NPATH, int K, int R>
-cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream) {
+cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream, bool exclusive) {
   auto kernel = sweep_kernel<REGS, NPATH, K, R>;
-  // At least 116 KB so that one CTA holds an SM alone: two row blocks on one SM halve each
-  // other's step rate, while a later block never needs an SM before an earlier one finishes.
-  const int shared = std::max(SweepLayout<REGS, NPATH, K, R>::total, 116 * 1024);
+  // Exclusive: at least 116 KB so that one CTA holds an SM alone (two row blocks on one SM halve
+  // each other's step rate, while a later block never needs an SM before an earlier one
+  // finishes).  Batched pairs instead share SMs, filling each other's idle issue slots.
+  const int shared = exclusive ? std::max(SweepLayout<REGS, NPATH, K, R>::total, 116 * 1024)
+                               : SweepLayout<REGS, NPATH, K, R>::total;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
   kernel<<<2 * a.nb, (R + 2) * 32, shared, stream>>>(a);
@@ -1304,10 +1306,10 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   switch (regs * 4 + (eight ? 2 : 0) + (F.rows == 8 ? 1 : 0)) {
 #define CSGM_SWEEP_CASE(R_, NP_)                                                       \
   case R_ * 4 + (NP_ == 4 ? 2 : 0):                                                   \
-    e = launch_sweep<R_, NP_, kChunk, 4>(a, ctx.stream);                              \
+    e = launch_sweep<R_, NP_, kChunk, 4>(a, ctx.stream, ctx.exclusive_sweep);         \
     break;                                                                             \
   case R_ * 4 + (NP_ == 4 ? 2 : 0) + 1:                                               \
-    e = launch_sweep<R_, NP_, kChunk, 8>(a, ctx.stream);                              \
+    e = launch_sweep<R_, NP_, kChunk, 8>(a, ctx.stream, ctx.exclusive_sweep);         \
     break;
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)

@@ -92,3 +92,15 @@ def test_options_validation():
     o.compute = "cpu"
     with pytest.raises(ValueError, match="no CPU fallback"):
         o.validate()
+
+
+def test_batch_entry_points_reject_bad_arguments(lib):
+    """The batch calls validate their arguments on the host before touching a device."""
+    request = ctypes.c_int64()
+    assert lib.csgm_batch_configure(None, 4, 0) == _abi.CSGM_E_INVALID
+    assert lib.csgm_batch_submit(None, None, None, None, None, None, 64, 64, None, None, None,
+                                 None, None, ctypes.byref(request)) == _abi.CSGM_E_INVALID
+    assert lib.csgm_batch_poll(None, 1, 0, None) == _abi.CSGM_E_INVALID
+    assert lib.csgm_batch_status(None, None, None, None) == _abi.CSGM_E_INVALID
+    ptr = ctypes.c_void_p()
+    assert lib.csgm_host_alloc(0, ctypes.byref(ptr)) == _abi.CSGM_E_INVALID
