@@ -42,7 +42,12 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfg1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"], default="cfg1",
+                    help="cfg3: 48 uneven pairs batched; cfg4: Poisson-served pairs")
+    ap.add_argument("--slots", type=int, default=3, help="cfg3/cfg4: batch slots")
+    ap.add_argument("--pairs", type=int, default=48, help="cfg3: pairs in the batch")
+    ap.add_argument("--rates", default="10,25,50,100,200,400", help="cfg4: offered pairs/s")
+    ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate (max)")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-pairs", type=int, default=0,
@@ -424,10 +429,278 @@ def run_profile_pairs(args):
     return 0
 
 
+# ---------------------------------------------------------------------------------------------
+# Batched (cfg3) and served (cfg4) pairs: uneven sizes, disparity ranges and cost modes.
+def mixed_pair_specs(count: int, seed: int, mpix=None):
+    """cfg3: widths U[800, 3000], aspect 3:2 or 4:3; cfg4 (mpix given): log-uniform sizes in
+    [0.3, 6] Mpix.  D from {64, 128, 192, 256}, Census or AD-Census, each pair generated as the
+    640x480 workload (3 slanted planes, d in [4, 60]) from seed + i."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        aspect = (1.5, 4.0 / 3.0)[int(rng.integers(2))]
+        if mpix is None:
+            w = int(rng.uniform(800, 3000))
+        else:
+            area = float(np.exp(rng.uniform(np.log(mpix[0]), np.log(mpix[1])))) * 1e6
+            w = int(round((area * aspect) ** 0.5))
+        h = int(round(w / aspect))
+        d = int(rng.choice([64, 128, 192, 256]))
+        cost = ("census", "ad-census")[int(rng.integers(2))]
+        out.append(dict(w=w, h=h, D=d, cost=cost, seed=seed + i))
+    return out
+
+
+def _make_mixed(item):
+    from pose_b200.synthetic import PairSpec, make_pair
+
+    left, right, _ = make_pair(PairSpec(item["w"], item["h"], planes=3, d_min=4, d_max=60,
+                                        seed=item["seed"]))
+    return left, right
+
+
+def generate_mixed(items):
+    """Pairs generated in a spawn-started process pool (before any GPU call of this process)."""
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(len(items), os.cpu_count() or 1)) as pool:
+        return pool.map(_make_mixed, items)
+
+
+def mixed_params(item):
+    from pose_b200.options import Options
+    from pose_b200.stereo_cost import params_from_options
+
+    o = Options()
+    o.census, o.censusHeight = 9, 7
+    o.disparities, o.matchingCost, o.directions = item["D"], item["cost"], 8
+    prm = params_from_options(o)
+    prm.p1, prm.p2 = 10, 120
+    return prm
+
+
+def run_batched(args):
+    """cfg3: the pairs through csgm_pair one after another (the per-pair GPU path) and through
+    the batch slots; both with pinned host buffers, outputs compared bit for bit."""
+    import numpy as np
+
+    from pose_b200.batch import PairBatch, PinnedArray
+    from pose_b200.sgm import GpuSgm
+
+    items = mixed_pair_specs(args.pairs, 3000)
+    images = generate_mixed(items)
+    session = GpuSgm(0)
+    lib = session.lib
+    pinned = []
+    for item, (left, right) in zip(items, images):
+        n = item["w"] * item["h"]
+        b = {"left": PinnedArray(lib, n, np.uint8), "right": PinnedArray(lib, n, np.uint8),
+             "checked": PinnedArray(lib, n, np.float32)}
+        b["left"].array[:] = left
+        b["right"].array[:] = right
+        pinned.append(b)
+    params = [mixed_params(item) for item in items]
+    cells = sum(it["w"] * it["h"] * it["D"] for it in items)
+
+    from pose_b200._abi import CsgmStats, check
+
+    stats = CsgmStats()
+
+    def sequential():
+        outs = []
+        for prm, item, b in zip(params, items, pinned):
+            check(lib.csgm_pair(session.handle, ctypes.byref(prm), b["left"].ptr, b["right"].ptr,
+                                None, None, item["w"], item["h"], b["checked"].ptr, None, None,
+                                None, None, ctypes.byref(stats)))
+            outs.append(b["checked"].array.copy())
+        return outs
+
+    batch = PairBatch(session, slots=args.slots, budget_bytes=120 << 30)
+
+    def batched():
+        order, ids, done = list(range(len(items))), {}, {}
+        t_sub = {}
+        while order or ids:
+            while order:
+                i = order[0]
+                rid = batch.submit_pinned(params[i], pinned[i], items[i]["w"], items[i]["h"])
+                if rid is None:
+                    break
+                ids[rid] = i
+                t_sub[i] = time.perf_counter()
+                order.pop(0)
+            rid = next(iter(ids))
+            r = batch.poll(rid, wait=True, copy=True)
+            done[ids.pop(rid)] = r.disparity
+        return [done[i] for i in range(len(items))]
+
+    for _ in range(max(1, args.warmup // 3)):  # resident workspaces, kernels loaded
+        sequential()
+        batched()
+    seq_times, bat_times = [], []
+    for _ in range(max(1, args.steps // 5)):
+        t = time.perf_counter()
+        seq_out = sequential()
+        seq_times.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        bat_out = batched()
+        bat_times.append(time.perf_counter() - t)
+    exact = all(np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                for a, b in zip(seq_out, bat_out))
+    seq_s, bat_s = min(seq_times), min(bat_times)
+    line = {
+        "metric": "batched pairs/s (48 uneven pairs, bit-exact) vs per-pair GPU path",
+        "value": round(len(items) / bat_s, 2), "unit": "pairs/s", "n_gpus": 1,
+        "steps": len(bat_times), "warmup": max(1, args.warmup // 3),
+        "ms_per_step": round(bat_s * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": f"cfg3 {len(items)} pairs, widths 800-3000, aspect 3:2/4:3, D in "
+                               "{64,128,192,256}, census/AD-census, 8 paths",
+                   "slots": args.slots, "budget_gib": 120, "host_buffers": "pinned"},
+        "per_pair_gpu": {"value": round(len(items) / seq_s, 2), "unit": "pairs/s",
+                         "ms_per_step": round(seq_s * 1e3, 2)},
+        "speedup_vs_per_pair": round(seq_s / bat_s, 3),
+        "gcells_per_s": {"batched": round(cells / bat_s / 1e9, 2),
+                         "per_pair": round(cells / seq_s / 1e9, 2)},
+        "bit_exact_vs_per_pair": bool(exact),
+    }
+    session.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_served(args):
+    """cfg4: an open-loop Poisson stream of pair requests, served by continuous batching
+    (batch slots, admission under a 120 GB budget) and, for comparison, by the per-pair GPU path
+    (one pair at a time, first come first served).  Latency = completion - arrival."""
+    import collections
+
+    import numpy as np
+
+    from pose_b200.batch import PairBatch, PinnedArray
+    from pose_b200.sgm import GpuSgm
+
+    pool_items = mixed_pair_specs(24, 4000, mpix=(0.3, 6.0))
+    images = generate_mixed(pool_items)
+    session = GpuSgm(0)
+    lib = session.lib
+    inputs = []
+    for item, (left, right) in zip(pool_items, images):
+        n = item["w"] * item["h"]
+        b = {"left": PinnedArray(lib, n, np.uint8), "right": PinnedArray(lib, n, np.uint8)}
+        b["left"].array[:] = left
+        b["right"].array[:] = right
+        inputs.append(b)
+    params = [mixed_params(item) for item in pool_items]
+    max_n = max(it["w"] * it["h"] for it in pool_items)
+    outputs = [PinnedArray(lib, max_n, np.float32) for _ in range(args.slots)]
+    batch = PairBatch(session, slots=args.slots, budget_bytes=120 << 30)
+    for i in range(len(pool_items)):  # warm: kernels, resident workspaces of both servers
+        session.pair(params[i], inputs[i]["left"].array, inputs[i]["right"].array,
+                     pool_items[i]["w"], pool_items[i]["h"])
+    order = sorted(range(len(pool_items)), key=lambda i: -pool_items[i]["w"] * pool_items[i]["h"]
+                   * pool_items[i]["D"])
+    for start in range(0, len(order), args.slots):  # every slot grows to the largest pairs
+        ids = []
+        for k in order[start:start + args.slots]:
+            buf = dict(inputs[k])
+            buf["checked"] = outputs[len(ids)]
+            rid = batch.submit_pinned(params[k], buf, pool_items[k]["w"], pool_items[k]["h"])
+            if rid is not None:
+                ids.append(rid)
+        for rid in ids:
+            batch.poll(rid, wait=True, copy=False)
+
+    def arrivals(rate, count, seed):
+        rng = np.random.default_rng(seed)
+        return np.cumsum(rng.exponential(1.0 / rate, count)), rng.integers(0, len(pool_items),
+                                                                           count)
+
+    def serve_batched(times, which):
+        free_out = list(range(len(outputs)))
+        queue, inflight, lat = collections.deque(), {}, []
+        t0, i, count = time.perf_counter(), 0, len(times)
+        while i < count or queue or inflight:
+            now = time.perf_counter() - t0
+            while i < count and times[i] <= now:
+                queue.append(i)
+                i += 1
+            busy = False
+            while queue and free_out:
+                r = queue[0]
+                k = which[r]
+                buf = dict(inputs[k])
+                buf["checked"] = outputs[free_out[-1]]
+                rid = batch.submit_pinned(params[k], buf, pool_items[k]["w"], pool_items[k]["h"])
+                if rid is None:
+                    break
+                inflight[rid] = (r, free_out.pop())
+                queue.popleft()
+                busy = True
+            for rid in list(inflight):
+                if batch.poll(rid, wait=False, copy=False) is not None:
+                    r, o = inflight.pop(rid)
+                    free_out.append(o)
+                    lat.append(time.perf_counter() - t0 - times[r])
+                    busy = True
+            if not busy:
+                time.sleep(0.0002)
+        return np.array(lat), time.perf_counter() - t0
+
+    def serve_per_pair(times, which):
+        lat, t0 = [], time.perf_counter()
+        out = outputs[0]
+        for r in range(len(times)):
+            now = time.perf_counter() - t0
+            if times[r] > now:
+                time.sleep(times[r] - now)
+            k = which[r]
+            session.pair(params[k], inputs[k]["left"].array, inputs[k]["right"].array,
+                         pool_items[k]["w"], pool_items[k]["h"])
+            lat.append(time.perf_counter() - t0 - times[r])
+        return np.array(lat), time.perf_counter() - t0
+
+    rows = []
+    for rate in [float(x) for x in args.rates.split(",")]:
+        count = int(min(args.requests, max(40, rate * 4)))
+        times, which = arrivals(rate, count, int(rate * 7))
+        lb, tb = serve_batched(times, which)
+        lp, tp = serve_per_pair(times, which)
+        rows.append({"offered_pairs_s": rate, "requests": count,
+                     "batched": {"pairs_s": round(count / tb, 2),
+                                 "p50_ms": round(float(np.percentile(lb, 50)) * 1e3, 2),
+                                 "p99_ms": round(float(np.percentile(lb, 99)) * 1e3, 2)},
+                     "per_pair": {"pairs_s": round(count / tp, 2),
+                                  "p50_ms": round(float(np.percentile(lp, 50)) * 1e3, 2),
+                                  "p99_ms": round(float(np.percentile(lp, 99)) * 1e3, 2)}})
+    top = rows[-1]
+    line = {
+        "metric": "served pairs/s with p50/p99 latency (Poisson arrivals) vs per-pair GPU path",
+        "value": top["batched"]["pairs_s"], "unit": "pairs/s", "n_gpus": 1,
+        "steps": sum(r["requests"] for r in rows), "warmup": len(pool_items),
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16", "data": "synthetic",
+        "config": {"workload": "cfg4 Poisson open loop, sizes log-uniform 0.3-6 Mpix, aspect "
+                               "3:2/4:3, D in {64,128,192,256}, census/AD-census, 8 paths, "
+                               "24 distinct pairs drawn at random",
+                   "slots": args.slots, "budget_gib": 120, "host_buffers": "pinned"},
+        "rates": rows,
+    }
+    session.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.profile_pairs:
         return run_profile_pairs(args)
+    if args.workload == "cfg3":
+        return run_batched(args)
+    if args.workload == "cfg4":
+        return run_served(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

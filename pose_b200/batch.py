@@ -92,8 +92,9 @@ class PairBatch:
         self._requests[request.value] = _Request(w, h, buffers)
         return request.value
 
-    def poll(self, request: int, wait: bool = True) -> Result | None:
-        """The finished pair (outputs copied out of the pinned buffers), or None if still running."""
+    def poll(self, request: int, wait: bool = True, copy: bool = True) -> Result | None:
+        """The finished pair, or None if still running.  With copy=False the result's arrays are
+        views of the request's pinned buffers (valid while the caller keeps them)."""
         cstats = CsgmStats()
         status = self.lib.csgm_batch_poll(self.session.handle, int(request), int(bool(wait)),
                                           ctypes.byref(cstats))
@@ -104,7 +105,9 @@ class PairBatch:
         b = r.buffers
 
         def out(key):
-            return b[key].array.copy() if key in b else None
+            if key not in b:
+                return None
+            return b[key].array.copy() if copy else b[key].array
 
         return Result(r.w, r.h, out("checked"), Stats.from_c(cstats), out("dl"), out("dr"),
                       out("reasons"), out("boundary"))

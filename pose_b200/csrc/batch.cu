@@ -1,9 +1,11 @@
-// batch.cu - batched and served pairs: a session's slots each hold one pair in flight on their own
-// CUDA stream with a resident workspace, so pairs submitted back to back overlap on the GPU (the
-// sweep is latency-bound, and concurrent pairs fill each other's idle issue slots).  Admission
-// checks each pair's device memory (W*H*D bytes of cost volumes and aggregates, plus images and
-// outputs) against the batch budget; a pair that does not fit right now is refused with
-// CSGM_E_BUSY and can be submitted again once a slot or memory frees up (continuous batching).
+// batch.cu - batched and served pairs.  A session's slots each hold one pair in flight with its own
+// CUDA stream and a resident device workspace (stream-ordered allocations from a pool that keeps
+// freed memory).  All slots' sweeps share one high-priority stream, so sweeps run back to back at
+// the speed of a lone pair, while the other pairs' uploads, census, cost volumes, selections and
+// downloads overlap them on the SMs a sweep leaves idle.  Admission checks each pair's device
+// memory (W*H*D bytes of cost volumes and aggregates, plus images and outputs) against the batch
+// budget; a pair that does not fit right now is refused with CSGM_E_BUSY and can be submitted
+// again once a slot or memory frees up (continuous batching).
 //
 // There is no batch interface in the reference: GpuSgm serves one pair per call and one session
 // per Java thread (GpuSgm.java:22,163-303).  The per-pair semantics, and so every result, are
@@ -11,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <cstdlib>
 
 #include "collinea_sgm.h"
 #include "pipeline.h"
@@ -28,6 +32,9 @@ void release_slots(csgm_session* s) {
       cudaStreamSynchronize(slot.stream);  // stream-ordered frees complete
       cudaStreamDestroy(slot.stream);
     }
+    if (slot.sweep_stream) cudaStreamDestroy(slot.sweep_stream);
+    if (slot.sweep_ready) cudaEventDestroy(slot.sweep_ready);
+    if (slot.sweep_done) cudaEventDestroy(slot.sweep_done);
     if (slot.done) cudaEventDestroy(slot.done);
     if (slot.host_stats) cudaFreeHost(slot.host_stats);
   }
@@ -61,9 +68,30 @@ int csgm_batch_configure(csgm_session* s, int32_t slots, int64_t budget_bytes) {
   release_slots(s);
   s->batch_budget = budget_bytes == 0 ? s->memory / 10 * 7
                                       : std::min<size_t>(s->memory / 100 * 95, (size_t)budget_bytes);
+  // Slot workspaces grow and shrink stream-ordered: memory they give back stays in the device's
+  // pool for the next pair instead of returning to the driver.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   s->slots.resize((size_t)slots);
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
   for (auto& slot : s->slots) {
-    e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithPriority(&slot.stream, cudaStreamNonBlocking, least);
+    // One high-priority stream carries every slot's sweep: sweeps run back to back at the speed
+    // of a lone pair (each sweep fills the GPU with its chain of row blocks; two at once slow each
+    // other down more than they gain), while the other slots' uploads, cost volumes, selections
+    // and downloads use the SMs a sweep leaves idle.
+    if (e == cudaSuccess && &slot != &s->slots[0]) {
+      slot.sweep_stream = nullptr;  // borrows slot 0's stream below
+    } else if (e == cudaSuccess) {
+      e = cudaStreamCreateWithPriority(&slot.sweep_stream, cudaStreamNonBlocking, greatest);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.sweep_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.sweep_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&slot.host_stats, sizeof(DeviceStats));
     if (e != cudaSuccess) {
@@ -73,6 +101,8 @@ int csgm_batch_configure(csgm_session* s, int32_t slots, int64_t budget_bytes) {
     slot.ws.async_stream = slot.stream;
     slot.ws.budget = s->batch_budget;
   }
+  for (auto& slot : s->slots)
+    if (!slot.sweep_stream) slot.shared_sweep = s->slots[0].sweep_stream;
   return CSGM_OK;
 }
 
@@ -119,7 +149,9 @@ int csgm_batch_submit(csgm_session* s, const csgm_params* p, const uint8_t* left
     return fail(CSGM_E_BUSY, "batch memory held by pairs in flight");
   slot->ws.budget = s->batch_budget - held;
   Context ctx{slot->stream, s->sm_count, &slot->ws, &slot->prof, &slot->profile};
-  ctx.exclusive_sweep = false;
+  ctx.sweep_stream = slot->sweep_stream ? slot->sweep_stream : slot->shared_sweep;
+  ctx.sweep_ready = slot->sweep_ready;
+  ctx.sweep_done = slot->sweep_done;
   rc = enqueue_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                          reasons, boundary, slot->host_stats);
   if (rc == CSGM_OK) {

@@ -73,11 +73,17 @@ struct Context {
   csgm_profile* profile;
   // One sweep CTA per SM (a lone pair runs fastest so); batched pairs share SMs instead.
   bool exclusive_sweep = true;
+  // Optional separate stream for the sweep (ordered after and before ctx.stream by the events).
+  cudaStream_t sweep_stream = nullptr;
+  cudaEvent_t sweep_ready = nullptr, sweep_done = nullptr;
 };
 
 // One batch slot: a pair in flight with its own stream and resident workspace.
 struct BatchSlot {
   cudaStream_t stream = nullptr;
+  cudaStream_t sweep_stream = nullptr;  // high priority, owned by this slot
+  cudaStream_t shared_sweep = nullptr;  // or another slot's (not owned)
+  cudaEvent_t sweep_ready = nullptr, sweep_done = nullptr;
   cudaEvent_t done = nullptr;
   Workspace ws;
   Profiler prof;

@@ -1302,14 +1302,23 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
   const int regs = F.Dp / 32;
   const bool eight = p.directions == 8;
+  // Batched pairs launch the sweep on a high-priority stream: its pending CTAs then take SMs ahead
+  // of other pairs' bandwidth-bound kernels, so a pair's chain of row blocks is not held up.
+  cudaStream_t sweep_stream = ctx.stream;
+  if (ctx.sweep_stream) {
+    e = cudaEventRecord(ctx.sweep_ready, ctx.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx.sweep_stream, ctx.sweep_ready, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "sweep stream ordering");
+    sweep_stream = ctx.sweep_stream;
+  }
   ctx.prof->kernel_begin();
   switch (regs * 4 + (eight ? 2 : 0) + (F.rows == 8 ? 1 : 0)) {
 #define CSGM_SWEEP_CASE(R_, NP_)                                                       \
   case R_ * 4 + (NP_ == 4 ? 2 : 0):                                                   \
-    e = launch_sweep<R_, NP_, kChunk, 4>(a, ctx.stream, ctx.exclusive_sweep);         \
+    e = launch_sweep<R_, NP_, kChunk, 4>(a, sweep_stream, ctx.exclusive_sweep);       \
     break;                                                                             \
   case R_ * 4 + (NP_ == 4 ? 2 : 0) + 1:                                               \
-    e = launch_sweep<R_, NP_, kChunk, 8>(a, ctx.stream, ctx.exclusive_sweep);         \
+    e = launch_sweep<R_, NP_, kChunk, 8>(a, sweep_stream, ctx.exclusive_sweep);       \
     break;
     CSGM_SWEEP_CASE(2, 2)
     CSGM_SWEEP_CASE(2, 4)
@@ -1323,6 +1332,11 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
   if (e != cudaSuccess) return cuda_fail(e, "sweep kernel launch");
+  if (ctx.sweep_stream) {
+    e = cudaEventRecord(ctx.sweep_done, ctx.sweep_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx.stream, ctx.sweep_done, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "sweep stream ordering");
+  }
   ctx.prof->kernel_end("sweep");
 
   WtaArgs t{};
