@@ -19,7 +19,7 @@ int validate_params(const csgm_params* p, int w, int h);
 
 enum Slot {
   kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
-  kCostL, kCostR, kSum, kSumUp, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
+  kCostL, kCostR, kSum, kSumUp, kSumLines, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
   kCarry, kFlags, kSlotCount
 };
 

@@ -794,7 +794,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   const int yp = b * R + w;  // row in stream order
   if (yp >= H) {
     // Rows beyond the image: nobody reads them, but the warp takes part in every step barrier.
-    for (int step = 0; step < W + 2 * (R - 1); step++) rows_barrier(R * 32);
+    for (int step = 0; step < W + (R - 1); step++) rows_barrier(R * 32);
     return;
   }
   const int y = mirror ? H - 1 - yp : yp;
@@ -856,7 +856,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   int carry_ready = 0;
 
   // Idle steps before this row starts (the 2-pixel lag behind the row above).
-  for (int step = 0; step < 2 * w; step++) rows_barrier(R * 32);
+  for (int step = 0; step < w; step++) rows_barrier(R * 32);
 
   // The sweep of one row.  CARRY_IN: the row above is the previous block's carry row (waited for
   // chunk by chunk); PUBLISH: this row's vertical states are also stored as this block's carry.
@@ -881,17 +881,12 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
       load_path<REGS>(up_a + (xs & up_mask) * L::vslot, 0, prev[1]);
       if constexpr (NPATH > 2) {
         const uint32_t pd = xs > 0 ? up_a + ((xs - 1) & up_mask) * L::vslot : zero_a;
-        const uint32_t pa = xs + 1 < W ? up_a + ((xs + 1) & up_mask) * L::vslot : zero_a;
         load_path<REGS>(pd, 1, prev[2]);
-        load_path<REGS>(pa, 2, prev[3]);
       }
       uint32_t q[NPATH];
       q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
       q[1] = pw.y;  // normalised predecessors: minimum 0
-      if constexpr (NPATH > 2) {
-        q[2] = pw.z;
-        q[3] = pw.w;
-      }
+      if constexpr (NPATH > 2) q[2] = pw.z;
       PathState<REGS> out[NPATH];
       paths_step<REGS, NPATH>(prev, q, p1x2, cst, lo_edge, hi_edge, out);
       // Partial aggregate of this stream's paths.
@@ -951,9 +946,6 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
       const uint32_t slot = slots_a + (c % NB) * L::cslot;
 #pragma unroll
       for (int off = 0; off < K; off++) {
-        if constexpr (CARRY_IN) {
-          if (off == K - 1) wait_carry(c + 1);
-        }
         pixel(c * K + off, slot + cost_first_full + off * cost_step, slot + 2 * K * Dp + 16 * off);
         rows_barrier(R * 32);
       }
@@ -981,10 +973,187 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
     sweep_row(std::false_type{}, std::false_type{});
 
   // Idle steps after this row finished (the rows below are still running).
-  for (int step = 0; step < 2 * (R - 1 - w); step++) rows_barrier(R * 32);
+  for (int step = 0; step < R - 1 - w; step++) rows_barrier(R * 32);
   // After an expired wait, give outstanding chunk copies a bounded chance to land before exit.
   for (int cc = max(0, issued - NB); cc < issued; cc++)
     wait_bar(&my_full[cc % NB], (cc / NB) & 1, err, limit / 4, 5, false);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The anti-diagonal paths (-1,1) and (1,-1) (CensusSgm.java:421-459, direction table entries 5
+// and 6) follow the lines x + y = s, which are independent of each other: one warp per line,
+// both views packed as in the sweep.  The forward pass walks (-1,1) from the line's upper-right
+// end and stores its path costs as the line partial; the backward pass walks (1,-1) from the
+// lower-left end, adds its path costs and stores the sum.  Costs, penalty records and (backward)
+// the stored forward costs are prefetched kPrefetch pixels ahead.  Word 3 of the down stream's
+// penalty record of a pixel is pathP2 - P1 towards (x+1, y-1), word 3 of the up stream's record
+// pathP2 - P1 towards (x-1, y+1).
+struct LineArgs {
+  const uint8_t* cost[2];  // [H][W][Dp] per view
+  const uint4* pen;        // [2 streams][H][W] penalty records, stream order
+  uint32_t* part;          // [H][W][Dp] partial aggregate of the two anti-diagonal paths
+  int W, H, D, p1;
+};
+
+constexpr int kLineWarps = 8;
+constexpr int kPrefetch = 8;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Per-warp ring of kPrefetch pixel slots: costs of both views (Dp bytes each), the penalty record
+// (16 bytes) and, on the return pass, the stored forward costs (Dp x 4 bytes).
+template <int REGS>
+struct LineSlot {
+  static constexpr int Dp = 32 * REGS;
+  static constexpr int cost = 0, pen = 2 * Dp, part = 2 * Dp + 16;
+  static constexpr int bytes = 2 * Dp + 16 + 4 * Dp;
+};
+
+template <int REGS>
+__global__ void __launch_bounds__(kLineWarps * 32) lines_kernel(const LineArgs a) {
+  constexpr int Dp = 32 * REGS, CH = Dp / 16;  // 16-byte chunks per view's cost line
+  using S = LineSlot<REGS>;
+  extern __shared__ __align__(16) uint8_t lsm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int line = blockIdx.x * kLineWarps + warp;
+  const int W = a.W, H = a.H;
+  if (line >= W + H - 1) return;
+  const uint32_t ring = smem_u32(lsm) + warp * kPrefetch * S::bytes;
+  const int x0 = min(line, W - 1), y0 = line - x0;  // upper-right end of the line
+  const int len = min(x0 + 1, H - y0);               // pixel i: (x0 - i, y0 + i)
+  const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
+  const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
+  uint32_t pad[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
+  const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
+  uint32_t* part = a.part + lane * REGS;
+  const int64_t step = (int64_t)W - 1;  // pixel-index step along the line (down-left)
+  const int64_t p0 = (int64_t)y0 * W + x0;
+
+  // Issues the copies of pixel i into ring slot `slot` as one commit group (empty if i is off
+  // the line, so the group count stays in step).
+  auto fetch = [&](int slot, int i, bool back) {
+    if (i >= 0 && i < len) {
+      const int64_t p = p0 + i * step;
+      const uint32_t s = ring + slot * S::bytes;
+      if (lane < 2 * CH) {
+        const int view = lane / CH, chunk = lane % CH;
+        cp_async16(s + S::cost + view * Dp + chunk * 16,
+                   (view ? a.cost[1] : a.cost[0]) + p * Dp + chunk * 16);
+      }
+      if (lane == 31) {
+        const int y = y0 + i, x = x0 - i;
+        const uint4* rec = back ? &a.pen[((int64_t)H + (H - 1 - y)) * W + (W - 1 - x)]
+                                : &a.pen[p];
+        cp_async16(s + S::pen, rec);
+      }
+      if (back) {
+#pragma unroll
+        for (int c = lane; c < Dp / 4; c += 32)
+          cp_async16(s + S::part + c * 16, a.part + p * Dp + c * 4);
+      }
+    }
+    cp_async_commit();
+  };
+  // Consumes ring slot `slot`: this lane's widened costs, penalty and texture words.
+  auto take = [&](int slot, uint32_t (&c)[REGS], uint32_t& pq, uint32_t& pt) {
+    const uint32_t s = ring + slot * S::bytes;
+    widen_costs<REGS>(s + S::cost + lane * REGS, s + S::cost + Dp + lane * REGS, pad, c);
+    const uint4 r = lds_v4(s + S::pen);
+    pq = r.w;
+    pt = r.x;
+  };
+
+  PathState<REGS> cur;
+  // Forward: (-1,1), pixel i's predecessor is pixel i - 1.
+  zero_state(cur);
+#pragma unroll
+  for (int k = 0; k < kPrefetch; k++) fetch(k, k, false);
+  for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; k++) {
+      const int i = base + k;
+      if (i < len) {
+        cp_async_wait<kPrefetch - 1>();
+        __syncwarp();
+        uint32_t c[REGS], pq, pt;
+        take(k, c, pq, pt);
+        __syncwarp();  // every lane has read the slot before it is refilled
+        fetch(k, i + kPrefetch, false);
+        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+        const uint32_t keep = prmt(pt, 0, 0xbb99u);
+        PathState<REGS> prev[1] = {cur}, out[1];
+        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+        store_words<REGS>(part + (p0 + i * step) * Dp, out[0].v);
+        cur = out[0];
+        if (keep != 0xffffffffu) {
+#pragma unroll
+          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+          cur.m &= keep;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  // The return pass copies the stored forward costs back from L2 (cp.async.cg), some of them
+  // written by other lanes just now: every lane's stores reach L2 before any lane copies.
+  __threadfence();
+  __syncwarp();
+  // Backward: (1,-1), pixel i's predecessor is pixel i + 1; adds to the stored forward costs.
+  zero_state(cur);
+#pragma unroll
+  for (int k = 0; k < kPrefetch; k++) fetch(k, len - 1 - k, true);
+  for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; k++) {
+      const int i = len - 1 - (base + k);
+      if (i >= 0) {
+        cp_async_wait<kPrefetch - 1>();
+        __syncwarp();
+        uint32_t c[REGS], pq, pt, fwd[REGS];
+        take(k, c, pq, pt);
+        lds_words<REGS>(ring + k * S::bytes + S::part + lane * REGS * 4, fwd);
+        __syncwarp();
+        fetch(k, i - kPrefetch, true);
+        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+        const uint32_t keep = prmt(pt, 0, 0xbb99u);
+        PathState<REGS> prev[1] = {cur}, out[1];
+        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+        uint32_t sum[REGS];
+#pragma unroll
+        for (int j = 0; j < REGS; j++) sum[j] = fwd[j] + out[0].v[j];
+        store_words_cs<REGS>(part + (p0 + i * step) * Dp, sum);
+        cur = out[0];
+        if (keep != 0xffffffffu) {
+#pragma unroll
+          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+          cur.m &= keep;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+template <int REGS>
+cudaError_t launch_lines(const LineArgs& a, cudaStream_t stream) {
+  const int lines = a.W + a.H - 1;
+  const int shared = kLineWarps * kPrefetch * LineSlot<REGS>::bytes;
+  cudaError_t e = cudaFuncSetAttribute(lines_kernel<REGS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
+  if (e != cudaSuccess) return e;
+  lines_kernel<REGS><<<(lines + kLineWarps - 1) / kLineWarps, kLineWarps * 32, shared, stream>>>(a);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -997,6 +1166,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
 struct WtaArgs {
   const uint32_t* down;  // [H][W][Dp] left | right << 16
   const uint32_t* up;
+  const uint32_t* lines;  // anti-diagonal paths (8-path mode), else null
   float* disp[2];
   uint8_t* reasons;    // left view only
   uint8_t* boundary;   // left view only
@@ -1072,20 +1242,25 @@ __global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
   const int64_t stride = (int64_t)gridDim.x * kWtaWarps;
   unsigned counts[6] = {0, 0, 0, 0, 0, 0};
   // Software pipeline: the next pixel's aggregates are in flight while this one is selected.
-  uint32_t d[REGS], u[REGS];
+  uint32_t d[REGS], u[REGS], g[REGS];
+  const bool three = a.lines != nullptr;
+#pragma unroll
+  for (int j = 0; j < REGS; j++) g[j] = 0;
   int64_t p = (int64_t)blockIdx.x * kWtaWarps + warp;
   if (p < n) {
     load_words<REGS>(a.down + p * Dp + lane * REGS, d);
     load_words<REGS>(a.up + p * Dp + lane * REGS, u);
+    if (three) load_words<REGS>(a.lines + p * Dp + lane * REGS, g);
   }
   for (; p < n; p += stride) {
     const int y = (int)(p / W), x = (int)(p - (int64_t)y * W);
     uint32_t tot[REGS];
 #pragma unroll
-    for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j];
+    for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j] + g[j];
     if (p + stride < n) {
       load_words<REGS>(a.down + (p + stride) * Dp + lane * REGS, d);
       load_words<REGS>(a.up + (p + stride) * Dp + lane * REGS, u);
+      if (three) load_words<REGS>(a.lines + (p + stride) * Dp + lane * REGS, g);
     }
     int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
     if (y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx) {
@@ -1189,7 +1364,7 @@ struct FusedLayout {
     Dp = padded_d(p.disparities);
     rows = rows_for(Dp / 32);
     nb = (h + rows - 1) / rows;
-    const int nv = p.directions == 8 ? 3 : 1;
+    const int nv = p.directions == 8 ? 2 : 1;
     vslot = nv * Dp * 4;
     size_t n = (size_t)w * h;
     cost = n * Dp;
@@ -1197,7 +1372,7 @@ struct FusedLayout {
     pen = 2 * n * 16;
     carry = (size_t)2 * nb * w * vslot;
     flags = ((size_t)2 * nb + 8) * sizeof(int);
-    total = 2 * cost + 2 * sum + pen + carry + flags + 6 * 256;
+    total = 2 * cost + (p.directions == 8 ? 3 : 2) * sum + pen + carry + flags + 7 * 256;
   }
 };
 
@@ -1230,6 +1405,11 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   if (!sum_down) return status;
   uint32_t* sum_up = (uint32_t*)ctx.ws->get(kSumUp, F.sum, &status);
   if (!sum_up) return status;
+  uint32_t* sum_lines = nullptr;
+  if (p.directions == 8) {
+    sum_lines = (uint32_t*)ctx.ws->get(kSumLines, F.sum, &status);
+    if (!sum_lines) return status;
+  }
   uint4* pen = (uint4*)ctx.ws->get(kPen, F.pen, &status);
   if (!pen) return status;
   uint8_t* carry = (uint8_t*)ctx.ws->get(kCarry, F.carry, &status);
@@ -1280,6 +1460,23 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     if (le != cudaSuccess) return cuda_fail(le, "penalty kernel launch");
     ctx.prof->kernel_end("penalty");
   }
+  if (sum_lines) {
+    // The anti-diagonal lines, on the pair's own stream before the sweep (beside the sweep on a
+    // second stream they slowed it by more than their own run time: 4.63 ms per pair against
+    // 4.47 ms one after the other).
+    LineArgs la{{cost_l, cost_r}, pen, sum_lines, w, h, p.disparities, p.p1};
+    cudaError_t le;
+    ctx.prof->kernel_begin();
+    switch (F.Dp / 32) {
+      case 2: le = launch_lines<2>(la, ctx.stream); break;
+      case 4: le = launch_lines<4>(la, ctx.stream); break;
+      case 6: le = launch_lines<6>(la, ctx.stream); break;
+      case 8: le = launch_lines<8>(la, ctx.stream); break;
+      default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
+    }
+    if (le != cudaSuccess) return cuda_fail(le, "line kernel launch");
+    ctx.prof->kernel_end("lines");
+  }
   cudaError_t e = cudaMemsetAsync(flags, 0, F.flags, ctx.stream);
   if (e != cudaSuccess) return cuda_fail(e, "flag clear");
 
@@ -1314,20 +1511,20 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   ctx.prof->kernel_begin();
   switch (regs * 4 + (eight ? 2 : 0) + (F.rows == 8 ? 1 : 0)) {
 #define CSGM_SWEEP_CASE(R_, NP_)                                                       \
-  case R_ * 4 + (NP_ == 4 ? 2 : 0):                                                   \
+  case R_ * 4 + (NP_ == 3 ? 2 : 0):                                                   \
     e = launch_sweep<R_, NP_, kChunk, 4>(a, sweep_stream, ctx.exclusive_sweep);       \
     break;                                                                             \
-  case R_ * 4 + (NP_ == 4 ? 2 : 0) + 1:                                               \
+  case R_ * 4 + (NP_ == 3 ? 2 : 0) + 1:                                               \
     e = launch_sweep<R_, NP_, kChunk, 8>(a, sweep_stream, ctx.exclusive_sweep);       \
     break;
     CSGM_SWEEP_CASE(2, 2)
-    CSGM_SWEEP_CASE(2, 4)
+    CSGM_SWEEP_CASE(2, 3)
     CSGM_SWEEP_CASE(4, 2)
-    CSGM_SWEEP_CASE(4, 4)
+    CSGM_SWEEP_CASE(4, 3)
     CSGM_SWEEP_CASE(6, 2)
-    CSGM_SWEEP_CASE(6, 4)
+    CSGM_SWEEP_CASE(6, 3)
     CSGM_SWEEP_CASE(8, 2)
-    CSGM_SWEEP_CASE(8, 4)
+    CSGM_SWEEP_CASE(8, 3)
 #undef CSGM_SWEEP_CASE
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
@@ -1342,6 +1539,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   WtaArgs t{};
   t.down = sum_down;
   t.up = sum_up;
+  t.lines = sum_lines;
   t.disp[0] = v.disp_l;
   t.disp[1] = v.disp_r;
   t.reasons = v.reasons;
