@@ -151,12 +151,17 @@ def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int):
     table = {
         "cost_pair": 2,                   # both views' uint8 cost volumes, written once
         "sweep": 4 * (1 + sb),            # 2 streams x 2 views: cost read + partial aggregate write
-        "wta": 4 * sb,                    # 2 views x (down, up) partial aggregates read
+        "penalty": None,
+        # 2 views x the partial aggregates read: down, up (+ anti-diagonal lines with 8 paths)
+        "wta": (3 if prm.directions == 8 else 2) * 2 * sb,
+        # anti-diagonal lines: costs of both views read by both passes, the forward path's costs
+        # written and read back, the lines partial written (both views)
+        "lines": 4 + 3 * 2 * sb,
         "cost_volume": 1,                 # general path: one view's uint8 cost volume
         "paths_line": 1 + 2 * sb,         # general path: cost read + aggregate read-modify-write
         "winners": 1 + sb,                # general path: cost validity + aggregate read
     }
-    if kernel not in table:
+    if table.get(kernel) is None:
         return None
     return table[kernel] * cells
 
