@@ -5,33 +5,33 @@
 // general kernels (stereo_kernels.cu) and to the CPU reference.
 //
 // Design (B200):
-//  * cost_pair_kernel writes both views' cost volumes once, as uint8 [H][W][Dp] with
-//    Dp = D rounded up to 64 and 0x80 marking the reference's invalid cost 512.
+//  * cost_rows_kernel (census modes) / cost_pair_kernel (ZNCC) write both views' cost volumes
+//    once, as uint8 [H][W][Dp] with Dp = D rounded up to 64 and 0x80 marking the reference's
+//    invalid cost 512.  penalty_kernel writes one record of per-path P2' - P1 per stream pixel.
+//  * lines_kernel aggregates the two anti-diagonal paths (-1,1) and (1,-1): the lines x + y = s
+//    are independent, one warp walks a line forward and back and stores their sum as the lines
+//    partial aggregate.
 //  * sweep_kernel runs two wavefront streams in one launch, each over both views: "down"
-//    processes rows top to bottom, pixels left to right, and owns the paths whose predecessor
-//    lies above or to the left: (1,0), (0,1), (1,1), (-1,1); "up" is the same code on the image
-//    mirrored in x and y and owns the four opposite paths.
-//  * One CTA = R consecutive image rows; warp w holds row w of BOTH views (lanes 0-15 the left
-//    view, lanes 16-31 the right view) and processes pixel x at step x + 2w, all warps in lock
-//    step (one CTA barrier per step).  The (0,1), (1,1), (-1,1) path states of a row reach the
-//    next row through a shared-memory ring; the (1,0) state stays in registers.  The last row of
-//    a CTA also writes a global carry row that the next CTA of the stream reads
-//    (release/acquire progress counter).
-//  * Each stream stores its partial aggregate (uint16, 4 paths); the down stream marks cells whose
-//    cost is invalid with 0xffff (a valid 4-path partial sum stays below 0x8000).  The streams
-//    never wait for each other.
-//  * wta_kernel streams both partial aggregates through shared memory (bulk copies), adds them
-//    and runs winner-take-all, uniqueness and the parabolic sub-pixel step with one thread per
-//    pixel.
-//  * Disparities live in registers as packed uint16 pairs (REGS registers per lane per path,
-//    16 lanes per view-row); the min-plus step uses the DPX instructions __vimin3_u16x2 /
-//    __viaddmin_u16x2, and the per-row minima of two paths share one 16-lane shuffle butterfly
-//    on packed uint16 pairs.
-//  * Cost, partial-aggregate and carry slices are staged in shared memory by cp.async.bulk with
-//    mbarrier completion (no multicast).  Every wait is bounded; a wait that runs out sets an
-//    error flag that the host turns into CSGM_E_TIMEOUT.
-//  * CTAs take tickets in launch order; a CTA only waits on lower tickets, so the schedule cannot
-//    deadlock even when not every CTA is resident.
+//    processes rows top to bottom, pixels left to right, and owns (1,0), (0,1), (1,1); "up" is
+//    the same code on the image mirrored in x and y and owns the three opposite paths.
+//  * One sweep CTA = R consecutive image rows; warp w holds row w of BOTH views (each register
+//    packs a disparity's left-view value in its low and right-view value in its high 16 bits)
+//    and processes pixel x at step x + w, all row warps in lock step (one named barrier per
+//    step).  The (0,1) and (1,1) states of a row reach the next row through a shared-memory
+//    ring; the (1,0) state stays in registers.  The last row of a CTA also writes a global carry
+//    row that the next CTA of the stream reads (release/acquire progress counter).
+//  * Each stream stores its partial aggregate (uint16 pairs, 3 paths).  No cell is marked
+//    invalid: a valid path cost stays below 512 and an invalid one is at least 512, so a total of
+//    at least directions x 512 is an invalid cell.  The streams never wait for each other.
+//  * wta_kernel adds the partial aggregates (a warp per pixel, both views at once) and runs
+//    winner-take-all, uniqueness and the parabolic sub-pixel step, lane v selecting view v.
+//  * The min-plus step uses the DPX instructions __vimin3_u16x2 / __viaddmin_u16x2 on the
+//    packed pairs; the row minima of both views are two redux.sync.min per path.
+//  * Sweep cost chunks and carry rows are staged in shared memory by cp.async.bulk with mbarrier
+//    completion (no multicast); the line kernel prefetches with cp.async.  Every wait is
+//    bounded; a wait that runs out sets an error flag that the host turns into CSGM_E_TIMEOUT.
+//  * Sweep CTAs take tickets in launch order; a CTA only waits on lower tickets, so the schedule
+//    cannot deadlock even when not every CTA is resident.
 #include <climits>
 #include <cstdlib>
 #include <type_traits>
@@ -676,11 +676,12 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
 }
 
 // One CTA = R row warps + a carry-in warp + a publisher warp, one row block of one stream.
-//  * "down" (stream 0) runs rows top to bottom and pixels left to right and owns the paths whose
-//    predecessor lies above or to the left: (1,0), (0,1), (1,1), (-1,1); "up" (stream 1) is the
-//    same code on the image mirrored in x and y and owns the four opposite paths.
+//  * "down" (stream 0) runs rows top to bottom and pixels left to right and owns (1,0), (0,1),
+//    (1,1) (NPATH = 3; (1,0), (0,1) in 4-path mode, NPATH = 2); "up" (stream 1) is the same code
+//    on the image mirrored in x and y and owns the opposite paths.  The anti-diagonal paths,
+//    whose predecessor lies one pixel ahead in the row above, are lines_kernel's.
 //  * Row warp w holds stream row b*R + w of both views and processes stream pixel xs at step
-//    xs + 2w; the row warps meet at a named barrier once per step.  The vertical path states of
+//    xs + w; the row warps meet at a named barrier once per step.  The vertical path states of
 //    a pixel reach the next row through a shared-memory ring; the (1,0) state stays in registers.
 //  * Each row warp bulk-copies its own cost chunks (both views + penalty records) NB chunks
 //    ahead; the last row warp also stores its vertical states as the block's carry row.
@@ -855,7 +856,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   zero_state(horiz);
   int carry_ready = 0;
 
-  // Idle steps before this row starts (the 2-pixel lag behind the row above).
+  // Idle steps before this row starts (the 1-pixel lag behind the row above).
   for (int step = 0; step < w; step++) rows_barrier(R * 32);
 
   // The sweep of one row.  CARRY_IN: the row above is the previous block's carry row (waited for
