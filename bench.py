@@ -143,11 +143,14 @@ def pair_model_bytes_per_cell(prm) -> int:
     return 5 + 4 * prm.aggregate_bytes
 
 
-def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int):
+def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int, lines_in_sweep=False):
     """Algorithmic HBM bytes of one launch of `kernel`, from the bytes each kernel must move per
-    cell (uint8 costs, Sb-byte partial aggregates, both views).  None for per-pixel kernels."""
+    cell (uint8 costs, Sb-byte partial aggregates, both views).  None for per-pixel kernels and
+    for the leftover-lines launch.  `lines_in_sweep`: the sweep's CTAs also walk the anti-diagonal
+    lines (the session profile then names a `lines_rest` launch)."""
     cells = w * h * prm.disparities
     sb = prm.aggregate_bytes
+    lines = 4 + 3 * 2 * sb
     table = {
         "cost_pair": 2,                   # both views' uint8 cost volumes, written once
         "sweep": 4 * (1 + sb),            # 2 streams x 2 views: cost read + partial aggregate write
@@ -156,13 +159,16 @@ def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int):
         "wta": (3 if prm.directions == 8 else 2) * 2 * sb,
         # anti-diagonal lines: costs of both views read by both passes, the forward path's costs
         # written and read back, the lines partial written (both views)
-        "lines": 4 + 3 * 2 * sb,
+        "lines": lines,
+        "lines_rest": None,
         "cost_volume": 1,                 # general path: one view's uint8 cost volume
         "paths_line": 1 + 2 * sb,         # general path: cost read + aggregate read-modify-write
         "winners": 1 + sb,                # general path: cost validity + aggregate read
     }
     if table.get(kernel) is None:
         return None
+    if kernel == "sweep" and lines_in_sweep:
+        return (table["sweep"] + lines) * cells
     return table[kernel] * cells
 
 
@@ -361,7 +367,7 @@ def run_ours(args):
     roofline = None
     if kernels:
         name, (count, total_ns) = max(kernels.items(), key=lambda kv: kv[1][1])
-        per_launch = algorithmic_bytes_per_launch(name, prm, w, h)
+        per_launch = algorithmic_bytes_per_launch(name, prm, w, h, "lines_rest" in kernels)
         peak, peak_kind = measured_peak_gbs()
         if per_launch and count:
             achieved = per_launch / (total_ns / count / 1e9) / 1e9

@@ -73,6 +73,10 @@ struct Context {
   csgm_profile* profile;
   // One sweep CTA per SM (a lone pair runs fastest so); batched pairs share SMs instead.
   bool exclusive_sweep = true;
+  // 8 paths: the sweep's CTAs also walk the anti-diagonal lines (line warps on the issue slots
+  // the row warps leave idle).  Batched pairs run them as a kernel of their own on the pair's
+  // stream instead, beside the other pairs' sweeps.
+  bool lines_in_sweep = true;
   // Optional separate stream for the sweep (ordered after and before ctx.stream by the events).
   cudaStream_t sweep_stream = nullptr;
   cudaEvent_t sweep_ready = nullptr, sweep_done = nullptr;

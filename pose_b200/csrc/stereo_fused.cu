@@ -391,6 +391,60 @@ __global__ void penalty_kernel(const PenaltyArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The anti-diagonal paths (-1,1) and (1,-1) (CensusSgm.java:421-459, direction table entries 5
+// and 6) follow the lines x + y = s, which are independent of each other: one warp per line,
+// both views packed as in the sweep.  The forward pass walks (-1,1) from the line's upper-right
+// end and stores its path costs as the line partial; the backward pass walks (1,-1) from the
+// lower-left end, adds its path costs and stores the sum.  Costs, penalty records and (backward)
+// the stored forward costs are prefetched kPrefetch pixels ahead.  Word 3 of the down stream's
+// penalty record of a pixel is pathP2 - P1 towards (x+1, y-1), word 3 of the up stream's record
+// pathP2 - P1 towards (x-1, y+1).
+struct LineArgs {
+  const uint8_t* cost[2];  // [H][W][Dp] per view
+  const uint4* pen;        // [2 streams][H][W] penalty records, stream order
+  uint32_t* part;          // [H][W][Dp] partial aggregate of the two anti-diagonal paths
+  int W, H, D, p1;
+  int* next;  // queue of lines (longest first) shared with the sweep's line warps; null: a warp
+              // per line
+};
+
+constexpr int kLineWarps = 8;
+constexpr int kPrefetch = 8;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Per-warp ring of kPrefetch pixel slots: costs of both views (Dp bytes each), the penalty record
+// (16 bytes) and, on the return pass, the stored forward costs (Dp x 4 bytes).
+template <int REGS>
+struct LineSlot {
+  static constexpr int Dp = 32 * REGS;
+  static constexpr int cost = 0, pen = 2 * Dp, part = 2 * Dp + 16;
+  static constexpr int bytes = 2 * Dp + 16 + 4 * Dp;
+};
+
+// Queue position idx -> line x + y = s, longest lines first: the min(W, H)-pixel plateau, then
+// the two ramps from their long ends, alternately.
+__device__ __forceinline__ int line_of(int idx, int W, int H) {
+  const int m = min(W, H), M = max(W, H), plateau = M - m + 1;
+  if (idx < plateau) return m - 1 + idx;
+  const int j = idx - plateau, k = j / 2 + 1;
+  return (j & 1) ? M - 1 + k : m - 1 - k;
+}
+__device__ __forceinline__ int line_len_at(int idx, int W, int H) {
+  const int m = min(W, H), plateau = max(W, H) - m + 1;
+  return idx < plateau ? m : m - ((idx - plateau) / 2 + 1);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Aggregation sweep.  Both views of one image row live in one warp: every 32-bit register holds
 // one disparity of the left view (low half) and the same disparity of the right view (high
 // half), lane l owning disparities l*REGS .. l*REGS+REGS-1.  The d-1 / d+1 neighbours of a
@@ -406,6 +460,8 @@ struct SweepArgs {
   int* error;
   int W, H, D, nb, p1;
   long long timeout;
+  LineArgs line;  // the anti-diagonal lines taken by the sweep's line warps (LW > 0)
+  int line_slack;  // a line warp takes a line of len pixels while 100 * len <= slack * pixels left
 };
 
 // Shared-memory layout (byte offsets) of one sweep CTA.
@@ -428,6 +484,9 @@ struct SweepLayout {
   static constexpr int carry = ring + R * RING * vslot;
   static constexpr int zero = carry + CS * K * vslot;  // a pixel slot of zeros
   static constexpr int total = zero + vslot;
+  // Rings of the line warps, kPrefetch LineSlots each.
+  static constexpr int lines = (total + 127) / 128 * 128;
+  static constexpr int with_lines(int lw) { return lines + lw * kPrefetch * LineSlot<REGS>::bytes; }
 };
 
 __device__ __forceinline__ int ld_acquire_cta(const int* p) {
@@ -675,11 +734,158 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
   }
 }
 
-// One CTA = R row warps + a carry-in warp + a publisher warp, one row block of one stream.
+// One warp walks line x + y = `line` forward and back; `ring` is the warp's shared-memory ring of
+// kPrefetch LineSlots.  Returns with no copy in flight.
+template <int REGS>
+__device__ __forceinline__ void walk_line(const LineArgs& a, int line, uint32_t ring, int lane) {
+  constexpr int Dp = 32 * REGS, CH = Dp / 16;  // 16-byte chunks per view's cost line
+  using S = LineSlot<REGS>;
+  const int W = a.W, H = a.H;
+  const int x0 = min(line, W - 1), y0 = line - x0;  // upper-right end of the line
+  const int len = min(x0 + 1, H - y0);               // pixel i: (x0 - i, y0 + i)
+  const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
+  const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
+  uint32_t pad[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
+  const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
+  uint32_t* part = a.part + lane * REGS;
+  const int64_t step = (int64_t)W - 1;  // pixel-index step along the line (down-left)
+  const int64_t p0 = (int64_t)y0 * W + x0;
+
+  // Issues the copies of pixel i into ring slot `slot` as one commit group (empty if i is off
+  // the line, so the group count stays in step).
+  auto fetch = [&](int slot, int i, bool back) {
+    if (i >= 0 && i < len) {
+      const int64_t p = p0 + i * step;
+      const uint32_t s = ring + slot * S::bytes;
+      if (lane < 2 * CH) {
+        const int view = lane / CH, chunk = lane % CH;
+        cp_async16(s + S::cost + view * Dp + chunk * 16,
+                   (view ? a.cost[1] : a.cost[0]) + p * Dp + chunk * 16);
+      }
+      if (lane == 31) {
+        const int y = y0 + i, x = x0 - i;
+        const uint4* rec = back ? &a.pen[((int64_t)H + (H - 1 - y)) * W + (W - 1 - x)]
+                                : &a.pen[p];
+        cp_async16(s + S::pen, rec);
+      }
+      if (back) {
+#pragma unroll
+        for (int c = lane; c < Dp / 4; c += 32)
+          cp_async16(s + S::part + c * 16, a.part + p * Dp + c * 4);
+      }
+    }
+    cp_async_commit();
+  };
+  // Consumes ring slot `slot`: this lane's widened costs, penalty and texture words.
+  auto take = [&](int slot, uint32_t (&c)[REGS], uint32_t& pq, uint32_t& pt) {
+    const uint32_t s = ring + slot * S::bytes;
+    widen_costs<REGS>(s + S::cost + lane * REGS, s + S::cost + Dp + lane * REGS, pad, c);
+    const uint4 r = lds_v4(s + S::pen);
+    pq = r.w;
+    pt = r.x;
+  };
+
+  PathState<REGS> cur;
+  // Forward: (-1,1), pixel i's predecessor is pixel i - 1.
+  zero_state(cur);
+#pragma unroll
+  for (int k = 0; k < kPrefetch; k++) fetch(k, k, false);
+  for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; k++) {
+      const int i = base + k;
+      if (i < len) {
+        cp_async_wait<kPrefetch - 1>();
+        __syncwarp();
+        uint32_t c[REGS], pq, pt;
+        take(k, c, pq, pt);
+        __syncwarp();  // every lane has read the slot before it is refilled
+        fetch(k, i + kPrefetch, false);
+        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+        const uint32_t keep = prmt(pt, 0, 0xbb99u);
+        PathState<REGS> prev[1] = {cur}, out[1];
+        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+        store_words<REGS>(part + (p0 + i * step) * Dp, out[0].v);
+        cur = out[0];
+        if (keep != 0xffffffffu) {
+#pragma unroll
+          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+          cur.m &= keep;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  // The return pass copies the stored forward costs back from L2 (cp.async.cg), some of them
+  // written by other lanes just now: every lane's stores reach L2 before any lane copies.
+  __threadfence();
+  __syncwarp();
+  // Backward: (1,-1), pixel i's predecessor is pixel i + 1; adds to the stored forward costs.
+  zero_state(cur);
+#pragma unroll
+  for (int k = 0; k < kPrefetch; k++) fetch(k, len - 1 - k, true);
+  for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; k++) {
+      const int i = len - 1 - (base + k);
+      if (i >= 0) {
+        cp_async_wait<kPrefetch - 1>();
+        __syncwarp();
+        uint32_t c[REGS], pq, pt, fwd[REGS];
+        take(k, c, pq, pt);
+        lds_words<REGS>(ring + k * S::bytes + S::part + lane * REGS * 4, fwd);
+        __syncwarp();
+        fetch(k, i - kPrefetch, true);
+        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+        const uint32_t keep = prmt(pt, 0, 0xbb99u);
+        PathState<REGS> prev[1] = {cur}, out[1];
+        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+        uint32_t sum[REGS];
+#pragma unroll
+        for (int j = 0; j < REGS; j++) sum[j] = fwd[j] + out[0].v[j];
+        store_words_cs<REGS>(part + (p0 + i * step) * Dp, sum);
+        cur = out[0];
+        if (keep != 0xffffffffu) {
+#pragma unroll
+          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+          cur.m &= keep;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+template <int REGS>
+__global__ void __launch_bounds__(kLineWarps * 32) lines_kernel(const LineArgs a) {
+  extern __shared__ __align__(16) uint8_t lsm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t ring = smem_u32(lsm) + warp * kPrefetch * LineSlot<REGS>::bytes;
+  const int lines = a.W + a.H - 1;
+  if (!a.next) {
+    const int line = blockIdx.x * kLineWarps + warp;
+    if (line < lines) walk_line<REGS>(a, line, ring, lane);
+    return;
+  }
+  // The lines the sweep's line warps left: taken from the queue until it is empty.
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(a.next, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= lines) return;
+    walk_line<REGS>(a, line_of(idx, a.W, a.H), ring, lane);
+  }
+}
+
+// One CTA = R row warps + a carry-in warp + a publisher warp (+ LW line warps), one row block of
+// one stream.
 //  * "down" (stream 0) runs rows top to bottom and pixels left to right and owns (1,0), (0,1),
 //    (1,1) (NPATH = 3; (1,0), (0,1) in 4-path mode, NPATH = 2); "up" (stream 1) is the same code
 //    on the image mirrored in x and y and owns the opposite paths.  The anti-diagonal paths,
-//    whose predecessor lies one pixel ahead in the row above, are lines_kernel's.
+//    whose predecessor lies one pixel ahead in the row above, are walked line by line: by the
+//    line warps (walk_line) on the issue slots the row warps leave idle, or by lines_kernel.
 //  * Row warp w holds stream row b*R + w of both views and processes stream pixel xs at step
 //    xs + w; the row warps meet at a named barrier once per step.  The vertical path states of
 //    a pixel reach the next row through a shared-memory ring; the (1,0) state stays in registers.
@@ -690,8 +896,11 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
 //    GPU-scope fence (both off the row warps' critical path).
 //  * CTAs take tickets in launch order and only wait on lower tickets, so the schedule cannot
 //    deadlock even when not every CTA is resident.
-template <int REGS, int NPATH, int K, int R>
-__global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) {
+//  * One CTA per SM at most is planned for, so the compiler may give a thread all the registers
+//    it wants (about 90 at D = 128: 2.39 ms per cfg1 sweep, against 2.71 ms at the 63 it picks
+//    when asked to fit three CTAs).
+template <int REGS, int NPATH, int K, int R, int LW>
+__global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   using L = SweepLayout<REGS, NPATH, K, R>;
   constexpr int Dp = L::Dp, NV = L::NV, RING = L::RING, NB = L::NB, CS = L::CS;
@@ -699,6 +908,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   uint64_t* carry_full = full + R * NB;             // [CS]
   int* carry_consumed = (int*)(smem + L::counters);  // carry chunks row warp 0 no longer needs
   int* published = carry_consumed + 1;              // carry chunks row warp R-1 has written
+  int* row_done = carry_consumed + 2;               // chunks row warp 0 has finished
   uint8_t* carry_buf = smem + L::carry;
   __shared__ int s_ticket;
 
@@ -708,6 +918,7 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
     for (int i = 0; i < R * NB + CS; i++) mbar_init(&full[i], 1);
     *carry_consumed = 0;
     *published = 0;
+    *row_done = 0;
   }
   for (int i = threadIdx.x; i < L::vslot / 4; i += blockDim.x) ((uint32_t*)(smem + L::zero))[i] = 0;
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -762,6 +973,30 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
     // Every issued carry copy lands before the CTA's shared memory is released.
     for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
       wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, limit / 4, 5, false);
+    return;
+  }
+  if (w >= R + 2) {
+    // --------------------------------------------------------------- line warps
+    // Anti-diagonal lines from the queue, longest first, while this block's rows are busy: a
+    // warp takes the next line only if it is no longer than the pixels row warp 0 still has to
+    // go (a line step costs well under half a sweep step), so the line work does not hold the
+    // SM beyond the block's own rows.  The lines nobody took are walked after the sweep.
+    if constexpr (LW > 0) {
+      const uint32_t ring = smem_u32(smem) + L::lines + (w - R - 2) * kPrefetch * LineSlot<REGS>::bytes;
+      const int lines = W + H - 1;
+      for (;;) {
+        int idx = INT_MAX;
+        if (lane == 0) {
+          const int head = *(volatile int*)a.line.next;
+          const int left = W - K * *(volatile int*)row_done;
+          if (head < lines && 100 * line_len_at(head, W, H) <= a.line_slack * left)
+            idx = atomicAdd(a.line.next, 1);
+        }
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= lines) break;
+        walk_line<REGS>(a.line, line_of(idx, W, H), ring, lane);
+      }
+    }
     return;
   }
   if (w == R + 1) {
@@ -936,6 +1171,8 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
         if (c + NB < nchunks) issue_chunk(c + NB);
         if constexpr (PUBLISH) st_release_cta(published, c + 1);
         if constexpr (CARRY_IN) st_release_cta(carry_consumed, c);
+        if constexpr (LW > 0)
+          if (w == 0) *(volatile int*)row_done = c + 1;
       }
       __syncwarp();
       if (c + NB < nchunks) issued = c + NB + 1;
@@ -978,172 +1215,6 @@ __global__ void __launch_bounds__((R + 2) * 32) sweep_kernel(const SweepArgs a) 
   // After an expired wait, give outstanding chunk copies a bounded chance to land before exit.
   for (int cc = max(0, issued - NB); cc < issued; cc++)
     wait_bar(&my_full[cc % NB], (cc / NB) & 1, err, limit / 4, 5, false);
-}
-
-// ---------------------------------------------------------------------------------------------
-// The anti-diagonal paths (-1,1) and (1,-1) (CensusSgm.java:421-459, direction table entries 5
-// and 6) follow the lines x + y = s, which are independent of each other: one warp per line,
-// both views packed as in the sweep.  The forward pass walks (-1,1) from the line's upper-right
-// end and stores its path costs as the line partial; the backward pass walks (1,-1) from the
-// lower-left end, adds its path costs and stores the sum.  Costs, penalty records and (backward)
-// the stored forward costs are prefetched kPrefetch pixels ahead.  Word 3 of the down stream's
-// penalty record of a pixel is pathP2 - P1 towards (x+1, y-1), word 3 of the up stream's record
-// pathP2 - P1 towards (x-1, y+1).
-struct LineArgs {
-  const uint8_t* cost[2];  // [H][W][Dp] per view
-  const uint4* pen;        // [2 streams][H][W] penalty records, stream order
-  uint32_t* part;          // [H][W][Dp] partial aggregate of the two anti-diagonal paths
-  int W, H, D, p1;
-};
-
-constexpr int kLineWarps = 8;
-constexpr int kPrefetch = 8;
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Per-warp ring of kPrefetch pixel slots: costs of both views (Dp bytes each), the penalty record
-// (16 bytes) and, on the return pass, the stored forward costs (Dp x 4 bytes).
-template <int REGS>
-struct LineSlot {
-  static constexpr int Dp = 32 * REGS;
-  static constexpr int cost = 0, pen = 2 * Dp, part = 2 * Dp + 16;
-  static constexpr int bytes = 2 * Dp + 16 + 4 * Dp;
-};
-
-template <int REGS>
-__global__ void __launch_bounds__(kLineWarps * 32) lines_kernel(const LineArgs a) {
-  constexpr int Dp = 32 * REGS, CH = Dp / 16;  // 16-byte chunks per view's cost line
-  using S = LineSlot<REGS>;
-  extern __shared__ __align__(16) uint8_t lsm[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int line = blockIdx.x * kLineWarps + warp;
-  const int W = a.W, H = a.H;
-  if (line >= W + H - 1) return;
-  const uint32_t ring = smem_u32(lsm) + warp * kPrefetch * S::bytes;
-  const int x0 = min(line, W - 1), y0 = line - x0;  // upper-right end of the line
-  const int len = min(x0 + 1, H - y0);               // pixel i: (x0 - i, y0 + i)
-  const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
-  const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
-  uint32_t pad[REGS];
-#pragma unroll
-  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
-  const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
-  uint32_t* part = a.part + lane * REGS;
-  const int64_t step = (int64_t)W - 1;  // pixel-index step along the line (down-left)
-  const int64_t p0 = (int64_t)y0 * W + x0;
-
-  // Issues the copies of pixel i into ring slot `slot` as one commit group (empty if i is off
-  // the line, so the group count stays in step).
-  auto fetch = [&](int slot, int i, bool back) {
-    if (i >= 0 && i < len) {
-      const int64_t p = p0 + i * step;
-      const uint32_t s = ring + slot * S::bytes;
-      if (lane < 2 * CH) {
-        const int view = lane / CH, chunk = lane % CH;
-        cp_async16(s + S::cost + view * Dp + chunk * 16,
-                   (view ? a.cost[1] : a.cost[0]) + p * Dp + chunk * 16);
-      }
-      if (lane == 31) {
-        const int y = y0 + i, x = x0 - i;
-        const uint4* rec = back ? &a.pen[((int64_t)H + (H - 1 - y)) * W + (W - 1 - x)]
-                                : &a.pen[p];
-        cp_async16(s + S::pen, rec);
-      }
-      if (back) {
-#pragma unroll
-        for (int c = lane; c < Dp / 4; c += 32)
-          cp_async16(s + S::part + c * 16, a.part + p * Dp + c * 4);
-      }
-    }
-    cp_async_commit();
-  };
-  // Consumes ring slot `slot`: this lane's widened costs, penalty and texture words.
-  auto take = [&](int slot, uint32_t (&c)[REGS], uint32_t& pq, uint32_t& pt) {
-    const uint32_t s = ring + slot * S::bytes;
-    widen_costs<REGS>(s + S::cost + lane * REGS, s + S::cost + Dp + lane * REGS, pad, c);
-    const uint4 r = lds_v4(s + S::pen);
-    pq = r.w;
-    pt = r.x;
-  };
-
-  PathState<REGS> cur;
-  // Forward: (-1,1), pixel i's predecessor is pixel i - 1.
-  zero_state(cur);
-#pragma unroll
-  for (int k = 0; k < kPrefetch; k++) fetch(k, k, false);
-  for (int base = 0; base < len; base += kPrefetch) {
-#pragma unroll
-    for (int k = 0; k < kPrefetch; k++) {
-      const int i = base + k;
-      if (i < len) {
-        cp_async_wait<kPrefetch - 1>();
-        __syncwarp();
-        uint32_t c[REGS], pq, pt;
-        take(k, c, pq, pt);
-        __syncwarp();  // every lane has read the slot before it is refilled
-        fetch(k, i + kPrefetch, false);
-        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
-        const uint32_t keep = prmt(pt, 0, 0xbb99u);
-        PathState<REGS> prev[1] = {cur}, out[1];
-        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
-        store_words<REGS>(part + (p0 + i * step) * Dp, out[0].v);
-        cur = out[0];
-        if (keep != 0xffffffffu) {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
-          cur.m &= keep;
-        }
-      }
-    }
-  }
-  cp_async_wait<0>();
-  // The return pass copies the stored forward costs back from L2 (cp.async.cg), some of them
-  // written by other lanes just now: every lane's stores reach L2 before any lane copies.
-  __threadfence();
-  __syncwarp();
-  // Backward: (1,-1), pixel i's predecessor is pixel i + 1; adds to the stored forward costs.
-  zero_state(cur);
-#pragma unroll
-  for (int k = 0; k < kPrefetch; k++) fetch(k, len - 1 - k, true);
-  for (int base = 0; base < len; base += kPrefetch) {
-#pragma unroll
-    for (int k = 0; k < kPrefetch; k++) {
-      const int i = len - 1 - (base + k);
-      if (i >= 0) {
-        cp_async_wait<kPrefetch - 1>();
-        __syncwarp();
-        uint32_t c[REGS], pq, pt, fwd[REGS];
-        take(k, c, pq, pt);
-        lds_words<REGS>(ring + k * S::bytes + S::part + lane * REGS * 4, fwd);
-        __syncwarp();
-        fetch(k, i - kPrefetch, true);
-        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
-        const uint32_t keep = prmt(pt, 0, 0xbb99u);
-        PathState<REGS> prev[1] = {cur}, out[1];
-        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
-        uint32_t sum[REGS];
-#pragma unroll
-        for (int j = 0; j < REGS; j++) sum[j] = fwd[j] + out[0].v[j];
-        store_words_cs<REGS>(part + (p0 + i * step) * Dp, sum);
-        cur = out[0];
-        if (keep != 0xffffffffu) {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
-          cur.m &= keep;
-        }
-      }
-    }
-  }
-  cp_async_wait<0>();
 }
 
 template <int REGS>
@@ -1329,17 +1400,18 @@ cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-template <int REGS, int NPATH, int K, int R>
+template <int REGS, int NPATH, int K, int R, int LW>
 cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream, bool exclusive) {
-  auto kernel = sweep_kernel<REGS, NPATH, K, R>;
+  auto kernel = sweep_kernel<REGS, NPATH, K, R, LW>;
+  using L = SweepLayout<REGS, NPATH, K, R>;
   // Exclusive: at least 116 KB so that one CTA holds an SM alone (two row blocks on one SM halve
   // each other's step rate, while a later block never needs an SM before an earlier one
   // finishes).  Batched pairs instead share SMs, filling each other's idle issue slots.
-  const int shared = exclusive ? std::max(SweepLayout<REGS, NPATH, K, R>::total, 116 * 1024)
-                               : SweepLayout<REGS, NPATH, K, R>::total;
+  const int need = LW > 0 ? L::with_lines(LW) : L::total;
+  const int shared = exclusive ? std::max(need, 116 * 1024) : need;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
   if (e != cudaSuccess) return e;
-  kernel<<<2 * a.nb, (R + 2) * 32, shared, stream>>>(a);
+  kernel<<<2 * a.nb, (R + 2 + LW) * 32, shared, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -1356,6 +1428,66 @@ int rows_for(int regs) {
     return v == 4 || v == 8 ? v : 0;
   }();
   return forced ? forced : rows_default(regs);
+}
+
+// Line warps per sweep CTA in 8-path mode: the anti-diagonal lines run inside the sweep's CTAs on
+// the issue slots the row warps leave idle, when the line rings fit beside the sweep's shared
+// memory (227 KB per CTA); 0 runs them as a separate kernel before the sweep.
+// CSGM_SWEEP_LINE_WARPS (0, 4 or 8) overrides the default for tuning runs.
+constexpr int kSweepLineWarps = 8;
+constexpr int kMaxSharedPerBlock = 227 * 1024;
+
+template <int REGS, int R>
+int sweep_smem_with_lines(int lw) { return SweepLayout<REGS, 3, kChunk, R>::with_lines(lw); }
+
+int line_warps_for(int regs, int rows) {
+  static const int forced = [] {
+    const char* e = getenv("CSGM_SWEEP_LINE_WARPS");
+    const int v = e ? atoi(e) : -1;
+    return v == 0 || v == 4 || v == 8 ? v : -1;
+  }();
+  int lw = forced >= 0 ? forced : kSweepLineWarps;
+  auto smem = [&](int l) {
+    switch (regs * 16 + rows) {
+      case 2 * 16 + 4: return sweep_smem_with_lines<2, 4>(l);
+      case 2 * 16 + 8: return sweep_smem_with_lines<2, 8>(l);
+      case 4 * 16 + 4: return sweep_smem_with_lines<4, 4>(l);
+      case 4 * 16 + 8: return sweep_smem_with_lines<4, 8>(l);
+      case 6 * 16 + 4: return sweep_smem_with_lines<6, 4>(l);
+      case 6 * 16 + 8: return sweep_smem_with_lines<6, 8>(l);
+      case 8 * 16 + 4: return sweep_smem_with_lines<8, 4>(l);
+      default: return sweep_smem_with_lines<8, 8>(l);
+    }
+  };
+  while (lw > 0 && smem(lw) > kMaxSharedPerBlock) lw -= 4;
+  return lw;
+}
+
+// How much of a block's remaining row pixels a line may take (percent): a line warp's pixel costs
+// well under half a sweep step, so 100 leaves slack.  CSGM_SWEEP_LINE_SLACK overrides it for
+// tuning runs.
+int line_slack() {
+  static const int v = [] {
+    const char* e = getenv("CSGM_SWEEP_LINE_SLACK");
+    const int x = e ? atoi(e) : 0;
+    return x >= 10 && x <= 1000 ? x : 100;
+  }();
+  return v;
+}
+
+template <int REGS, int NPATH>
+cudaError_t launch_sweep_for(const SweepArgs& a, cudaStream_t stream, bool exclusive, int rows,
+                             int lw) {
+  if constexpr (NPATH == 3) {
+    if (lw == 8)
+      return rows == 8 ? launch_sweep<REGS, 3, kChunk, 8, 8>(a, stream, exclusive)
+                       : launch_sweep<REGS, 3, kChunk, 4, 8>(a, stream, exclusive);
+    if (lw == 4)
+      return rows == 8 ? launch_sweep<REGS, 3, kChunk, 8, 4>(a, stream, exclusive)
+                       : launch_sweep<REGS, 3, kChunk, 4, 4>(a, stream, exclusive);
+  }
+  return rows == 8 ? launch_sweep<REGS, NPATH, kChunk, 8, 0>(a, stream, exclusive)
+                   : launch_sweep<REGS, NPATH, kChunk, 4, 0>(a, stream, exclusive);
 }
 
 struct FusedLayout {
@@ -1461,20 +1593,25 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     if (le != cudaSuccess) return cuda_fail(le, "penalty kernel launch");
     ctx.prof->kernel_end("penalty");
   }
-  if (sum_lines) {
-    // The anti-diagonal lines, on the pair's own stream before the sweep (beside the sweep on a
-    // second stream they slowed it by more than their own run time: 4.63 ms per pair against
-    // 4.47 ms one after the other).
-    LineArgs la{{cost_l, cost_r}, pen, sum_lines, w, h, p.disparities, p.p1};
+  const int regs = F.Dp / 32;
+  // The anti-diagonal lines: inside the sweep's CTAs (line warps), or as their own kernel on the
+  // pair's stream before the sweep (beside the sweep on a second stream they slowed it by more
+  // than their own run time: 4.63 ms per pair against 4.47 ms one after the other).
+  const int line_warps = sum_lines && ctx.lines_in_sweep ? line_warps_for(regs, F.rows) : 0;
+  LineArgs la{{cost_l, cost_r}, pen, sum_lines, w, h, p.disparities, p.p1,
+              line_warps ? flags + 2 * F.nb + 2 : nullptr};
+  auto run_lines = [&](cudaStream_t stream) {
+    switch (regs) {
+      case 2: return launch_lines<2>(la, stream);
+      case 4: return launch_lines<4>(la, stream);
+      case 6: return launch_lines<6>(la, stream);
+      default: return launch_lines<8>(la, stream);
+    }
+  };
+  if (sum_lines && !line_warps) {
     cudaError_t le;
     ctx.prof->kernel_begin();
-    switch (F.Dp / 32) {
-      case 2: le = launch_lines<2>(la, ctx.stream); break;
-      case 4: le = launch_lines<4>(la, ctx.stream); break;
-      case 6: le = launch_lines<6>(la, ctx.stream); break;
-      case 8: le = launch_lines<8>(la, ctx.stream); break;
-      default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
-    }
+    le = run_lines(ctx.stream);
     if (le != cudaSuccess) return cuda_fail(le, "line kernel launch");
     ctx.prof->kernel_end("lines");
   }
@@ -1498,7 +1635,8 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.nb = F.nb;
   a.p1 = p.p1;
   a.timeout = 4000000000LL;  // ~2 s at 2 GHz
-  const int regs = F.Dp / 32;
+  a.line = la;
+  a.line_slack = line_slack();
   const bool eight = p.directions == 8;
   // Batched pairs launch the sweep on a high-priority stream: its pending CTAs then take SMs ahead
   // of other pairs' bandwidth-bound kernels, so a pair's chain of row blocks is not held up.
@@ -1510,32 +1648,32 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     sweep_stream = ctx.sweep_stream;
   }
   ctx.prof->kernel_begin();
-  switch (regs * 4 + (eight ? 2 : 0) + (F.rows == 8 ? 1 : 0)) {
-#define CSGM_SWEEP_CASE(R_, NP_)                                                       \
-  case R_ * 4 + (NP_ == 3 ? 2 : 0):                                                   \
-    e = launch_sweep<R_, NP_, kChunk, 4>(a, sweep_stream, ctx.exclusive_sweep);       \
-    break;                                                                             \
-  case R_ * 4 + (NP_ == 3 ? 2 : 0) + 1:                                               \
-    e = launch_sweep<R_, NP_, kChunk, 8>(a, sweep_stream, ctx.exclusive_sweep);       \
-    break;
-    CSGM_SWEEP_CASE(2, 2)
-    CSGM_SWEEP_CASE(2, 3)
-    CSGM_SWEEP_CASE(4, 2)
-    CSGM_SWEEP_CASE(4, 3)
-    CSGM_SWEEP_CASE(6, 2)
-    CSGM_SWEEP_CASE(6, 3)
-    CSGM_SWEEP_CASE(8, 2)
-    CSGM_SWEEP_CASE(8, 3)
-#undef CSGM_SWEEP_CASE
+  switch (regs * 2 + (eight ? 1 : 0)) {
+    case 2 * 2: e = launch_sweep_for<2, 2>(a, sweep_stream, ctx.exclusive_sweep, F.rows, 0); break;
+    case 2 * 2 + 1: e = launch_sweep_for<2, 3>(a, sweep_stream, ctx.exclusive_sweep, F.rows, line_warps); break;
+    case 4 * 2: e = launch_sweep_for<4, 2>(a, sweep_stream, ctx.exclusive_sweep, F.rows, 0); break;
+    case 4 * 2 + 1: e = launch_sweep_for<4, 3>(a, sweep_stream, ctx.exclusive_sweep, F.rows, line_warps); break;
+    case 6 * 2: e = launch_sweep_for<6, 2>(a, sweep_stream, ctx.exclusive_sweep, F.rows, 0); break;
+    case 6 * 2 + 1: e = launch_sweep_for<6, 3>(a, sweep_stream, ctx.exclusive_sweep, F.rows, line_warps); break;
+    case 8 * 2: e = launch_sweep_for<8, 2>(a, sweep_stream, ctx.exclusive_sweep, F.rows, 0); break;
+    case 8 * 2 + 1: e = launch_sweep_for<8, 3>(a, sweep_stream, ctx.exclusive_sweep, F.rows, line_warps); break;
     default: return fail(CSGM_E_UNSUPPORTED, "fused path: unsupported D");
   }
   if (e != cudaSuccess) return cuda_fail(e, "sweep kernel launch");
+  ctx.prof->kernel_end("sweep");
+  if (line_warps) {
+    // The lines the sweep's line warps did not take (a queue that is already empty costs one
+    // short launch).
+    ctx.prof->kernel_begin();
+    e = run_lines(sweep_stream);
+    if (e != cudaSuccess) return cuda_fail(e, "line kernel launch");
+    ctx.prof->kernel_end("lines_rest");
+  }
   if (ctx.sweep_stream) {
     e = cudaEventRecord(ctx.sweep_done, ctx.sweep_stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx.stream, ctx.sweep_done, 0);
     if (e != cudaSuccess) return cuda_fail(e, "sweep stream ordering");
   }
-  ctx.prof->kernel_end("sweep");
 
   WtaArgs t{};
   t.down = sum_down;
