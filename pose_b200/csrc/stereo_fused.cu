@@ -1230,11 +1230,14 @@ cudaError_t launch_lines(const LineArgs& a, cudaStream_t stream) {
 
 // ---------------------------------------------------------------------------------------------
 // Winner-take-all, uniqueness and sub-pixel selection of both views (CensusSgm.java:460-515).
-// One warp per pixel: lane l adds the two streams' partial aggregates of its REGS disparities
-// (both views packed), the first strict minimum and the second minimum outside best-1..best+1
-// are warp reductions of (total << 8 | k) keys, and lane v then selects view v.  A total of at
-// least `invalid` (directions x 512) marks a cell whose cost is invalid: every valid total is
-// smaller because each valid path cost is at most bits + P2 < 512.
+// A warp takes pixels 16 at a time.  Per pixel, lane l adds the partial aggregates (down, up and
+// the anti-diagonal lines) of its REGS disparities, both views packed, and the first strict
+// minimum and the second minimum outside best-1..best+1 are warp reductions of (total << 8 | k)
+// keys; lanes 0/1 note the record of view 0/1.  Then every lane runs the FP64 selection of one
+// (pixel, view) record of the group, so the long selection chain runs 32 at a time instead of 2.
+// The partials arrive through a per-warp cp.async ring two pixels deep.  A total of at least
+// `invalid` (directions x 512) marks a cell whose cost is invalid: every valid total is smaller
+// because each valid path cost is at most bits + P2 < 512.
 struct WtaArgs {
   const uint32_t* down;  // [H][W][Dp] left | right << 16
   const uint32_t* up;
@@ -1303,82 +1306,120 @@ __device__ __forceinline__ void select_pixel_record(int best, int value, int sec
 
 constexpr int kWtaWarps = 8;
 
-template <int REGS>
+template <int REGS, int PF>
 __global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
   constexpr int Dp = 32 * REGS;
+  constexpr int kSlot = 3 * Dp * 4;  // one pixel's down, up and lines partials
+  constexpr int G = 16;              // pixels per group: 16 pixels x 2 views = one per lane
+  extern __shared__ __align__(16) uint8_t wsm[];
   __shared__ __align__(16) uint32_t stage[kWtaWarps][Dp];
+  __shared__ int4 rec_a[kWtaWarps][2 * G];  // best, value, second, before of (pixel, view)
+  __shared__ int rec_b[kWtaWarps][2 * G];   // after | flags << 16
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t ring = smem_u32(wsm) + warp * PF * kSlot;
   const uint16_t* t16 = (const uint16_t*)stage[warp] + lane;  // view `lane` of k at t16[2k]
   const int W = a.W, H = a.H, D = a.D, invalid = a.invalid;
   const int64_t n = (int64_t)W * H;
   const int64_t stride = (int64_t)gridDim.x * kWtaWarps;
   unsigned counts[6] = {0, 0, 0, 0, 0, 0};
-  // Software pipeline: the next pixel's aggregates are in flight while this one is selected.
-  uint32_t d[REGS], u[REGS], g[REGS];
+  // The partials of this warp's next PF pixels are in flight (cp.async into a shared-memory ring,
+  // one commit group per pixel, empty past the end) while one pixel's minima are found.
   const bool three = a.lines != nullptr;
-#pragma unroll
-  for (int j = 0; j < REGS; j++) g[j] = 0;
-  int64_t p = (int64_t)blockIdx.x * kWtaWarps + warp;
-  if (p < n) {
-    load_words<REGS>(a.down + p * Dp + lane * REGS, d);
-    load_words<REGS>(a.up + p * Dp + lane * REGS, u);
-    if (three) load_words<REGS>(a.lines + p * Dp + lane * REGS, g);
-  }
-  for (; p < n; p += stride) {
-    const int y = (int)(p / W), x = (int)(p - (int64_t)y * W);
-    uint32_t tot[REGS];
-#pragma unroll
-    for (int j = 0; j < REGS; j++) tot[j] = d[j] + u[j] + g[j];
-    if (p + stride < n) {
-      load_words<REGS>(a.down + (p + stride) * Dp + lane * REGS, d);
-      load_words<REGS>(a.up + (p + stride) * Dp + lane * REGS, u);
-      if (three) load_words<REGS>(a.lines + (p + stride) * Dp + lane * REGS, g);
+  auto fetch = [&](int slot, int64_t q) {
+    if (q < n) {
+      const uint32_t sl = ring + slot * kSlot;
+      for (int c = lane; c < Dp / 4; c += 32) {
+        cp_async16(sl + c * 16, a.down + q * Dp + c * 4);
+        cp_async16(sl + Dp * 4 + c * 16, a.up + q * Dp + c * 4);
+        if (three) cp_async16(sl + 2 * Dp * 4 + c * 16, a.lines + q * Dp + c * 4);
+      }
     }
-    int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
-    if (y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx) {
-      // Pass 1: first strict minimum, as key = total << 8 | k.
-      uint32_t k0 = 0xffffffffu, k1 = 0xffffffffu;
+    cp_async_commit();
+  };
+  const int64_t first = (int64_t)blockIdx.x * kWtaWarps + warp;
 #pragma unroll
-      for (int j = 0; j < REGS; j++) {
-        const uint32_t k = lane * REGS + j;
-        k0 = min(k0, ((tot[j] << 8) & 0xffff00u) | k);
-        k1 = min(k1, ((tot[j] >> 8) & 0xffff00u) | k);
-      }
-      k0 = __reduce_min_sync(0xffffffffu, k0);
-      k1 = __reduce_min_sync(0xffffffffu, k1);
-      // Pass 2: minimum outside best-1..best+1.
-      const int b0 = (int)(k0 & 0xffu), b1 = (int)(k1 & 0xffu);
-      uint32_t s0 = 0xffffu, s1 = 0xffffu;
-#pragma unroll
-      for (int j = 0; j < REGS; j++) {
-        const int k = lane * REGS + j;
-        if ((unsigned)(k - b0 + 1) > 2u) s0 = min(s0, tot[j] & 0xffffu);
-        if ((unsigned)(k - b1 + 1) > 2u) s1 = min(s1, tot[j] >> 16);
-      }
-      s0 = __reduce_min_sync(0xffffffffu, s0);
-      s1 = __reduce_min_sync(0xffffffffu, s1);
-      store_words<REGS>(stage[warp] + lane * REGS, tot);
+  for (int k = 0; k < PF; k++) fetch(k, first + k * stride);
+  int slot = 0;
+  // Groups of G of this warp's pixels: the minima of each pixel by warp reductions (whole warp),
+  // then the selection of the group's 2G (pixel, view) records, one per lane, side by side.
+  for (int64_t base = first; base < n; base += G * stride) {
+    for (int i = 0; i < G; i++) {
+      const int64_t p = base + i * stride;
+      if (p >= n) break;
+      const int y = (int)(p / W), x = (int)(p - (int64_t)y * W);
+      cp_async_wait<PF - 1>();
       __syncwarp();
-      if (lane < 2) {
-        const uint32_t key = lane ? k1 : k0;
-        if ((int)(key >> 8) < invalid) {
-          best = (int)(key & 0xffu);
-          value = (int)(key >> 8);
-          const int sec = (int)(lane ? s1 : s0);
-          second = sec < invalid ? sec : INT_MAX;
-          if (best >= 1 && t16[2 * (best - 1)] < invalid) before = t16[2 * (best - 1)];
-          if (best + 1 < D && t16[2 * (best + 1)] < invalid) after = t16[2 * (best + 1)];
-          flags = (t16[0] < invalid ? 1 : 0) | (t16[2 * (D - 1)] < invalid ? 2 : 0);
+      uint32_t tot[REGS], u[REGS], g[REGS] = {};
+      const uint32_t sl = ring + slot * kSlot + lane * REGS * 4;
+      lds_words<REGS>(sl, tot);
+      lds_words<REGS>(sl + Dp * 4, u);
+      if (three) lds_words<REGS>(sl + 2 * Dp * 4, g);
+#pragma unroll
+      for (int j = 0; j < REGS; j++) tot[j] += u[j] + g[j];
+      __syncwarp();  // every lane has read the slot before it is refilled
+      fetch(slot, p + PF * stride);
+      slot = slot + 1 == PF ? 0 : slot + 1;
+      int best = -1, value = 0, second = INT_MAX, before = -1, after = -1, flags = 0;
+      if (y >= a.ry && y < H - a.ry && x >= a.rx && x < W - a.rx) {
+        // Pass 1: first strict minimum, as key = total << 8 | k.
+        uint32_t k0 = 0xffffffffu, k1 = 0xffffffffu;
+#pragma unroll
+        for (int j = 0; j < REGS; j++) {
+          const uint32_t k = lane * REGS + j;
+          k0 = min(k0, ((tot[j] << 8) & 0xffff00u) | k);
+          k1 = min(k1, ((tot[j] >> 8) & 0xffff00u) | k);
         }
+        k0 = __reduce_min_sync(0xffffffffu, k0);
+        k1 = __reduce_min_sync(0xffffffffu, k1);
+        // Pass 2: minimum outside best-1..best+1.
+        const int b0 = (int)(k0 & 0xffu), b1 = (int)(k1 & 0xffu);
+        uint32_t s0 = 0xffffu, s1 = 0xffffu;
+#pragma unroll
+        for (int j = 0; j < REGS; j++) {
+          const int k = lane * REGS + j;
+          if ((unsigned)(k - b0 + 1) > 2u) s0 = min(s0, tot[j] & 0xffffu);
+          if ((unsigned)(k - b1 + 1) > 2u) s1 = min(s1, tot[j] >> 16);
+        }
+        s0 = __reduce_min_sync(0xffffffffu, s0);
+        s1 = __reduce_min_sync(0xffffffffu, s1);
+        store_words<REGS>(stage[warp] + lane * REGS, tot);
+        __syncwarp();
+        if (lane < 2) {
+          const uint32_t key = lane ? k1 : k0;
+          if ((int)(key >> 8) < invalid) {
+            best = (int)(key & 0xffu);
+            value = (int)(key >> 8);
+            const int sec = (int)(lane ? s1 : s0);
+            second = sec < invalid ? sec : INT_MAX;
+            if (best >= 1 && t16[2 * (best - 1)] < invalid) before = t16[2 * (best - 1)];
+            if (best + 1 < D && t16[2 * (best + 1)] < invalid) after = t16[2 * (best + 1)];
+            flags = (t16[0] < invalid ? 1 : 0) | (t16[2 * (D - 1)] < invalid ? 2 : 0);
+          }
+        }
+        __syncwarp();
       }
-      __syncwarp();
+      if (lane < 2) {
+        rec_a[warp][2 * i + lane] = make_int4(best, value, second, before);
+        rec_b[warp][2 * i + lane] = (after & 0xffff) | flags << 16;
+      }
     }
-    if (lane < 2)
-      select_pixel_record(best, value, second, before, after, flags, D, a.min_disparity,
-                          a.uniqueness, (lane ? a.disp[1] : a.disp[0]) + p,
-                          lane == 0 && a.reasons ? a.reasons + p : nullptr,
-                          lane == 0 && a.boundary ? a.boundary + p : nullptr, counts, lane == 0);
+    __syncwarp();
+    {
+      const int i = lane >> 1, view = lane & 1;
+      const int64_t p = base + i * stride;
+      if (p < n) {
+        const int4 r = rec_a[warp][lane];
+        const int rb = rec_b[warp][lane];
+        const int after = (int)(int16_t)(rb & 0xffff), flags = rb >> 16;
+        select_pixel_record(r.x, r.y, r.z, r.w, after, flags, D, a.min_disparity, a.uniqueness,
+                            (view ? a.disp[1] : a.disp[0]) + p,
+                            view == 0 && a.reasons ? a.reasons + p : nullptr,
+                            view == 0 && a.boundary ? a.boundary + p : nullptr, counts, view == 0);
+      }
+    }
+    __syncwarp();
   }
+  cp_async_wait<0>();
   if (a.stats) {
     unsigned long long* dst[6] = {&a.stats->lower_boundary_rejected,
                                   &a.stats->full_interval_pixels, &a.stats->boundary_rejected,
@@ -1392,12 +1433,22 @@ __global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
   }
 }
 
-template <int REGS>
-cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
+template <int REGS, int PF>
+cudaError_t launch_wta_t(const WtaArgs& a, int sm_count, cudaStream_t stream) {
+  auto kernel = wta_kernel<REGS, PF>;
+  const int shared = kWtaWarps * PF * 3 * 32 * REGS * 4;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
+  if (e != cudaSuccess) return e;
   const int64_t n = (int64_t)a.W * a.H;
   const int grid = (int)std::min<int64_t>((n + kWtaWarps - 1) / kWtaWarps, (int64_t)sm_count * 8);
-  wta_kernel<REGS><<<grid, kWtaWarps * 32, 0, stream>>>(a);
+  kernel<<<grid, kWtaWarps * 32, shared, stream>>>(a);
   return cudaGetLastError();
+}
+
+// Two pixels in flight per warp: more (4) measured the same, and its ring costs a CTA per SM.
+template <int REGS>
+cudaError_t launch_wta(const WtaArgs& a, int sm_count, cudaStream_t stream) {
+  return launch_wta_t<REGS, 2>(a, sm_count, stream);
 }
 
 template <int REGS, int NPATH, int K, int R, int LW>
