@@ -118,15 +118,20 @@ __device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* er
 
 // ---------------------------------------------------------------------------------------------
 // Cost volumes of both views (uint8, 0x80 = invalid), StereoCost.value semantics
-// (StereoCost.java:50-90) with CensusSgm.java:405-420 validity.  A CTA item is a segment of
-// kCostSeg pixels of one row of one view.  The segment's descriptors and the target view's
-// descriptors over the disparity span are staged in shared memory, each target with a validity
-// byte (inside [r, w-r) and textured) and, for the blended modes, its gray value or packed
-// central-difference gradient.  Thread t computes pixel t % kCostSeg for a slice of disparity
-// groups (consecutive threads read consecutive targets: no bank conflicts) into a padded tile
-// that the CTA then writes out as coalesced 16-byte stores.  The blended modes divide by
-// 1000 * cap through an exact 64-bit reciprocal (floor(n * ceil(2^64 / d) / 2^64) == n / d for
-// n, d < 2^32).  ZNCC (FP64 window sums) stays on the general per-cell path.
+// (StereoCost.java:50-90) with CensusSgm.java:405-420 validity.  The right view's cost of pixel
+// x' at disparity index k is the left view's cost of pixel x' + min_disparity + k at k: the same
+// two descriptors, the same validity (both pixels inside [r, w-r) and textured, the row inside)
+// and a symmetric cost.  So each cell is computed once: a CTA takes one image row, computes the
+// left view in segments of kCostSeg pixels into a shared-memory ring of left-view cost rows, writes
+// them out, and gathers each right-view segment from the ring's diagonals as soon as every left
+// pixel it needs is in the ring.  Per left segment the segment's descriptors and the target
+// view's descriptors over the disparity span are staged in shared memory, each target with a
+// validity byte and, for the blended modes, its gray value or packed central-difference
+// gradient.  Thread t computes pixel t % kCostSeg for a slice of disparity groups (consecutive
+// threads read consecutive targets: no bank conflicts).  All stores are coalesced 16-byte
+// stores.  The blended modes divide by 1000 * cap through an exact 64-bit reciprocal
+// (floor(n * ceil(2^64 / d) / 2^64) == n / d for n, d < 2^32).  ZNCC (FP64 window sums) stays on
+// the general per-cell path.
 struct CostPairArgs {
   CostArgs view[2];  // per view: a = matching image, b = target image, reverse 0/1
   uint8_t* out[2];
@@ -134,14 +139,19 @@ struct CostPairArgs {
   unsigned long long recip;  // ceil(2^64 / (1000 * cap)) of the blended modes
 };
 
-constexpr int kCostSeg = 64;       // pixels per CTA item
+constexpr int kCostSeg = 64;       // pixels per left-view segment
 constexpr int kCostThreads = 256;  // 4 threads per pixel
 
 template <int DP>
 struct CostLayout {
-  static constexpr int pitch = DP + 16;                   // tile row pitch (bank spread)
-  static constexpr int tile = 0;                          // [kCostSeg][pitch] cost bytes
-  static constexpr int da = tile + kCostSeg * pitch;       // [2][kCostSeg] u64
+  // Ring of left-view cost rows, a power of two >= DP + 127 pixels: a right-view segment needs
+  // the 64 + DP - 1 left pixels from x' + min_disparity on, and becomes complete one segment
+  // after its last one is computed.  The row pitch DP + 4 spreads a warp's diagonal reads over
+  // the 32 banks.
+  static constexpr int ring_px = DP + 127 <= 256 ? 256 : 512;
+  static constexpr int pitch = DP + 4;
+  static constexpr int ring = 0;                           // [ring_px][pitch] cost bytes
+  static constexpr int da = ring + ring_px * pitch;        // [2][kCostSeg] u64
   static constexpr int span = kCostSeg + DP;               // staged targets (>= seg + DP - 1)
   static constexpr int db = da + 2 * kCostSeg * 8;         // [2][span] u64
   static constexpr int aux = db + 2 * span * 8;            // [span] u32 gray / gradient of targets
@@ -149,6 +159,7 @@ struct CostLayout {
   static constexpr int inside = valid + span;              // [kCostSeg] u8
   static constexpr int aaux = inside + kCostSeg;           // [kCostSeg] u32 of the segment pixels
   static constexpr int total = (aaux + kCostSeg * 4 + 15) / 16 * 16;
+  static_assert(da % 8 == 0, "u64 staging alignment");
 };
 
 // Packed central-difference gradient (dx | dy << 16, each as int16) of pixel (x, y).
@@ -164,107 +175,146 @@ template <int DP, int MODE, int WORDS>
 __global__ void __launch_bounds__(kCostThreads) cost_rows_kernel(const CostPairArgs a) {
   extern __shared__ __align__(16) uint8_t csm[];
   using L = CostLayout<DP>;
-  constexpr int G = DP / 16;              // 16-disparity groups per pixel
+  constexpr int G = DP / 16;                    // 16-disparity groups per pixel
   constexpr int TPP = kCostThreads / kCostSeg;  // threads per pixel
-  uint8_t* tile = csm + L::tile;
+  constexpr int RMASK = L::ring_px - 1;
+  uint8_t* ring = csm + L::ring;
   uint64_t* da = (uint64_t*)(csm + L::da);
   uint64_t* db = (uint64_t*)(csm + L::db);
   uint32_t* aux = (uint32_t*)(csm + L::aux);
   uint8_t* valid = csm + L::valid;
   uint8_t* inside = csm + L::inside;
   uint32_t* aaux = (uint32_t*)(csm + L::aaux);
-  const int w = a.view[0].w, h = a.view[0].h, D = a.view[0].D, mind = a.view[0].min_disparity;
-  const int rx = a.view[0].wx / 2, ry = a.view[0].wy / 2;
+  const CostArgs& c = a.view[0];  // left view: matching image left, targets right
+  const int w = c.w, h = c.h, D = c.D, mind = c.min_disparity;
+  const int rx = c.wx / 2, ry = c.wy / 2;
   const int segs = (w + kCostSeg - 1) / kCostSeg;
   const int64_t n = (int64_t)w * h;
-  const int64_t items = 2LL * h * segs;
-  for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-    const int view = (int)(item / ((int64_t)h * segs));
-    const int rest = (int)(item - (int64_t)view * h * segs);
-    const int y = rest / segs, x0 = (rest % segs) * kCostSeg;
-    const CostArgs& c = view ? a.view[1] : a.view[0];
-    uint8_t* out = view ? a.out[1] : a.out[0];
-    // Target pixel of (x0 + i, k): qlo + i + DP - 1 - k (left view), qlo + i + k (right view).
-    const int qlo = view ? x0 + mind : x0 - mind - (DP - 1);
+  for (int y = blockIdx.x; y < h; y += gridDim.x) {
     const bool row_inside = y >= ry && y < h - ry;
     const int64_t row = (int64_t)y * w;
-    __syncthreads();  // the previous item's tile has been written out
-    for (int i = threadIdx.x; i < kCostSeg; i += kCostThreads) {
-      const int x = x0 + i;
-      const bool ok = x < w;
+    int next_r = 0;  // next right-view segment to gather
+    for (int s = 0; s < segs; s++) {
+      const int x0 = s * kCostSeg;
+      // Target of (x0 + i, k): qlo + i + DP - 1 - k.
+      const int qlo = x0 - mind - (DP - 1);
+      __syncthreads();  // the previous segment's staging and gathers are done
+      for (int i = threadIdx.x; i < kCostSeg; i += kCostThreads) {
+        const int x = x0 + i;
+        const bool ok = x < w;
 #pragma unroll
-      for (int j = 0; j < WORDS; j++) da[j * kCostSeg + i] = ok ? c.desc_a[j * n + row + x] : 0;
-      inside[i] = ok && row_inside && x >= rx && x < w - rx && c.tex_a[row + x];
-      if (MODE == CSGM_COST_AD_CENSUS) aaux[i] = ok ? c.gray_a[row + x] : 0;
-      if (MODE == CSGM_COST_CENSUS_GRADIENT) aaux[i] = ok ? gradient_of(c.gray_a, w, h, x, y) : 0;
-    }
-    for (int i = threadIdx.x; i < kCostSeg + DP - 1; i += kCostThreads) {
-      const int q = qlo + i;
-      const bool ok = q >= rx && q < w - rx;
-#pragma unroll
-      for (int j = 0; j < WORDS; j++) db[j * L::span + i] = ok ? c.desc_b[j * n + row + q] : 0;
-      valid[i] = ok && c.tex_b[row + q] ? 0xff : 0;
-      if (MODE == CSGM_COST_AD_CENSUS) aux[i] = ok ? c.gray_b[row + q] : 0;
-      if (MODE == CSGM_COST_CENSUS_GRADIENT) aux[i] = ok ? gradient_of(c.gray_b, w, h, q, y) : 0;
-    }
-    __syncthreads();
-    {
-      const int i = threadIdx.x % kCostSeg;
-      const bool in = inside[i];
-      const uint64_t a0 = da[i], a1 = WORDS > 1 ? da[kCostSeg + i] : 0;
-      const uint32_t av = aaux[i];
-      const int cap = MODE == CSGM_COST_AD_CENSUS ? c.ad_cap : c.grad_cap;
-      const uint32_t wh = (uint32_t)(c.weight * cap), wd = (uint32_t)((1000 - c.weight) * c.bits);
-      const uint32_t half = (uint32_t)(1000 * cap / 2);
-      for (int g = threadIdx.x / kCostSeg; g < G; g += TPP) {
-        uint32_t word[4] = {0x80808080u, 0x80808080u, 0x80808080u, 0x80808080u};
-        if (in) {
-#pragma unroll
-          for (int m = 0; m < 4; m++) {
-            uint32_t v[4];
-#pragma unroll
-            for (int b = 0; b < 4; b++) {
-              const int k = g * 16 + m * 4 + b;
-              const int qi = view ? i + k : i + DP - 1 - k;  // inside the staged span
-              uint32_t ham = __popcll(a0 ^ db[qi]);
-              if (WORDS > 1) ham += __popcll(a1 ^ db[L::span + qi]);
-              uint32_t cost = ham;
-              if (MODE != CSGM_COST_CENSUS) {
-                uint32_t diff;
-                if (MODE == CSGM_COST_AD_CENSUS) {
-                  diff = (uint32_t)abs((int)av - (int)aux[qi]);
-                } else {
-                  const uint32_t d2 = __vabsdiffs2(av, aux[qi]);
-                  diff = (d2 & 0xffffu) + (d2 >> 16);
-                }
-                const uint32_t num = wh * ham + wd * min(diff, (uint32_t)cap) + half;
-                cost = (uint32_t)__umul64hi((unsigned long long)num, a.recip);
-              }
-              // valid[] is 0x00 / 0xff: cost where the target is valid, 0x80 elsewhere.
-              const uint32_t keep = (uint32_t)(int32_t)(int8_t)valid[qi];
-              v[b] = (cost & keep) | (0x80u & ~keep);
-            }
-            word[m] = __byte_perm(__byte_perm(v[0], v[1], 0x0040), __byte_perm(v[2], v[3], 0x0040),
-                                  0x5410);
-          }
-          if (g * 16 + 16 > D) {  // disparities >= D are invalid
-#pragma unroll
-            for (int m = 0; m < 4; m++)
-#pragma unroll
-              for (int b = 0; b < 4; b++)
-                if (g * 16 + m * 4 + b >= D) word[m] = (word[m] & ~(0xffu << (8 * b))) | (0x80u << (8 * b));
-          }
-        }
-        *(uint4*)(tile + i * L::pitch + g * 16) = make_uint4(word[0], word[1], word[2], word[3]);
+        for (int j = 0; j < WORDS; j++) da[j * kCostSeg + i] = ok ? c.desc_a[j * n + row + x] : 0;
+        inside[i] = ok && row_inside && x >= rx && x < w - rx && c.tex_a[row + x];
+        if (MODE == CSGM_COST_AD_CENSUS) aaux[i] = ok ? c.gray_a[row + x] : 0;
+        if (MODE == CSGM_COST_CENSUS_GRADIENT) aaux[i] = ok ? gradient_of(c.gray_a, w, h, x, y) : 0;
       }
-    }
-    __syncthreads();
-    // Coalesced write-out: the segment's pixels are contiguous in the volume.
-    const int npx = min(kCostSeg, w - x0);
-    uint8_t* dst = out + (row + x0) * DP;
-    for (int t = threadIdx.x; t < npx * G; t += kCostThreads) {
-      const int i = t / G, g = t % G;
-      __stcs((uint4*)(dst + (int64_t)i * DP + g * 16), *(const uint4*)(tile + i * L::pitch + g * 16));
+      for (int i = threadIdx.x; i < kCostSeg + DP - 1; i += kCostThreads) {
+        const int q = qlo + i;
+        const bool ok = q >= rx && q < w - rx;
+#pragma unroll
+        for (int j = 0; j < WORDS; j++) db[j * L::span + i] = ok ? c.desc_b[j * n + row + q] : 0;
+        valid[i] = ok && c.tex_b[row + q] ? 0xff : 0;
+        if (MODE == CSGM_COST_AD_CENSUS) aux[i] = ok ? c.gray_b[row + q] : 0;
+        if (MODE == CSGM_COST_CENSUS_GRADIENT) aux[i] = ok ? gradient_of(c.gray_b, w, h, q, y) : 0;
+      }
+      __syncthreads();
+      {
+        const int i = threadIdx.x % kCostSeg;
+        const bool in = inside[i];
+        const uint64_t a0 = da[i], a1 = WORDS > 1 ? da[kCostSeg + i] : 0;
+        const uint32_t av = aaux[i];
+        const int cap = MODE == CSGM_COST_AD_CENSUS ? c.ad_cap : c.grad_cap;
+        const uint32_t wh = (uint32_t)(c.weight * cap), wd = (uint32_t)((1000 - c.weight) * c.bits);
+        const uint32_t half = (uint32_t)(1000 * cap / 2);
+        uint32_t* dst_row = (uint32_t*)(ring + ((x0 + i) & RMASK) * L::pitch);
+        for (int g = threadIdx.x / kCostSeg; g < G; g += TPP) {
+          uint32_t word[4] = {0x80808080u, 0x80808080u, 0x80808080u, 0x80808080u};
+          if (in) {
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+              uint32_t v[4];
+#pragma unroll
+              for (int b = 0; b < 4; b++) {
+                const int k = g * 16 + m * 4 + b;
+                const int qi = i + DP - 1 - k;  // inside the staged span
+                uint32_t ham = __popcll(a0 ^ db[qi]);
+                if (WORDS > 1) ham += __popcll(a1 ^ db[L::span + qi]);
+                uint32_t cost = ham;
+                if (MODE != CSGM_COST_CENSUS) {
+                  uint32_t diff;
+                  if (MODE == CSGM_COST_AD_CENSUS) {
+                    diff = (uint32_t)abs((int)av - (int)aux[qi]);
+                  } else {
+                    const uint32_t d2 = __vabsdiffs2(av, aux[qi]);
+                    diff = (d2 & 0xffffu) + (d2 >> 16);
+                  }
+                  const uint32_t num = wh * ham + wd * min(diff, (uint32_t)cap) + half;
+                  cost = (uint32_t)__umul64hi((unsigned long long)num, a.recip);
+                }
+                // valid[] is 0x00 / 0xff: cost where the target is valid, 0x80 elsewhere.
+                const uint32_t keep = (uint32_t)(int32_t)(int8_t)valid[qi];
+                v[b] = (cost & keep) | (0x80u & ~keep);
+              }
+              word[m] = __byte_perm(__byte_perm(v[0], v[1], 0x0040), __byte_perm(v[2], v[3], 0x0040),
+                                    0x5410);
+            }
+            if (g * 16 + 16 > D) {  // disparities >= D are invalid
+#pragma unroll
+              for (int m = 0; m < 4; m++)
+#pragma unroll
+                for (int b = 0; b < 4; b++)
+                  if (g * 16 + m * 4 + b >= D) word[m] = (word[m] & ~(0xffu << (8 * b))) | (0x80u << (8 * b));
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < 4; m++) dst_row[g * 4 + m] = word[m];
+        }
+      }
+      __syncthreads();
+      // Left view: the segment's rows, coalesced.
+      {
+        const int npx = min(kCostSeg, w - x0);
+        uint8_t* dst = a.out[0] + (row + x0) * DP;
+        for (int t = threadIdx.x; t < npx * G; t += kCostThreads) {
+          const int i = t / G, g = t % G;
+          const uint32_t* src = (const uint32_t*)(ring + ((x0 + i) & RMASK) * L::pitch) + g * 4;
+          __stcs((uint4*)(dst + (int64_t)i * DP + g * 16), make_uint4(src[0], src[1], src[2], src[3]));
+        }
+      }
+      // Right view: every segment whose left pixels are all in the ring (all of them after the
+      // last left segment; left pixels outside the image give 0x80).
+      const int x_end = min(w - 1, x0 + kCostSeg - 1);
+      const bool last = s == segs - 1;
+      for (; next_r < segs &&
+             (last || next_r * kCostSeg + kCostSeg - 1 + mind + DP - 1 <= x_end);
+           next_r++) {
+        const int xr0 = next_r * kCostSeg;
+        const int npx = min(kCostSeg, w - xr0);
+        uint8_t* dst = a.out[1] + (row + xr0) * DP;
+        for (int t = threadIdx.x; t < npx * G; t += kCostThreads) {
+          const int i = t / G, g = t % G;
+          const int xb = xr0 + i + mind + g * 16;  // left pixel of k = 16g; k = 16g + m at xb + m
+          uint32_t b[16];
+          if (xb >= 0 && xb + 15 < w && (xb & RMASK) + 15 <= RMASK) {
+            const uint8_t* src = ring + (xb & RMASK) * L::pitch + g * 16;
+#pragma unroll
+            for (int m = 0; m < 16; m++) b[m] = src[m * (L::pitch + 1)];
+          } else {
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+              const int x = xb + m;
+              b[m] = x >= 0 && x < w ? ring[(x & RMASK) * L::pitch + g * 16 + m] : 0x80u;
+            }
+          }
+          uint32_t word[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            word[q] = __byte_perm(__byte_perm(b[4 * q], b[4 * q + 1], 0x0040),
+                                  __byte_perm(b[4 * q + 2], b[4 * q + 3], 0x0040), 0x5410);
+          __stcs((uint4*)(dst + (int64_t)i * DP + g * 16),
+                 make_uint4(word[0], word[1], word[2], word[3]));
+        }
+      }
     }
   }
 }
@@ -275,9 +325,9 @@ cudaError_t launch_cost_rows_t(const CostPairArgs& a, int sm_count, cudaStream_t
   auto kernel = cost_rows_kernel<DP, MODE, WORDS>;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total);
   if (e != cudaSuccess) return e;
-  const int64_t items = 2LL * a.view[0].h * ((a.view[0].w + kCostSeg - 1) / kCostSeg);
-  const int grid = (int)std::min<int64_t>(items, (int64_t)sm_count * 8);
-  kernel<<<grid, kCostThreads, L::total, stream>>>(a);
+  // One CTA per image row (rows are equal work; the block scheduler balances them).
+  (void)sm_count;
+  kernel<<<a.view[0].h, kCostThreads, L::total, stream>>>(a);
   return cudaGetLastError();
 }
 
