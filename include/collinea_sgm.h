@@ -279,6 +279,39 @@ int csgm_batch_poll(csgm_session* session, int64_t request, int32_t wait, csgm_s
 int csgm_batch_status(csgm_session* session, int32_t* in_flight, int64_t* reserved_bytes,
                       int64_t* resident_bytes);
 
+/* Post-filter settings: the Options fields that computeRecorded reads after the LR check
+ * (src/main/java/sgm/CensusSgm.java:203-272; option checks src/main/java/sgm/Options.java). */
+typedef struct csgm_post {
+  int32_t median;                /* Options.median: odd window side 1..11 (1 = off) */
+  int32_t median_classic;        /* 1 = Options.medianMode "classic", 0 = "edge-preserving" */
+  int32_t median_edge_threshold; /* Options.medianEdgeThreshold, 0..255 (0 = no gray gate) */
+  int32_t correlation_window;    /* Options.correlationWindow, odd 3..15 */
+  int32_t speckle_size;          /* Options.speckleSize, >= 0 (<= 1 = off) */
+  int32_t speckle_connectivity;  /* Options.speckleConnectivity, 4 or 8 */
+  int32_t border;                /* reciprocity radius: Options.census / 2 */
+  int32_t reserved;              /* 0 */
+  double median_max_change;      /* Options.medianMaxChange, >= 0 */
+  double correlation;            /* Options.correlation, -1..1 */
+  double lr_threshold;           /* Options.lrThreshold, > 0 */
+  double speckle_range;          /* Options.speckleRange, >= 0 */
+} csgm_post;
+
+/*
+ * The post-filters of CensusSgm.computeRecorded on the GPU (src/main/java/sgm/CensusSgm.java:
+ * 203-272): the classic (:557-573) or edge-preserving (:576-601) median of the LR-checked map,
+ * the post-median reciprocity check against the right view (:226-239, :604-612), the ZNCC
+ * photometric gate on the gray images (:240-257, :615-644, FP64) and the speckle removal
+ * (:264-271, :647-681).  checked is updated in place; reasons (optional) receives 5 / 6 / 7 where
+ * a pixel is rejected by the reciprocity check / the gate / the speckle removal.  stats (optional):
+ * post_median_lr_rejected, photometric_rejected and valid are added to, speckle_rejected is set.
+ *   left, right : gray images uint8 [h][w] (the matcher's inputs)
+ *   disp_r      : the right view's disparities (csgm_pair's disp_r)
+ * All pointers are HOST pointers; the call returns when the outputs are written.
+ */
+int csgm_postfilter(csgm_session* s, const csgm_post* post, const uint8_t* left,
+                    const uint8_t* right, const float* disp_r, int32_t w, int32_t h,
+                    float* checked, uint8_t* reasons, csgm_stats* stats);
+
 /* Page-locked host memory (cudaMallocHost) for batch inputs and outputs; csgm_host_free releases
  * it.  No counterpart in the reference (its FFM arenas are pageable). */
 int csgm_host_alloc(int64_t bytes, void** ptr);

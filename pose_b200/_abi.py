@@ -72,6 +72,25 @@ class CsgmStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_int64) for name in STATS_FIELDS]
 
 
+class CsgmPost(ctypes.Structure):
+    """csgm_post: the post-filter Options fields (CensusSgm.java:203-272)."""
+
+    _fields_ = [
+        ("median", ctypes.c_int32),
+        ("median_classic", ctypes.c_int32),
+        ("median_edge_threshold", ctypes.c_int32),
+        ("correlation_window", ctypes.c_int32),
+        ("speckle_size", ctypes.c_int32),
+        ("speckle_connectivity", ctypes.c_int32),
+        ("border", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("median_max_change", ctypes.c_double),
+        ("correlation", ctypes.c_double),
+        ("lr_threshold", ctypes.c_double),
+        ("speckle_range", ctypes.c_double),
+    ]
+
+
 class CsgmDeviceInfo(ctypes.Structure):
     _fields_ = [
         ("name", ctypes.c_char * 256),
@@ -160,6 +179,10 @@ SIGNATURES = {
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
          ctypes.POINTER(CsgmStats)],
+    ),
+    "csgm_postfilter": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmPost), _P, _P, _P, _I32, _I32, _P, _P, ctypes.POINTER(CsgmStats)],
     ),
     "csgm_lr_check_noalloc": (
         ctypes.c_int,

@@ -13,7 +13,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import CsgmDeviceInfo, CsgmParams, CsgmProfile, CsgmStats, check
+from ._abi import CsgmDeviceInfo, CsgmParams, CsgmPost, CsgmProfile, CsgmStats, check
 from .stereo_cost import params_from_options
 
 
@@ -214,6 +214,27 @@ class GpuSgm:
                                  _ptr(validLeft), _ptr(validRight), w, h, _ptr(checked), _ptr(dl),
                                  _ptr(dr), _ptr(reasons), _ptr(boundary), ctypes.byref(cstats)))
         return Result(w, h, checked, Stats.from_c(cstats), dl, dr, reasons, boundary)
+
+    def postfilter(self, post: CsgmPost, left, right, disp_r, w: int, h: int, checked,
+                   reasons=None, stats: CsgmStats | None = None):
+        """The post-filters of CensusSgm.computeRecorded (:203-272) on the GPU: median,
+        post-median reciprocity, photometric gate, speckles.  `checked` (float32) and `reasons`
+        (uint8) are numpy arrays updated in place; `stats` (CsgmStats) is updated like the
+        reference's Stats."""
+        n = w * h
+        left, right = _u8(left, n), _u8(right, n)
+        disp_r = np.ascontiguousarray(disp_r, np.float32)
+        if checked.dtype != np.float32 or not checked.flags.c_contiguous or checked.size != n:
+            raise ValueError("checked must be a contiguous float32 array of w*h values")
+        if reasons is not None and (reasons.dtype != np.uint8 or not reasons.flags.c_contiguous
+                                    or reasons.size != n):
+            raise ValueError("reasons must be a contiguous uint8 array of w*h values")
+        if disp_r.size != n:
+            raise ValueError("disp_r must hold w*h values")
+        check(self.lib.csgm_postfilter(self.handle, ctypes.byref(post), _ptr(left), _ptr(right),
+                                       _ptr(disp_r), w, h, _ptr(checked), _ptr(reasons),
+                                       ctypes.byref(stats) if stats is not None else None))
+        return checked
 
 
 class CensusSgm:

@@ -94,6 +94,16 @@ def test_options_validation():
         o.validate()
 
 
+def test_postfilter_rejects_bad_arguments(lib):
+    """csgm_postfilter validates its arguments on the host before touching a device."""
+    post = _abi.CsgmPost(median=3, median_classic=0, median_edge_threshold=24,
+                         correlation_window=7, speckle_size=50, speckle_connectivity=8, border=4,
+                         median_max_change=0.5, correlation=0.55, lr_threshold=0.75,
+                         speckle_range=1.0)
+    assert lib.csgm_postfilter(None, ctypes.byref(post), None, None, None, 64, 64, None, None,
+                               None) == _abi.CSGM_E_INVALID
+
+
 def test_batch_entry_points_reject_bad_arguments(lib):
     """The batch calls validate their arguments on the host before touching a device."""
     request = ctypes.c_int64()
