@@ -237,6 +237,25 @@ class GpuSgm:
         return checked
 
 
+def post_settings(options) -> CsgmPost:
+    """csgm_post from Options: the fields computeRecorded reads after the LR check
+    (CensusSgm.java:203-272); the reciprocity radius is census / 2 as there."""
+    o = options
+    post = CsgmPost()
+    post.median = o.median
+    post.median_classic = 1 if o.medianMode == "classic" else 0
+    post.median_edge_threshold = o.medianEdgeThreshold
+    post.correlation_window = o.correlationWindow
+    post.speckle_size = o.speckleSize
+    post.speckle_connectivity = o.speckleConnectivity
+    post.border = o.census // 2
+    post.median_max_change = o.medianMaxChange
+    post.correlation = o.correlation
+    post.lr_threshold = o.lrThreshold
+    post.speckle_range = o.speckleRange
+    return post
+
+
 class CensusSgm:
     """CensusSgm (CensusSgm.java:10-280) over a GpuSgm session."""
 
@@ -258,6 +277,19 @@ class CensusSgm:
             raise NotImplementedError("color-distance census is not on the GPU path yet")
         return self.session.pair(self.params(), left, right, width, height, validLeft,
                                  validRight, want_views, want_reasons)
+
+    def compute(self, left, right, width: int, height: int, validLeft=None, validRight=None,
+                want_reasons=False) -> Result:
+        """CensusSgm.computeRecorded (CensusSgm.java:56-272): the matcher and the LR check, then
+        the median, post-median reciprocity, photometric gate and speckle removal, with the
+        Stats counters of both stages."""
+        res = self.match_pair(left, right, width, height, validLeft, validRight,
+                              want_views=True, want_reasons=want_reasons)
+        cstats = res.stats.to_c()
+        self.session.postfilter(post_settings(self.options), left, right, res.right, width,
+                                height, res.disparity, res.reasons, cstats)
+        res.stats = Stats.from_c(cstats)
+        return res
 
     def close(self):
         if self._own:
