@@ -279,6 +279,17 @@ int csgm_batch_poll(csgm_session* session, int64_t request, int32_t wait, csgm_s
 int csgm_batch_status(csgm_session* session, int32_t* in_flight, int64_t* reserved_bytes,
                       int64_t* resident_bytes);
 
+/*
+ * CensusSgm.colorCensus on the GPU (src/main/java/sgm/CensusSgm.java:302-332), the descriptor
+ * step of --census-mode color-distance that the reference runs on the CPU before GpuSgm.match:
+ * descriptors [words][w*h] (words = ceil((wx*wy-1)/64)) and the texture mask of an interleaved
+ * BGR image, for csgm_match.  Windows are odd, wx*wy - 1 <= 128 bits.  HOST pointers; returns when
+ * the outputs are written.
+ */
+int csgm_color_census(csgm_session* s, const uint8_t* bgr, int32_t w, int32_t h,
+                      int32_t window_x, int32_t window_y, uint64_t* descriptors,
+                      uint8_t* textured);
+
 /* Post-filter settings: the Options fields that computeRecorded reads after the LR check
  * (src/main/java/sgm/CensusSgm.java:203-272; option checks src/main/java/sgm/Options.java). */
 typedef struct csgm_post {

@@ -215,6 +215,20 @@ class GpuSgm:
                                  _ptr(dr), _ptr(reasons), _ptr(boundary), ctypes.byref(cstats)))
         return Result(w, h, checked, Stats.from_c(cstats), dl, dr, reasons, boundary)
 
+    def color_census(self, bgr, w: int, h: int, window_x: int, window_y: int):
+        """CensusSgm.colorCensus (CensusSgm.java:302-332) on the GPU: (descriptors uint64
+        [words][w*h], textured uint8 [w*h]) of an interleaved BGR image."""
+        n = w * h
+        bgr = np.ascontiguousarray(bgr, np.uint8).reshape(-1)
+        if bgr.size != 3 * n:
+            raise ValueError("bgr must hold 3*w*h bytes")
+        words = (window_x * window_y - 1 + 63) // 64
+        desc = np.empty((words, n), np.uint64)
+        tex = np.empty(n, np.uint8)
+        check(self.lib.csgm_color_census(self.handle, _ptr(bgr), w, h, window_x, window_y,
+                                         _ptr(desc), _ptr(tex)))
+        return desc, tex
+
     def postfilter(self, post: CsgmPost, left, right, disp_r, w: int, h: int, checked,
                    reasons=None, stats: CsgmStats | None = None):
         """The post-filters of CensusSgm.computeRecorded (:203-272) on the GPU: median,

@@ -94,6 +94,11 @@ def test_options_validation():
         o.validate()
 
 
+def test_color_census_rejects_bad_arguments(lib):
+    """csgm_color_census validates its arguments on the host before touching a device."""
+    assert lib.csgm_color_census(None, None, 64, 64, 5, 5, None, None) == _abi.CSGM_E_INVALID
+
+
 def test_postfilter_rejects_bad_arguments(lib):
     """csgm_postfilter validates its arguments on the host before touching a device."""
     post = _abi.CsgmPost(median=3, median_classic=0, median_edge_threshold=24,
