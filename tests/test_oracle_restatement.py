@@ -74,3 +74,58 @@ def test_rectangular_window_and_no_edge_scale(oracle_lib):
     cost_k, S_k, summary_k, disp_k, _ = kr.match(prm, da, db, a, b, ta, tb, w, h, 0)
     assert np.array_equal(ref["aggregate"].astype(np.int64), S_k.reshape(-1))
     assert np.array_equal(ref["disp"].view(np.uint32), disp_k.view(np.uint32))
+
+
+POST_CASES = {
+    "defaults": {},
+    "classic_5": {"median": 5, "medianMode": "classic"},
+    "edge_7_no_gray_gate": {"median": 7, "medianEdgeThreshold": 0, "medianMaxChange": 0.25},
+    "tight_gate_9": {"median": 1, "correlation": 0.9, "correlationWindow": 9},
+    "four_connected": {"speckleConnectivity": 4, "speckleSize": 30, "speckleRange": 0.5},
+}
+
+
+@pytest.mark.parametrize("case", sorted(POST_CASES))
+def test_postfilter_restatement_bit_exact(oracle_lib, case):
+    """The C oracle's post-filters equal the independent Python restatement of
+    CensusSgm.java:203-272 bit for bit (map, reasons, counters)."""
+    import postfilter_restatement as pr
+    from pose_b200.synthetic import PairSpec, make_pair
+    from reference_cpu import post_from_options
+
+    orc = oracle_lib
+    w, h = 72, 54
+    left, right, _ = make_pair(PairSpec(w, h, planes=3, d_min=3, d_max=14, seed=7))
+    o = Options()
+    o.census, o.disparities = 5, 16
+    for k, v in POST_CASES[case].items():
+        setattr(o, k, v)
+    res = orc.pair(params_from_options(o), left, right, w, h, want_reasons=True)
+    post = post_from_options(o)
+
+    want = res["checked"].copy()
+    want_reasons = res["reasons"].copy()
+    stats = res["stats"]
+    base = {k: getattr(stats, k) for k in ("post_median_lr_rejected", "photometric_rejected",
+                                           "valid")}
+    orc.postfilter(post, left, right, res["dr"], w, h, want, stats, want_reasons)
+
+    mine = res["checked"].copy()
+    mine_reasons = res["reasons"].copy()
+    counts = {"postMedianLrRejected": base["post_median_lr_rejected"],
+              "photometricRejected": base["photometric_rejected"], "speckleRejected": 0,
+              "valid": base["valid"]}
+    settings = {"median": o.median, "classic": o.medianMode == "classic",
+                "max_change": o.medianMaxChange, "edge": o.medianEdgeThreshold,
+                "lr": o.lrThreshold, "border": o.census // 2, "window": o.correlationWindow,
+                "correlation": o.correlation, "speckle": o.speckleSize, "range": o.speckleRange,
+                "connectivity": o.speckleConnectivity}
+    pr.postfilter(settings, left, right, res["dr"], w, h, mine, counts, mine_reasons)
+
+    assert np.array_equal(mine.view(np.uint32), want.view(np.uint32)), case
+    assert np.array_equal(mine_reasons, want_reasons), case
+    assert counts["postMedianLrRejected"] == stats.post_median_lr_rejected
+    assert counts["photometricRejected"] == stats.photometric_rejected
+    assert counts["speckleRejected"] == stats.speckle_rejected
+    assert counts["valid"] == stats.valid
+    assert (np.isfinite(res["checked"]) & ~np.isfinite(want)).any(), case
