@@ -1,21 +1,19 @@
-"""Independent restatement of CensusSgm.computeRecorded's post-filters (test infrastructure).
+"""Independent restatement of CensusSgm.computeRecorded's post-filters and of colorCensus
+(test infrastructure).
 
 Follows src/main/java/sgm/CensusSgm.java:203-272 with the helpers medianValid /
 medianEdgePreserving (:557-601), reciprocal (:604-612), zncc (:615-644) and removeSpeckles
-(:647-681), one gray channel.  Written from the Java source in plain Python, apart from the C
-oracle (oracle/sgm_oracle.c): the median sorts with Python's sorted(), the speckles are found by
-a depth-first walk instead of the oracle's queue, and FP64 follows Python floats (IEEE double,
-no fused operations) in the Java evaluation order.  Small images only.
+(:647-681), one gray channel, and colorCensus (:302-332).  Written from the Java source in plain
+Python, apart from the C oracle (oracle/sgm_oracle.c): the median sorts with Python's sorted(),
+the speckles are found by a depth-first walk instead of the oracle's queue, and FP64 follows
+Python floats (IEEE double, no fused operations) in the Java evaluation order.  Small images
+only.
 """
 from __future__ import annotations
 
 import math
 
 import numpy as np
-
-
-def _f32(v) -> float:
-    return float(np.float32(v))
 
 
 def _fsub(a, b) -> float:
@@ -164,3 +162,34 @@ def postfilter(post, left, right, dr, w, h, checked, counts, reasons):
                                                 post["connectivity"])
     counts["valid"] += int(np.isfinite(checked).sum())
     reasons[np.isfinite(before) & ~np.isfinite(checked)] = 7
+
+
+def color_census(bgr, w, h, wx, wy):
+    """CensusSgm.colorCensus (CensusSgm.java:302-332), generalised to wx x wy windows with the
+    same bit order: (descriptors uint64 [words][w*h], textured bool [w*h])."""
+    rx, ry = wx // 2, wy // 2
+    words = (wx * wy - 1 + 63) // 64
+    desc = np.zeros((words, w * h), np.uint64)
+    tex = np.zeros(w * h, bool)
+    img = np.asarray(bgr, np.int64).reshape(h, w, 3)
+    for y in range(ry, h - ry):
+        for x in range(rx, w - rx):
+            distances = []
+            for dy in range(-ry, ry + 1):
+                for dx in range(-rx, rx + 1):
+                    if dx == 0 and dy == 0:
+                        continue
+                    squared = 0.0
+                    for c in range(3):
+                        diff = int(img[y + dy, x + dx, c]) - int(img[y, x, c])
+                        squared += float(diff * diff)
+                    distances.append(math.sqrt(squared))
+            total = 0.0
+            for value in distances:
+                total += value
+            mean = total / (wx * wy)  # the centre's zero distance counts in the mean
+            tex[y * w + x] = max(distances) >= 4
+            for k, value in enumerate(distances):
+                if value >= mean:
+                    desc[k // 64, y * w + x] |= np.uint64(1 << (k % 64))
+    return desc, tex

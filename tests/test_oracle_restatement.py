@@ -129,3 +129,19 @@ def test_postfilter_restatement_bit_exact(oracle_lib, case):
     assert counts["speckleRejected"] == stats.speckle_rejected
     assert counts["valid"] == stats.valid
     assert (np.isfinite(res["checked"]) & ~np.isfinite(want)).any(), case
+
+
+@pytest.mark.parametrize("wx,wy", [(3, 3), (5, 5), (9, 7), (11, 11)])
+def test_color_census_restatement_bit_exact(oracle_lib, wx, wy):
+    """oracle_color_census equals the Python restatement of CensusSgm.colorCensus."""
+    import postfilter_restatement as pr
+
+    rng = np.random.default_rng(wx * 31 + wy)
+    w, h = 37, 29
+    bgr = rng.integers(0, 256, (h, w, 3)).astype(np.uint8)
+    bgr[5:15, 5:20] = (40, 80, 120)  # an untextured patch
+    want_desc, want_tex = oracle_lib.color_census(bgr.reshape(-1), w, h, wx, wy)
+    desc, tex = pr.color_census(bgr.reshape(-1), w, h, wx, wy)
+    assert np.array_equal(np.asarray(want_desc).reshape(-1), desc.reshape(-1))
+    assert np.array_equal(np.asarray(want_tex).astype(bool), tex)
+    assert tex.any() and not tex.all()
