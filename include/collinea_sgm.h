@@ -188,6 +188,15 @@ int csgm_kernel_times(csgm_session* session, csgm_kernel_time* out, int32_t capa
 /* Waits for all work queued on the session's stream. */
 int csgm_session_synchronize(csgm_session* session);
 
+/* Watchdog of the aggregation sweep's device-side waits (a CTA waiting for a bulk copy, for the
+ * previous row block's carry row or for its own row warps): a wait that sees no progress for
+ * `cycles` SM clock cycles gives up, the kernel winds down with no copy left in flight, and the
+ * call returns CSGM_E_TIMEOUT with the wait's site code (1 cost chunk, 3 carry chunk, 5 copy drain,
+ * 6 carry-in or publisher warp) in the message.  The context and the session stay usable.
+ * 0 restores the default, 4e9 cycles (about two seconds).  The reference has no device-side wait
+ * to bound: its OpenCL host blocks in clFinish (src/main/java/sgm/GpuSgm.java:606-609). */
+int csgm_session_set_wait_limit(csgm_session* session, int64_t cycles);
+
 /* ---- the hot path ------------------------------------------------------------------------ */
 
 /*
@@ -338,9 +347,10 @@ void csgm_host_free(void* ptr);
  *   stream : cudaStream_t to queue on (NULL = default stream); the call returns after queueing
  * For callers that cannot let the library allocate device memory: the only scratch is a fixed
  * array in the library's static device memory, sized for h <= 16384 rows (larger heights are
- * rejected with CSGM_E_INVALID).  The first call on a device looks the array up; make that first
- * call before any stream capture.  Calls whose work overlaps in time on one device share the
- * scratch and must be serialised by the caller.
+ * rejected with CSGM_E_INVALID).  The first call on a device looks the array up, and so does the
+ * first call after that device's context has been replaced (cudaDeviceReset); make those calls
+ * before any stream capture.  Calls whose work overlaps in time on one device share the scratch
+ * and must be serialised by the caller.
  */
 int csgm_lr_check_noalloc(const float* disp_l, const float* disp_r, int32_t w, int32_t h,
                           int32_t window_x, int32_t window_y, double lr_threshold,

@@ -165,6 +165,7 @@ SIGNATURES = {
         [_P, ctypes.POINTER(CsgmKernelTime), _I32, ctypes.POINTER(_I32), _I32],
     ),
     "csgm_session_synchronize": (ctypes.c_int, [_P]),
+    "csgm_session_set_wait_limit": (ctypes.c_int, [_P, _I64]),
     "csgm_pair_device": (
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,

@@ -150,6 +150,7 @@ int csgm_batch_submit(csgm_session* s, const csgm_params* p, const uint8_t* left
     return fail(CSGM_E_BUSY, "batch memory held by pairs in flight");
   slot->ws.budget = s->batch_budget - held;
   Context ctx{slot->stream, s->sm_count, &slot->ws, &slot->prof, &slot->profile};
+  ctx.wait_limit = s->wait_limit;
   ctx.sweep_stream = slot->sweep_stream ? slot->sweep_stream : slot->shared_sweep;
   ctx.sweep_ready = slot->sweep_ready;
   ctx.sweep_done = slot->sweep_done;

@@ -295,6 +295,13 @@ int csgm_session_set_budget(csgm_session* s, int64_t bytes) {
   return CSGM_OK;
 }
 
+int csgm_session_set_wait_limit(csgm_session* s, int64_t cycles) {
+  if (!s || cycles < 0) return fail(CSGM_E_INVALID, "invalid session or wait limit");
+  std::lock_guard<std::mutex> guard(s->lock);
+  s->wait_limit = cycles;
+  return CSGM_OK;
+}
+
 int csgm_session_set_profiling(csgm_session* s, int32_t level) {
   if (!s || level < 0 || level > 2) return fail(CSGM_E_INVALID, "invalid session or level");
   std::lock_guard<std::mutex> guard(s->lock);
@@ -386,6 +393,7 @@ int csgm_match(csgm_session* s, const csgm_params* p, const uint64_t* desc_a,
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
+  ctx.wait_limit = s->wait_limit;
   return run_match_host(ctx, *p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                         out_disp, out_summary, reasons, boundary, stats);
 }
@@ -404,6 +412,7 @@ int csgm_pair(csgm_session* s, const csgm_params* p, const uint8_t* left, const 
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
+  ctx.wait_limit = s->wait_limit;
   return run_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                        reasons, boundary, stats);
 }
@@ -423,6 +432,7 @@ int csgm_pair_device(csgm_session* s, const csgm_params* p, const uint8_t* left,
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
+  ctx.wait_limit = s->wait_limit;
   return run_pair_device(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                          reasons, boundary, stats, sync != 0);
 }

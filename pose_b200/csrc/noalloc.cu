@@ -105,10 +105,45 @@ __global__ void __launch_bounds__(kLrThreads) lr_check_rows_kernel(LrNoAllocArgs
 }
 
 std::mutex g_setup_mutex;
-unsigned int* g_scratch_ptr[kMaxDevices];
 
-// Address of the scratch array in the current device's copy of this module.  Looked up once per
-// device, on the first call made with that device current.
+// The scratch address per device, with the id of the context it was looked up in.
+struct ScratchAddress {
+  unsigned long long context = 0;  // cuCtxGetId of that context (0 = not looked up)
+  unsigned int* ptr = nullptr;
+};
+ScratchAddress g_scratch[kMaxDevices];
+
+// Unique id of the calling thread's current context (cuCtxGetCurrent + cuCtxGetId, reached
+// through the runtime's driver entry points, so the library links no driver library).  Ids are
+// never reused in a process, so a context recreated after cudaDeviceReset has a new one.
+// Returns false while no context is current.
+bool current_context_id(unsigned long long* id) {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    get_current = (GetCurrent)a;
+    get_id = (GetId)b;
+  }
+  void* ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return false;
+  return get_id(ctx, id) == 0 && *id != 0;
+}
+
+// Address of the scratch array in the current device's copy of this module.  It is looked up on
+// the first call made with the device current, and again whenever the device's context has been
+// replaced since (after cudaDeviceReset, the old address would point into a context that is
+// gone).  Checking the context costs two driver queries and allocates nothing.
 int scratch_for_current_device(unsigned int** out) {
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -117,13 +152,17 @@ int scratch_for_current_device(unsigned int** out) {
     return fail(CSGM_E_UNSUPPORTED, "csgm_lr_check_noalloc: device ordinal %d >= %d", device,
                 kMaxDevices);
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[device]) {
+  ScratchAddress& slot = g_scratch[device];
+  unsigned long long id = 0;
+  if (!current_context_id(&id) || id != slot.context || !slot.ptr) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_lr_scratch);
+    e = cudaGetSymbolAddress(&p, g_lr_scratch);  // makes the device's primary context current
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(lr scratch)");
-    g_scratch_ptr[device] = (unsigned int*)p;
+    if (!current_context_id(&id)) id = 0;  // no id: looked up again on the next call
+    slot.context = id;
+    slot.ptr = (unsigned int*)p;
   }
-  *out = g_scratch_ptr[device];
+  *out = slot.ptr;
   return CSGM_OK;
 }
 

@@ -80,6 +80,8 @@ struct Context {
   // Optional separate stream for the sweep (ordered after and before ctx.stream by the events).
   cudaStream_t sweep_stream = nullptr;
   cudaEvent_t sweep_ready = nullptr, sweep_done = nullptr;
+  // SM clock cycles a bounded device-side wait may go without progress (0 = the default).
+  long long wait_limit = 0;
 };
 
 // One batch slot: a pair in flight with its own stream and resident workspace.
@@ -142,6 +144,7 @@ struct csgm_session {
   csgm::Workspace workspace;
   csgm::Profiler profiler;
   csgm_profile profile{};
+  int64_t wait_limit = 0;  // csgm_session_set_wait_limit (0 = default)
   // Batched / served pairs (batch.cu).
   std::vector<csgm::BatchSlot> slots;
   size_t batch_budget = 0;

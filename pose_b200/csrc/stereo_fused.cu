@@ -95,26 +95,33 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return d;
 }
 
-// Bounded waits.  `error` short-circuits every later wait unless `shortcut` is false (the final
-// drain, which must see its copies land).  A wait that runs out stores `code` (the wait site:
-// 1 sweep cost chunk, 3 carry chunk, 4 selection tile, 5 drain; the sweep's producer warp
-// stores 6 when it made no progress for the limit).
+// Bounded waits.  `error` short-circuits every later wait unless `shortcut` is false (the drains,
+// which must see their copies land).  A wait that runs out stores `code` (the wait site: 1 sweep
+// cost chunk, 3 carry chunk, 5 drain; the sweep's carry-in and publisher warps store 6 when they
+// made no progress for the limit).  Returns true once the phase has completed, false when the
+// wait gave up (the copy may still be in flight: its slot must not be refilled).
 __device__ __forceinline__ bool mbar_probe(uint64_t* bar, uint32_t parity);
-__device__ __forceinline__ void wait_bar(uint64_t* bar, uint32_t parity, int* error,
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, int* error,
                                          long long limit, int code, bool shortcut = true) {
-  if (mbar_probe(bar, parity)) return;  // the common case: the copy has landed
+  if (mbar_probe(bar, parity)) return true;  // the common case: the copy has landed
   const long long start = clock64();
   for (unsigned spin = 1;; spin++) {
-    if (mbar_test(bar, parity)) return;
+    if (mbar_test(bar, parity)) return true;
     if ((spin & 15) == 0) {  // the error flag and the clock only every 16th probe
-      if (shortcut && *(volatile int*)error) return;
+      if (shortcut && *(volatile int*)error) return false;
       if (clock64() - start > limit) {
         atomicExch(error, code);
-        return;
+        return false;
       }
     }
   }
 }
+
+// Bound of the drains: a bulk copy from this GPU's own memory always completes (nothing it waits
+// for can stall), so its wait is bounded by the copy engine's progress alone and runs out only if
+// the device itself stops; the configurable limit does not shorten it.
+constexpr long long kDrainLimit = 1LL << 32;
+constexpr long long kDefaultWaitLimit = 4000000000LL;  // ~2 s at 2 GHz
 
 // ---------------------------------------------------------------------------------------------
 // Cost volumes of both views (uint8, 0x80 = invalid), StereoCost.value semantics
@@ -1005,6 +1012,9 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
         for (; next_carry < avail; next_carry++) {
           const int ch = next_carry;
           uint64_t* bar = &carry_full[ch % CS];
+          // The slot's previous copy has landed (row warp 0 waited for it before releasing the
+          // slot, unless its wait gave up after an error: then this wait sees the copy land).
+          if (ch >= CS) wait_bar(bar, ((ch - CS) / CS) & 1, err, kDrainLimit, 5, false);
           const uint32_t bytes = (uint32_t)(chunk_n(ch) * L::vslot);
           mbar_expect_tx(bar, bytes);
           bulk_copy(carry_buf + (ch % CS) * K * L::vslot, carry_in + (int64_t)ch * K * L::vslot,
@@ -1022,7 +1032,7 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
     }
     // Every issued carry copy lands before the CTA's shared memory is released.
     for (int ch = max(0, next_carry - CS); ch < next_carry; ch++)
-      wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, limit / 4, 5, false);
+      wait_bar(&carry_full[ch % CS], (ch / CS) & 1, err, kDrainLimit, 5, false);
     return;
   }
   if (w >= R + 2) {
@@ -1126,10 +1136,13 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
     bulk_copy(dst + K * Dp, cost_row1 + (int64_t)first * Dp, cb, bar);
     bulk_copy(dst + 2 * K * Dp, pen_row + c * K, 16u * n, bar);
   };
-  int issued = min(NB, nchunks);
+  int issued = min(NB, nchunks);  // chunks whose copies lane 0 has issued
   if (lane == 0)
     for (int c = 0; c < issued; c++) issue_chunk(c);
   __syncwarp();
+  // Set when one of lane 0's chunk waits gave up (an error anywhere in the sweep): the copy into
+  // that slot may still be in flight, so lane 0 issues no further copies.
+  bool aborted = false;
 
   const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
   const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
@@ -1218,18 +1231,20 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
     auto end_chunk = [&](int c) {
       __syncwarp();
       if (lane == 0) {
-        if (c + NB < nchunks) issue_chunk(c + NB);
+        if (c + NB < nchunks && !aborted) {
+          issue_chunk(c + NB);
+          issued = c + NB + 1;
+        }
         if constexpr (PUBLISH) st_release_cta(published, c + 1);
         if constexpr (CARRY_IN) st_release_cta(carry_consumed, c);
         if constexpr (LW > 0)
           if (w == 0) *(volatile int*)row_done = c + 1;
       }
       __syncwarp();
-      if (c + NB < nchunks) issued = c + NB + 1;
     };
     const int full_chunks = W / K;
     for (int c = 0; c < full_chunks; c++) {
-      wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
+      if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
       if constexpr (CARRY_IN) wait_carry(c);
       const uint32_t slot = slots_a + (c % NB) * L::cslot;
 #pragma unroll
@@ -1242,7 +1257,7 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
     if (full_chunks < nchunks) {
       // Partial last chunk.
       const int c = full_chunks, n = W - c * K;
-      wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1);
+      if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
       if constexpr (CARRY_IN) wait_carry(c);
       const uint32_t slot = slots_a + (c % NB) * L::cslot;
       const int first = (mirror ? (n - 1) * Dp : 0) + lane * REGS;
@@ -1262,9 +1277,11 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
 
   // Idle steps after this row finished (the rows below are still running).
   for (int step = 0; step < R - 1 - w; step++) rows_barrier(R * 32);
-  // After an expired wait, give outstanding chunk copies a bounded chance to land before exit.
+  // Every issued chunk copy lands before the CTA's shared memory is released.  A chunk below
+  // issued - NB has landed: lane 0 refilled its slot only after its wait for it succeeded.
+  issued = __shfl_sync(0xffffffffu, issued, 0);
   for (int cc = max(0, issued - NB); cc < issued; cc++)
-    wait_bar(&my_full[cc % NB], (cc / NB) & 1, err, limit / 4, 5, false);
+    wait_bar(&my_full[cc % NB], (cc / NB) & 1, err, kDrainLimit, 5, false);
 }
 
 template <int REGS>
@@ -1748,7 +1765,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.D = p.disparities;
   a.nb = F.nb;
   a.p1 = p.p1;
-  a.timeout = 4000000000LL;  // ~2 s at 2 GHz
+  a.timeout = ctx.wait_limit > 0 ? ctx.wait_limit : kDefaultWaitLimit;
   a.line = la;
   a.line_slack = line_slack();
   const bool eight = p.directions == 8;

@@ -167,6 +167,11 @@ class GpuSgm:
     def synchronize(self) -> None:
         check(self.lib.csgm_session_synchronize(self.handle))
 
+    def set_wait_limit(self, cycles: int) -> None:
+        """Watchdog of the device-side waits in SM clock cycles (0 = the default, ~2 s); a wait
+        that runs out makes the call fail with CSGM_E_TIMEOUT and leaves the session usable."""
+        check(self.lib.csgm_session_set_wait_limit(self.handle, int(cycles)))
+
     # -- the hot path ------------------------------------------------------------------------
     def match(self, params: CsgmParams, a, b, grayA, grayB, ta, tb, w: int, h: int,
               reverse: bool, stats: Stats | None = None, reasons=None, searchBoundary=None,

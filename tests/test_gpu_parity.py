@@ -233,29 +233,59 @@ def test_pair_band_of_cfg1(session, D):
     assert_pair_equal(session, o, band_l, band_r, w, h, params=bench_params(D=D))
 
 
+@pytest.fixture(scope="module")
+def oracle_threads():
+    """The full-size oracle runs use every host core (a cfg1 pair takes a few seconds)."""
+    import os
+
+    orc.set_threads(os.cpu_count() or 8)
+    yield
+    orc.set_threads(8)
+
+
 @pytest.mark.parametrize("cost", ["census", "census-gradient"])
-def test_full_size_cfg1_fused_equals_general(session, cost):
-    """1600x1067xD128: the fused sweep and the general kernels agree bit for bit at full size,
-    and the LR-checked map recovers the synthetic ground truth."""
+def test_full_size_cfg1_equals_oracle(session, oracle_threads, cost):
+    """The 1600x1067 D128 Census 9x7 benchmark pair, whole, on both GPU paths against the oracle:
+    left and right views, LR-checked map, reasons, boundary flags and counters bit for bit.  The
+    LR-checked map also recovers the synthetic ground truth."""
     from pose_b200.synthetic import make_pair, spec_for
 
     spec = spec_for("cfg1")
     left, right, truth = make_pair(spec)
-    w, h = spec.width, spec.height
-    prm = bench_params(cost=cost)
-    fused = session.pair(prm, left, right, w, h, want_views=True, want_reasons=True)
-    prm.flags = GENERAL
-    general = session.pair(prm, left, right, w, h, want_views=True, want_reasons=True)
-    prm.flags = 0
-    assert np.array_equal(bits(fused.disparity), bits(general.disparity))
-    assert np.array_equal(bits(fused.left), bits(general.left))
-    assert np.array_equal(bits(fused.right), bits(general.right))
-    assert np.array_equal(fused.reasons, general.reasons)
-    assert stats_tuple(fused.stats.to_c()) == stats_tuple(general.stats.to_c())
-    d = fused.disparity
+    o = Options()
+    o.census, o.censusHeight = 9, 7
+    got = assert_pair_equal(session, o, left, right, spec.width, spec.height,
+                            params=bench_params(cost=cost))
+    d = got.disparity
     ok = np.isfinite(d)
     assert ok.mean() > 0.5
     assert (np.abs(d[ok] - truth[ok]) < 1.0).mean() > 0.9
+
+
+@pytest.mark.parametrize("wx,wy,edge_scale", [(9, 9, 32), (9, 7, 32), (9, 9, 0)])
+def test_full_size_cfg0_equals_oracle(session, oracle_threads, wx, wy, edge_scale):
+    """The 640x480 D64 CPU-runnable workload, whole: Census 9x9 with Options p1=3 / p2=36 (the
+    effective P1=10 / P2=120 of 80-bit descriptors, StereoCost.java:17-23), the 9x7 extension
+    with the effective penalties given directly, and constant P2 (sgmEdgeScale 0)."""
+    from pose_b200.synthetic import make_pair, spec_for
+
+    spec = spec_for("cfg0")
+    left, right, truth = make_pair(spec)
+    o = Options()
+    o.census, o.censusHeight, o.disparities = wx, wy, 64
+    o.sgmEdgeScale = edge_scale
+    if wx == wy:
+        o.p1, o.p2 = 3, 36
+        prm = params_from_options(o)
+        assert (prm.p1, prm.p2) == (10, 120)
+    else:
+        prm = params_from_options(o)
+        prm.p1, prm.p2 = 10, 120
+    got = assert_pair_equal(session, o, left, right, spec.width, spec.height, params=prm)
+    d = got.disparity
+    ok = np.isfinite(d)
+    assert ok.mean() > 0.5
+    assert (np.abs(d[ok] - truth[ok]) < 1.0).mean() > 0.85
 
 
 def test_full_size_repeatable(session):
