@@ -362,6 +362,8 @@ def run_ours(args):
         step_host()
     e2e_s = max_over_ranks(time.perf_counter() - e0, dist, f"cuda:{local}")
     e2e_value = replica_throughput(cells, args.steps, world, e2e_s)
+    e2e_match = measure_match_api(args, lib, session, prm, left, right, w, h, cells, world, dist,
+                                  local)
 
     # Roofline of the dominant kernel (largest share of device time in the timed region).
     roofline = None
@@ -402,6 +404,7 @@ def run_ours(args):
                        wall / args.steps * 1e3, 4)},
         "e2e": {"value": round(e2e_value, 3), "unit": "Gcells/s", "h2d_bytes_per_step": 2 * n,
                 "d2h_bytes_per_step": 4 * n + ctypes.sizeof(CsgmStats)},
+        "e2e_match": e2e_match,
         "roofline": roofline,
         "cpu_baseline": baseline,
         "clocks": clock_info,
@@ -415,6 +418,67 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_match_api(args, lib, session, prm, left, right, w, h, cells, world, dist, local):
+    """The matcher through csgm_match, the GpuSgm.match drop-in: per pair the two calls
+    CensusSgm.computeRecorded makes (left view, then the mirrored right view,
+    CensusSgm.java:135-162), every input uploaded from and every output read back to host
+    buffers inside the timed region (wall clock).  Descriptors and masks are computed on the host
+    beforehand, as the Java side does.  Pinned buffers (the steps the headline e2e uses) and
+    pageable numpy buffers (a plain FFM arena); the general kernels (CSGM_FLAG_GENERAL, one view
+    per call) for comparison, on fewer steps."""
+    import numpy as np
+    import torch
+
+    from pose_b200 import census_host
+    from pose_b200._abi import CsgmStats, check
+
+    n = w * h
+    wx, wy = prm.window_x, prm.window_y
+    host = {"da": census_host.census(left, w, h, wx, wy),
+            "db": census_host.census(right, w, h, wx, wy),
+            "ga": left, "gb": right,
+            "ta": census_host.texture(left, w, h, wx, wy),
+            "tb": census_host.texture(right, w, h, wx, wy),
+            "ol": np.empty(n, np.float32), "or": np.empty(n, np.float32)}
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in host.items()}
+    st_l, st_r = CsgmStats(), CsgmStats()
+
+    def pair_of_calls(buf, ptr, flags):
+        prm.flags = flags
+        check(lib.csgm_match(session.handle, ctypes.byref(prm), ptr(buf["da"]), ptr(buf["db"]),
+                             ptr(buf["ga"]), ptr(buf["gb"]), ptr(buf["ta"]), ptr(buf["tb"]), w,
+                             h, 0, ptr(buf["ol"]), None, None, None, ctypes.byref(st_l)))
+        check(lib.csgm_match(session.handle, ctypes.byref(prm), ptr(buf["db"]), ptr(buf["da"]),
+                             ptr(buf["gb"]), ptr(buf["ga"]), ptr(buf["tb"]), ptr(buf["ta"]), w,
+                             h, 1, ptr(buf["or"]), None, None, None, ctypes.byref(st_r)))
+        prm.flags = 0
+
+    def timed(buf, ptr, flags, steps, warmup):
+        for _ in range(warmup):
+            pair_of_calls(buf, ptr, flags)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            pair_of_calls(buf, ptr, flags)
+        s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+        return round(replica_throughput(cells, steps, world, s), 3)
+
+    pin_ptr = lambda t: t.data_ptr()  # noqa: E731
+    np_ptr = lambda a: a.ctypes.data  # noqa: E731
+    value = timed(pinned, pin_ptr, 0, args.steps, max(1, args.warmup))
+    pageable = timed(host, np_ptr, 0, args.steps, 1)
+    general = timed(pinned, pin_ptr, 1, min(3, args.steps), 1)
+    in_bytes = 2 * host["da"].nbytes + 4 * n
+    return {"value": value, "unit": "Gcells/s",
+            "api": "csgm_match x2 per pair (reverse=false, then the mirrored reverse=true call)",
+            "pageable_value": pageable, "general_kernels_value": general,
+            "h2d_bytes_per_step": 2 * in_bytes,
+            # disparities of both views, the first call's counters of both views (2 x 64 B),
+            # the second call's comparison flag
+            "d2h_bytes_per_step": 2 * 4 * n + 2 * 64 + 4}
 
 
 def run_profile_pairs(args):

@@ -394,6 +394,7 @@ int csgm_match(csgm_session* s, const csgm_params* p, const uint64_t* desc_a,
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
   ctx.wait_limit = s->wait_limit;
+  ctx.twin = &s->twin;
   return run_match_host(ctx, *p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                         out_disp, out_summary, reasons, boundary, stats);
 }

@@ -5,6 +5,7 @@
 // A view: cost volume, path aggregation, winner selection.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "pipeline.h"
 #include "stereo_fused.h"
@@ -144,8 +145,9 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* lef
   ctx.prof->kernel_end("census_texture");
   if (use_fused(p)) {
     // Both views in one pass structure (stereo_fused.cu).
-    FusedViews v{desc_l, desc_r, tex_l, tex_r, left, right, disp_l, disp_r, reasons, boundary,
-                 dstats};
+    FusedViews v{desc_l,           desc_r,           tex_l,          tex_r,
+                 left,             right,            disp_l,         disp_r,
+                 {reasons, nullptr}, {boundary, nullptr}, {dstats, nullptr}, {nullptr, nullptr}};
     int* error_flag = nullptr;
     status = run_views_fused(ctx, p, v, w, h, &error_flag);
     if (status) return status;
@@ -297,11 +299,175 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
   return CSGM_OK;
 }
 
-int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
-                   const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
-                   const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
-                   float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
-                   csgm_stats* stats) {
+// Device bytes of csgm_match on the fused kernels (summary: winners records requested).
+static size_t match_fused_bytes(const csgm_params& p, int w, int h, bool summary) {
+  const size_t n = (size_t)w * h, words = (size_t)words_of(p);
+  const size_t inputs = 2 * n * words * 8 + 4 * n;  // one set: descriptors, grays, masks
+  return fused_workspace_bytes(p, w, h) + 2 * inputs +
+         2 * (4 * n + 2 * n + (summary ? 24 * n : 0) + sizeof(DeviceStats)) + 16 * 256;
+}
+
+// Caller's reason codes / boundary flags updated from the device's per-view codes, 0xff = the
+// selection did not decide this pixel (the caller's value stays), as GpuSgm.match copies back
+// only what the selection wrote (GpuSgm.java:289-296).
+static void merge_codes(const std::vector<uint8_t>& codes, uint8_t* dst) {
+  const size_t n = codes.size();
+  const uint8_t* c = codes.data();
+  for (size_t i = 0; i < n; i++) dst[i] = c[i] != 0xff ? c[i] : dst[i];
+}
+
+// csgm_match on the fused kernels.  Both views of the pair are computed; the requested one is
+// returned and the other is held on the device (MatchTwin) for the mirrored call that follows.
+// A call whose inputs, after upload, are byte-identical to the held pair's (and whose parameters
+// and size are equal) returns the held view without computing.
+static int run_match_fused(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                           const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
+                           const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
+                           float* out_disp, int32_t* out_summary, uint8_t* reasons,
+                           uint8_t* boundary, csgm_stats* stats) {
+  int status = CSGM_OK;
+  MatchTwin& twin = *ctx.twin;
+  const size_t n = (size_t)w * h;
+  const size_t desc_bytes = n * words_of(p) * 8;
+  const int view = reverse ? 1 : 0;
+  // Inputs in the pair's order: view 0 matches l against r.
+  const void* host_in[6] = {reverse ? desc_b : desc_a, reverse ? desc_a : desc_b,
+                            reverse ? gray_b : gray_a, reverse ? gray_a : gray_b,
+                            reverse ? tex_b : tex_a,   reverse ? tex_a : tex_b};
+  const size_t in_bytes[6] = {desc_bytes, desc_bytes, n, n, n, n};
+  const int set = twin.valid ? 1 - twin.set : 0;  // keep the held pair's inputs
+  const int base = set ? kMatchIn1 : kMatchIn0;
+  void* in[6];
+  for (int i = 0; i < 6; i++) {
+    in[i] = ctx.ws->get(base + i, in_bytes[i], &status);
+    if (!in[i]) return status;
+  }
+  WS(equal_flag, int, kMatchEqual, sizeof(int));
+  const bool timed = ctx.prof->level >= 1;
+  ctx.prof->begin_call(ctx.stream);
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (timed)
+    for (auto& e : ev) e = ctx.prof->event();
+  if (timed) CK(cudaEventRecord(ev[0], ctx.stream), "event record");
+  for (int i = 0; i < 6; i++)
+    CK(cudaMemcpyAsync(in[i], host_in[i], in_bytes[i], cudaMemcpyHostToDevice, ctx.stream),
+       "input upload");
+  if (timed) CK(cudaEventRecord(ev[1], ctx.stream), "event record");
+  uint8_t* codes_r[2];
+  uint8_t* codes_b[2];
+  float* disp[2];
+  for (int v = 0; v < 2; v++) {
+    WS(d, float, kMatchDisp + v, n * 4);
+    WS(r, uint8_t, kMatchReasons + v, n);
+    WS(b, uint8_t, kMatchBoundary + v, n);
+    disp[v] = d;
+    codes_r[v] = r;
+    codes_b[v] = b;
+  }
+  WS(dstats, DeviceStats, kMatchStats, 2 * sizeof(DeviceStats));
+  int32_t* summary[2] = {nullptr, nullptr};
+  const bool held = twin.valid && twin.view == view && twin.w == w && twin.h == h &&
+                    memcmp(&twin.params, &p, sizeof p) == 0 && (!out_summary || twin.summary);
+  bool served = false;
+  if (held) {
+    // The mirrored call: compare its inputs with the held pair's.
+    const int held_base = twin.set ? kMatchIn1 : kMatchIn0;
+    CK(cudaMemsetAsync(equal_flag, 0, sizeof(int), ctx.stream), "flag clear");
+    for (int i = 0; i < 6; i++) {
+      ctx.prof->kernel_begin();
+      CK(launch_bytes_differ(in[i], ctx.ws->buffers[held_base + i].ptr, in_bytes[i], equal_flag,
+                             ctx.sm_count, ctx.stream),
+         "input comparison");
+      ctx.prof->kernel_end("bytes_differ");
+    }
+    int differ = 1;
+    CK(cudaMemcpyAsync(&differ, equal_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream),
+       "flag readback");
+    CK(cudaStreamSynchronize(ctx.stream), "input comparison");
+    served = differ == 0;
+  }
+  twin.valid = false;
+  DeviceStats host_stats[2] = {};
+  if (served) {
+    host_stats[view] = twin.stats;
+    if (out_summary) {
+      WS(sm, int32_t, kMatchSummary + view, n * 24);
+      summary[view] = sm;
+    }
+  } else {
+    if (out_summary)
+      for (int v = 0; v < 2; v++) {
+        WS(sm, int32_t, kMatchSummary + v, n * 24);
+        summary[v] = sm;
+      }
+    for (int v = 0; v < 2; v++) {
+      CK(cudaMemsetAsync(codes_r[v], 0xff, n, ctx.stream), "reason codes init");
+      CK(cudaMemsetAsync(codes_b[v], 0xff, n, ctx.stream), "boundary codes init");
+    }
+    CK(cudaMemsetAsync(dstats, 0, 2 * sizeof(DeviceStats), ctx.stream), "stats clear");
+    FusedViews fv{(const uint64_t*)in[0], (const uint64_t*)in[1], (const uint8_t*)in[4],
+                  (const uint8_t*)in[5],  (const uint8_t*)in[2],  (const uint8_t*)in[3],
+                  disp[0],                disp[1],                {codes_r[0], codes_r[1]},
+                  {codes_b[0], codes_b[1]}, {dstats, dstats + 1}, {summary[0], summary[1]}};
+    int* error_flag = nullptr;
+    status = run_views_fused(ctx, p, fv, w, h, &error_flag);
+    if (status) return status;
+    CK(cudaMemcpyAsync(&dstats->pad, error_flag, sizeof(int), cudaMemcpyDeviceToDevice,
+                       ctx.stream),
+       "error flag copy");
+    CK(cudaMemcpyAsync(host_stats, dstats, 2 * sizeof(DeviceStats), cudaMemcpyDeviceToHost,
+                       ctx.stream),
+       "stats readback");
+  }
+  if (timed) CK(cudaEventRecord(ev[2], ctx.stream), "event record");
+  CK(cudaMemcpyAsync(out_disp, disp[view], n * 4, cudaMemcpyDeviceToHost, ctx.stream),
+     "readback");
+  if (out_summary)
+    CK(cudaMemcpyAsync(out_summary, summary[view], n * 24, cudaMemcpyDeviceToHost, ctx.stream),
+       "readback");
+  std::vector<uint8_t> rcodes(reasons ? n : 0), bcodes(boundary ? n : 0);
+  if (reasons)
+    CK(cudaMemcpyAsync(rcodes.data(), codes_r[view], n, cudaMemcpyDeviceToHost, ctx.stream),
+       "readback");
+  if (boundary)
+    CK(cudaMemcpyAsync(bcodes.data(), codes_b[view], n, cudaMemcpyDeviceToHost, ctx.stream),
+       "readback");
+  if (timed) CK(cudaEventRecord(ev[3], ctx.stream), "event record");
+  CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (!served && host_stats[0].pad)
+    return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host_stats[0].pad);
+  if (reasons) merge_codes(rcodes, reasons);
+  if (boundary) merge_codes(bcodes, boundary);
+  if (stats) copy_stats(host_stats[view], stats, true);
+  if (!served) {
+    twin.valid = true;
+    twin.set = set;
+    twin.view = 1 - view;
+    twin.params = p;
+    twin.w = w;
+    twin.h = h;
+    twin.summary = out_summary != nullptr;
+    twin.stats = host_stats[1 - view];
+  }
+  if (timed) {
+    ctx.profile->upload_ns += (int64_t)(elapsed_ms(ev[0], ev[1]) * 1e6);
+    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(ev[1], ev[2]) * 1e6);
+    ctx.profile->download_ns += (int64_t)(elapsed_ms(ev[2], ev[3]) * 1e6);
+    ctx.profile->uploaded_bytes += (int64_t)(2 * desc_bytes + 4 * n);
+    ctx.profile->downloaded_bytes += (int64_t)(n * 4 + (out_summary ? 24 * n : 0) +
+                                               (reasons ? n : 0) + (boundary ? n : 0));
+    ctx.profile->calls++;
+  }
+  ctx.prof->collect();
+  return CSGM_OK;
+}
+
+// csgm_match through the general kernels: one view, any D, uint32 aggregates, 16 paths.
+static int run_match_general(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                             const uint64_t* desc_b, const uint8_t* gray_a,
+                             const uint8_t* gray_b, const uint8_t* tex_a, const uint8_t* tex_b,
+                             int w, int h, int reverse, float* out_disp, int32_t* out_summary,
+                             uint8_t* reasons, uint8_t* boundary, csgm_stats* stats) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h, D = (size_t)p.disparities;
   int words = words_of(p);
@@ -361,6 +527,21 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
   if (stats) copy_stats(host, stats, true);
   ctx.prof->collect();
   return CSGM_OK;
+}
+
+int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                   const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,
+                   const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
+                   float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
+                   csgm_stats* stats) {
+  // The fused kernels when they apply and their workspace fits the budget; else the general ones.
+  if (ctx.twin && use_fused(p) && h <= 65535 &&
+      match_fused_bytes(p, w, h, out_summary != nullptr) <= ctx.ws->budget)
+    return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
+                           out_disp, out_summary, reasons, boundary, stats);
+  if (ctx.twin) ctx.twin->valid = false;
+  return run_match_general(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
+                           out_disp, out_summary, reasons, boundary, stats);
 }
 
 }  // namespace csgm

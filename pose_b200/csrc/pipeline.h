@@ -20,7 +20,26 @@ int validate_params(const csgm_params* p, int w, int h);
 enum Slot {
   kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
   kCostL, kCostR, kSum, kSumUp, kSumLines, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
-  kCarry, kFlags, kSlotCount
+  kCarry, kFlags,
+  // csgm_match on the fused kernels: two sets of view inputs (descriptors l/r, grays l/r, masks
+  // l/r in the pair's order), per-view outputs, the comparison flag.
+  kMatchIn0, kMatchIn1 = kMatchIn0 + 6, kMatchDisp = kMatchIn1 + 6, kMatchReasons = kMatchDisp + 2,
+  kMatchBoundary = kMatchReasons + 2, kMatchSummary = kMatchBoundary + 2,
+  kMatchStats = kMatchSummary + 2, kMatchEqual, kSlotCount
+};
+
+// csgm_match runs both views of a pair whenever it runs the fused kernels: the reference always
+// follows the left view's match(a, b, ..., reverse=false) with match(b, a, ..., reverse=true)
+// (CensusSgm.java:135-162), whose result is the pair's other view.  That view's results stay on
+// the device, with the inputs they came from, until a call whose inputs are identical asks for it.
+struct MatchTwin {
+  bool valid = false;
+  int set = 0;   // input set (kMatchIn0 / kMatchIn1) the pair was computed from
+  int view = 0;  // the view held: 0 = reverse false, 1 = reverse true
+  csgm_params params{};
+  int w = 0, h = 0;
+  bool summary = false;  // winners records were computed (reason codes and flags always are)
+  DeviceStats stats{};   // the held view's selection counters
 };
 
 // Device buffers owned by a session, grown on demand inside the memory budget.
@@ -82,6 +101,8 @@ struct Context {
   cudaEvent_t sweep_ready = nullptr, sweep_done = nullptr;
   // SM clock cycles a bounded device-side wait may go without progress (0 = the default).
   long long wait_limit = 0;
+  // The session's held view of csgm_match (null: csgm_match is not the caller).
+  MatchTwin* twin = nullptr;
 };
 
 // One batch slot: a pair in flight with its own stream and resident workspace.
@@ -145,6 +166,7 @@ struct csgm_session {
   csgm::Profiler profiler;
   csgm_profile profile{};
   int64_t wait_limit = 0;  // csgm_session_set_wait_limit (0 = default)
+  csgm::MatchTwin twin;    // csgm_match's held view
   // Batched / served pairs (batch.cu).
   std::vector<csgm::BatchSlot> slots;
   size_t batch_budget = 0;

@@ -1310,9 +1310,12 @@ struct WtaArgs {
   const uint32_t* up;
   const uint32_t* lines;  // anti-diagonal paths (8-path mode), else null
   float* disp[2];
-  uint8_t* reasons;    // left view only
-  uint8_t* boundary;   // left view only
-  DeviceStats* stats;  // left view only
+  // Per view, each optional: reason codes and boundary flags of the pixels decided here (others
+  // keep their value), selection counters (added to), winners records int32 [n][6].
+  uint8_t* reasons[2];
+  uint8_t* boundary[2];
+  DeviceStats* stats[2];
+  int32_t* summary[2];
   int W, H, D, min_disparity, rx, ry, invalid;
   double uniqueness;
 };
@@ -1322,24 +1325,24 @@ __device__ __forceinline__ void select_pixel_record(int best, int value, int sec
                                                     int after, int flags, int D, int min_disparity,
                                                     double uniqueness, float* out,
                                                     uint8_t* reasons, uint8_t* boundary,
-                                                    unsigned (&counts)[6], bool count) {
+                                                    unsigned (&counts)[6]) {
   float result = __int_as_float(0x7fc00000);
   if (best >= 0) {
     const bool full = flags == 3;
     bool done = false;
     if (full) {
-      counts[1] += count;
+      counts[1]++;
       if (boundary) *boundary = 4;
     }
     if (best == 0 || best == D - 1) {
-      counts[2] += count;
+      counts[2]++;
       if (reasons) *reasons = 2;
       if (full && best == 0) {
-        counts[0] += count;
+        counts[0]++;
         if (boundary) *boundary |= 1;
       }
       if (full && best == D - 1) {
-        counts[3] += count;
+        counts[3]++;
         if (boundary) *boundary |= 2;
       }
       done = true;
@@ -1347,7 +1350,7 @@ __device__ __forceinline__ void select_pixel_record(int best, int value, int sec
     if (!done && second != INT_MAX) {
       const double slack = fmax(1.0, __dmul_rn((double)value, uniqueness));
       if ((double)(second - value) <= slack) {
-        counts[4] += count;
+        counts[4]++;
         if (reasons) *reasons = 3;
         done = true;
       }
@@ -1364,7 +1367,7 @@ __device__ __forceinline__ void select_pixel_record(int best, int value, int sec
         }
       }
       result = __double2float_rn(__dadd_rn((double)(min_disparity + best), offset));
-      counts[5] += count;
+      counts[5]++;
       if (reasons) *reasons = 0;
     }
   }
@@ -1478,23 +1481,35 @@ __global__ void __launch_bounds__(kWtaWarps * 32) wta_kernel(const WtaArgs a) {
         const int4 r = rec_a[warp][lane];
         const int rb = rec_b[warp][lane];
         const int after = (int)(int16_t)(rb & 0xffff), flags = rb >> 16;
+        uint8_t* reasons = view ? a.reasons[1] : a.reasons[0];
+        uint8_t* boundary = view ? a.boundary[1] : a.boundary[0];
         select_pixel_record(r.x, r.y, r.z, r.w, after, flags, D, a.min_disparity, a.uniqueness,
-                            (view ? a.disp[1] : a.disp[0]) + p,
-                            view == 0 && a.reasons ? a.reasons + p : nullptr,
-                            view == 0 && a.boundary ? a.boundary + p : nullptr, counts, view == 0);
+                            (view ? a.disp[1] : a.disp[0]) + p, reasons ? reasons + p : nullptr,
+                            boundary ? boundary + p : nullptr, counts);
+        int32_t* summary = view ? a.summary[1] : a.summary[0];
+        if (summary) {
+          // The record of GpuStereo.java:758-769: no winner -> value INT_MAX.
+          int2* rec = (int2*)(summary + 6 * p);
+          rec[0] = make_int2(r.x, r.x >= 0 ? r.y : INT_MAX);
+          rec[1] = make_int2(r.z, r.w);
+          rec[2] = make_int2(after, flags);
+        }
       }
     }
     __syncwarp();
   }
   cp_async_wait<0>();
-  if (a.stats) {
-    unsigned long long* dst[6] = {&a.stats->lower_boundary_rejected,
-                                  &a.stats->full_interval_pixels, &a.stats->boundary_rejected,
-                                  &a.stats->upper_boundary_rejected,
-                                  &a.stats->ambiguity_rejected, &a.stats->selected};
+  // Lane l selected view l & 1 throughout: the counters of each view are the sums over its lanes.
+#pragma unroll
+  for (int view = 0; view < 2; view++) {
+    DeviceStats* st = a.stats[view];
+    if (!st) continue;
+    unsigned long long* dst[6] = {&st->lower_boundary_rejected, &st->full_interval_pixels,
+                                  &st->boundary_rejected, &st->upper_boundary_rejected,
+                                  &st->ambiguity_rejected, &st->selected};
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-      const unsigned total = __reduce_add_sync(0xffffffffu, counts[i]);
+      const unsigned total = __reduce_add_sync(0xffffffffu, (lane & 1) == view ? counts[i] : 0u);
       if (lane == 0 && total) atomicAdd(dst[i], (unsigned long long)total);
     }
   }
@@ -1812,9 +1827,12 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   t.lines = sum_lines;
   t.disp[0] = v.disp_l;
   t.disp[1] = v.disp_r;
-  t.reasons = v.reasons;
-  t.boundary = v.boundary;
-  t.stats = v.stats;
+  for (int view = 0; view < 2; view++) {
+    t.reasons[view] = v.reasons[view];
+    t.boundary[view] = v.boundary[view];
+    t.stats[view] = v.stats[view];
+    t.summary[view] = v.summary[view];
+  }
   t.W = w;
   t.H = h;
   t.D = p.disparities;

@@ -17,9 +17,11 @@ struct FusedViews {
   const uint8_t* gray_r;
   float* disp_l;
   float* disp_r;
-  uint8_t* reasons;   // left view only
-  uint8_t* boundary;  // left view only
-  DeviceStats* stats; // left view only
+  // Per view (0 left, 1 right), each optional.
+  uint8_t* reasons[2];   // reason codes of the pixels decided by the selection
+  uint8_t* boundary[2];  // searchBoundary flags of full-interval pixels
+  DeviceStats* stats[2]; // selection counters, added to
+  int32_t* summary[2];   // winners records [n][6]
 };
 
 bool fused_supported(const csgm_params& p);

@@ -358,6 +358,32 @@ cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, 
   return cudaGetLastError();
 }
 
+// 16-byte words where both buffers allow them (workspace buffers are 256-byte aligned), bytes for
+// the tail; one flag store per thread that found a difference.
+__global__ void bytes_differ_kernel(const uint8_t* a, const uint8_t* b, size_t bytes, int* differ) {
+  const size_t words = bytes / 16;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  bool diff = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) {
+    const uint4 x = __ldcs((const uint4*)a + i), y = __ldcs((const uint4*)b + i);
+    diff |= (x.x != y.x) | (x.y != y.y) | (x.z != y.z) | (x.w != y.w);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < bytes % 16) {
+    const size_t i = words * 16 + threadIdx.x;
+    diff |= a[i] != b[i];
+  }
+  if (diff) *differ = 1;
+}
+
+cudaError_t launch_bytes_differ(const void* a, const void* b, size_t bytes, int* differ,
+                                int sm_count, cudaStream_t stream) {
+  if (bytes == 0) return cudaSuccess;
+  if (((uintptr_t)a | (uintptr_t)b) % 16) return cudaErrorMisalignedAddress;
+  bytes_differ_kernel<<<grid_for((int64_t)(bytes / 16) + 1, 256, sm_count * 4), 256, 0, stream>>>(
+      (const uint8_t*)a, (const uint8_t*)b, bytes, differ);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_lr_check(const LrArgs& a, int sm_count, cudaStream_t stream) {
   int64_t n = (int64_t)a.w * a.h;
   lr_check_kernel<<<grid_for(n, 256, sm_count * 8), 256, 0, stream>>>(a);

@@ -111,5 +111,9 @@ cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int s
 cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, int sm_count,
                            cudaStream_t stream);
 cudaError_t launch_lr_check(const LrArgs& a, int sm_count, cudaStream_t stream);
+// Sets *differ to 1 when the device buffers a and b (bytes long) are not identical; *differ is
+// cleared by the caller and is never cleared here.
+cudaError_t launch_bytes_differ(const void* a, const void* b, size_t bytes, int* differ,
+                                int sm_count, cudaStream_t stream);
 
 }  // namespace csgm

@@ -81,19 +81,22 @@ def test_match_scaling_fixture(session, cost, directions, agg, reverse):
                      reasons=reasons_want, boundary=boundary_want)
     from pose_b200.sgm import Stats
 
-    st = Stats()
-    reasons = np.ones(n, np.uint8)
-    boundary = np.zeros(n, np.uint8)
-    disp, summary = session.match(prm, da, db, a, b, ta, tb, w, h, reverse, st, reasons,
-                                  boundary, summary=True)
-    assert np.array_equal(summary, want["summary"]), "winners record"
-    assert np.array_equal(bits(disp), bits(want["disp"]))
-    assert np.array_equal(reasons, reasons_want) and np.array_equal(boundary, boundary_want)
-    s = want["stats"]
-    assert (st.fullIntervalPixels, st.boundaryRejected, st.lowerBoundaryRejected,
-            st.upperBoundaryRejected, st.ambiguityRejected, st.selected) == (
-        s.full_interval_pixels, s.boundary_rejected, s.lower_boundary_rejected,
-        s.upper_boundary_rejected, s.ambiguity_rejected, s.selected)
+    for flags in (0, GENERAL):  # the fused kernels where they apply, and the general ones
+        prm.flags = flags
+        st = Stats()
+        reasons = np.ones(n, np.uint8)
+        boundary = np.zeros(n, np.uint8)
+        disp, summary = session.match(prm, da, db, a, b, ta, tb, w, h, reverse, st, reasons,
+                                      boundary, summary=True)
+        assert np.array_equal(summary, want["summary"]), "winners record"
+        assert np.array_equal(bits(disp), bits(want["disp"]))
+        assert np.array_equal(reasons, reasons_want) and np.array_equal(boundary, boundary_want)
+        s = want["stats"]
+        assert (st.fullIntervalPixels, st.boundaryRejected, st.lowerBoundaryRejected,
+                st.upperBoundaryRejected, st.ambiguityRejected, st.selected) == (
+            s.full_interval_pixels, s.boundary_rejected, s.lower_boundary_rejected,
+            s.upper_boundary_rejected, s.ambiguity_rejected, s.selected)
+    prm.flags = 0
 
 
 @pytest.mark.parametrize("census", [5, 11])
