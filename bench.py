@@ -33,6 +33,12 @@ WORKLOADS = {
     "cfg1": dict(spec="cfg1", census=(9, 7), D=128, cost="census", p1=10, p2=120),
     "cfg1-gradient": dict(spec="cfg1", census=(9, 7), D=128, cost="census-gradient", p1=10,
                           p2=120),
+    # 3000x2000, window 7x7, D256, 16 paths, uint32 forced, the reference's default penalties
+    # (effective 8 / 48 at 48 bits); AD-Census lambda_AD 10 = --ad-truncation 10, weight 0.5.
+    "cfg2-ad-census": dict(spec="cfg2", census=(7, 7), D=256, cost="ad-census", p1=None,
+                           p2=None, directions=16, aggregate="32", ad_truncation=10),
+    "cfg2-zncc": dict(spec="cfg2", census=(7, 7), D=256, cost="zncc", p1=None, p2=None,
+                      directions=16, aggregate="32"),
 }
 
 
@@ -64,9 +70,13 @@ def workload_params(name: str):
     wl = WORKLOADS[name]
     o = Options()
     o.census, o.censusHeight = wl["census"]
-    o.disparities, o.matchingCost, o.directions = wl["D"], wl["cost"], 8
+    o.disparities, o.matchingCost = wl["D"], wl["cost"]
+    o.directions = wl.get("directions", 8)
+    o.sgmAggregate = wl.get("aggregate", "auto")
+    o.adTruncation = wl.get("ad_truncation", o.adTruncation)
     prm = params_from_options(o)
-    prm.p1, prm.p2 = wl["p1"], wl["p2"]  # the workload's effective penalties
+    if wl["p1"] is not None:
+        prm.p1, prm.p2 = wl["p1"], wl["p2"]  # the workload's effective penalties
     return prm
 
 
@@ -230,6 +240,13 @@ def cpu_baseline(prm, left, right, w, h, rows: int, threads: int):
     return w * rows * prm.disparities / dt / 1e9, dt
 
 
+def default_cpu_rows(prm, h: int) -> int:
+    """Rows of the CPU sample: an eighth of the image at 8 paths and D <= 128, fewer for the
+    16-path D256 workload, so that one sample stays within seconds to tens of seconds."""
+    scale = max(1, prm.directions // 8) * max(1, prm.disparities // 128)
+    return max(prm.window_y + 2, h // (8 * scale * scale))
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -241,7 +258,7 @@ def run_reference(args):
     left, right, _ = make_pair(spec)
     w, h = spec.width, spec.height
     threads = os.cpu_count() or 1
-    rows = args.cpu_rows or max(prm.window_y + 2, h // 8)
+    rows = args.cpu_rows or default_cpu_rows(prm, h)
     values = []
     for i in range(args.warmup + args.steps):
         v, _ = cpu_baseline(prm, left, right, w, h, rows, threads)
@@ -254,7 +271,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": cells / (value * 1e9) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "cfg1 " + workload_desc(args.workload, prm),
+        "config": {"workload": args.workload + " " + workload_desc(args.workload, prm),
                    "sample": f"{w}x{rows} full-width band of the pair"},
         "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
                          "sample": f"{w}x{rows} band, census+both views+LR, {threads} threads"},
@@ -386,7 +403,7 @@ def run_ours(args):
 
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rows = args.cpu_rows or max(prm.window_y + 2, h // 8)
+        rows = args.cpu_rows or default_cpu_rows(prm, h)
         v, dt = cpu_baseline(prm, left, right, w, h, rows, 1)
         baseline = {"value": v, "unit": "Gcells/s", "cores": 1, "kind": "port",
                     "sample": f"{w}x{rows} full-width band of the pair, both views + LR "
@@ -395,7 +412,8 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Gcells/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16" if prm.aggregate_bytes == 2 else "u32",
         "data": "synthetic",
         "config": {"workload": args.workload + " " + workload_desc(args.workload, prm),
                    "pairs_per_step_per_gpu": 1,

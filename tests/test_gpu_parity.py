@@ -301,3 +301,45 @@ def test_full_size_repeatable(session):
     r2 = session.pair(prm, left, right, spec.width, spec.height)
     assert np.array_equal(bits(r1.disparity), bits(r2.disparity))
     assert r1.stats == r2.stats
+
+
+@pytest.mark.parametrize("cost", ["census", "ad-census", "zncc"])
+@pytest.mark.parametrize("agg", ["16", "32"])
+def test_pair_16_paths_fixture(session, cost, agg):
+    """The 16-path extension (the eight (+-1,+-2), (+-2,+-1) directions after the reference's
+    eight) on UpgradeStereoRegression's masked fixture, uint16 and uint32 aggregates."""
+    w, h, shift, a, b, ma, mb = upgrade_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 41, -3
+    o.matchingCost, o.directions, o.sgmAggregate = cost, 16, agg
+    prm = params_from_options(o)
+    assert prm.aggregate_bytes == (2 if agg == "16" else 4)
+    assert_pair_equal(session, o, a, b, w, h, ma, mb, params=prm)
+
+
+def cfg2_params(cost):
+    """The 3000x2000 workload: window 7x7, D256, 16 paths, uint32 forced; AD-Census lambda_AD 10
+    as --ad-truncation 10 with census weight 0.5; ZNCC 7x7 (cost scale 0..48); the reference's
+    default penalties (p1 4, p2 24 in 5x5 units: effective 8 / 48 at 48 bits)."""
+    o = Options()
+    o.census = 7
+    o.disparities, o.directions, o.sgmAggregate = 256, 16, "32"
+    o.matchingCost, o.adTruncation, o.censusWeight = cost, 10, 0.5
+    prm = params_from_options(o)
+    assert prm.aggregate_bytes == 4 and (prm.p1, prm.p2) == (8, 48)
+    return o, prm
+
+
+@pytest.mark.parametrize("cost", ["ad-census", "zncc"])
+def test_pair_band_of_cfg2(session, oracle_threads, cost):
+    """A full-width 3000 x 32 band of the 3000x2000 pair (10 planes, saturated specular patches)
+    against the oracle: 16 paths, uint32 aggregate, D256."""
+    from pose_b200.synthetic import make_pair, spec_for
+
+    spec = spec_for("cfg2")
+    left, right, _ = make_pair(spec)
+    w, h, y0 = spec.width, 32, 900
+    band_l = np.ascontiguousarray(left.reshape(spec.height, w)[y0:y0 + h]).reshape(-1)
+    band_r = np.ascontiguousarray(right.reshape(spec.height, w)[y0:y0 + h]).reshape(-1)
+    o, prm = cfg2_params(cost)
+    assert_pair_equal(session, o, band_l, band_r, w, h, params=prm)
