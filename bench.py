@@ -159,7 +159,9 @@ def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int, lines_in_swee
     for the leftover-lines launch.  `lines_in_sweep`: the sweep's CTAs also walk the anti-diagonal
     lines (the session profile then names a `lines_rest` launch)."""
     cells = w * h * prm.disparities
-    sb = prm.aggregate_bytes
+    # The fused kernels keep partial aggregates as uint16 pairs (exact within the proved bound,
+    # also for a forced uint32 aggregate); the general kernels use the aggregate's own width.
+    sb = 2
     lines = 4 + 3 * 2 * sb
     table = {
         "cost_pair": 2,                   # both views' uint8 cost volumes, written once
@@ -171,9 +173,12 @@ def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int, lines_in_swee
         # written and read back, the lines partial written (both views)
         "lines": lines,
         "lines_rest": None,
+        # 16 paths: four knight-move line families, each walked forward and back; a pass reads
+        # both views' costs and read-modify-writes the lines partial
+        "knights": 4 * 2 * (2 + 2 * 2 * sb),
         "cost_volume": 1,                 # general path: one view's uint8 cost volume
-        "paths_line": 1 + 2 * sb,         # general path: cost read + aggregate read-modify-write
-        "winners": 1 + sb,                # general path: cost validity + aggregate read
+        "paths_line": 1 + 2 * prm.aggregate_bytes,  # general: cost read + aggregate RMW
+        "winners": 1 + prm.aggregate_bytes,          # general: cost validity + aggregate read
     }
     if table.get(kernel) is None:
         return None

@@ -20,7 +20,7 @@ int validate_params(const csgm_params* p, int w, int h);
 enum Slot {
   kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
   kCostL, kCostR, kSum, kSumUp, kSumLines, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
-  kCarry, kFlags,
+  kCarry, kFlags, kPixelInfo,
   // csgm_match on the fused kernels: two sets of view inputs (descriptors l/r, grays l/r, masks
   // l/r in the pair's order), per-view outputs, the comparison flag.
   kMatchIn0, kMatchIn1 = kMatchIn0 + 6, kMatchDisp = kMatchIn1 + 6, kMatchReasons = kMatchDisp + 2,

@@ -417,7 +417,8 @@ __global__ void cost_pair_kernel(CostPairArgs a) {
 struct PenaltyArgs {
   const uint8_t* gray[2];
   const uint8_t* tex[2];
-  uint4* out;  // [2 streams][H][W]
+  uint4* out;      // [2 streams][H][W]
+  uint32_t* info;  // optional [H][W] pixel records of the 16-path line walks (KnightArgs::info)
   int W, H, p1, p2, edge_scale;
 };
 
@@ -445,6 +446,11 @@ __global__ void penalty_kernel(const PenaltyArgs a) {
     if (a.tex[v][(int64_t)y * W + x]) word[0] |= 0x8000u << (16 * v);
   }
   a.out[((int64_t)s * H + yp) * W + xs] = make_uint4(word[0], word[1], word[2], word[3]);
+  if (a.info && s == 0) {
+    const int64_t p = (int64_t)y * W + x;
+    a.info[p] = (uint32_t)a.gray[0][p] | (uint32_t)a.gray[1][p] << 8 |
+                (a.tex[0][p] ? 1u : 0u) << 16 | (a.tex[1][p] ? 1u : 0u) << 24;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -714,8 +720,14 @@ __device__ __forceinline__ void normalise(const PathState<REGS>& s, uint32_t kee
   for (int j = 0; j < REGS; j++) d[j] = (s.v[j] - s.m) & keep;
 }
 
+// Cost of the pad disparities D..Dp-1 in both halves.  A pad lane's path cost is at least 1536,
+// a real one at most 512 + P2 <= 1023, so a pad lane is never a row minimum and never the
+// strict minimum of a real lane's candidates (its normalised state exceeds P2 + 1); and with 16
+// paths a pad total stays below 16 x (1536 + 511) < 2^16, above the invalid threshold 16 x 512.
+constexpr uint32_t kPadCost = 0x06000600u;
+
 // This lane's costs of both views as packed u16 pairs: byte j of each view widened, 0x80 -> 512,
-// and pad[j] ORed in (disparities >= D are lifted to 0x1200 so they never win a minimum).
+// and pad[j] ORed in (disparities >= D are lifted to kPadCost so they never win a minimum).
 template <int REGS>
 __device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint32_t (&pad)[REGS],
                                             uint32_t (&c)[REGS]) {
@@ -804,7 +816,7 @@ __device__ __forceinline__ void walk_line(const LineArgs& a, int line, uint32_t 
   const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
   uint32_t pad[REGS];
 #pragma unroll
-  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? kPadCost : 0u;
   const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
   uint32_t* part = a.part + lane * REGS;
   const int64_t step = (int64_t)W - 1;  // pixel-index step along the line (down-left)
@@ -934,6 +946,154 @@ __global__ void __launch_bounds__(kLineWarps * 32) lines_kernel(const LineArgs a
     if (idx >= lines) return;
     walk_line<REGS>(a, line_of(idx, a.W, a.H), ring, lane);
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The 16-path extension's eight paths (+-1,+-2), (+-2,+-1) (direction table entries 8..15): four
+// families of independent lines, family (dx, dy) with dy > 0 covering the paths (dx, dy) and
+// (-dx, -dy).  A line starts at a pixel whose predecessor (x - dx, y - dy) is outside the image
+// and visits start + i * (dx, dy).  One warp walks a line forward (path (dx, dy)) and back (path
+// (-dx, -dy)), both views packed as in the sweep, and each pass adds its path costs to the lines
+// partial aggregate: the families run one after another after the anti-diagonal lines, so every
+// read-modify-write of a pixel's partial is ordered.  Per pixel the warp's ring brings both views'
+// costs, the pixel's record (both grays and texture flags) and the partial, kPrefetch pixels
+// ahead; pathP2 - P1 (StereoCost.java:44-48) comes from a per-CTA table over |gray difference|.
+struct KnightArgs {
+  const uint8_t* cost[2];  // [H][W][Dp] per view
+  const uint32_t* info;    // [H][W] gray_l | gray_r << 8 | textured_l << 16 | textured_r << 24
+  uint32_t* part;          // [H][W][Dp] lines partial, accumulated
+  int W, H, D, p1, p2, edge_scale, dx, dy;
+};
+
+template <int REGS>
+struct KnightSlot {
+  static constexpr int Dp = 32 * REGS;
+  static constexpr int cost = 0, info = 2 * Dp, part = 2 * Dp + 16;
+  static constexpr int bytes = 2 * Dp + 16 + 4 * Dp;
+};
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+
+template <int REGS>
+__global__ void __launch_bounds__(kLineWarps * 32) knight_kernel(const KnightArgs a) {
+  constexpr int Dp = 32 * REGS, CH = Dp / 16;
+  using S = KnightSlot<REGS>;
+  extern __shared__ __align__(16) uint8_t ksm[];
+  __shared__ uint32_t step_p2[256];  // pathP2 - P1 for a gray difference d
+  for (int d = threadIdx.x; d < 256; d += blockDim.x)
+    step_p2[d] = (uint32_t)(path_p2(a.p1, a.p2, a.edge_scale, d, 0) - a.p1);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int W = a.W, H = a.H, dx = a.dx, dy = a.dy;
+  const int64_t line = (int64_t)blockIdx.x * kLineWarps + warp;
+  if (line >= line_count(W, H, dx, dy)) return;
+  int x0, y0;
+  line_start(line, W, H, dx, dy, x0, y0);
+  const int len = min((H - 1 - y0) / dy + 1, dx > 0 ? (W - 1 - x0) / dx + 1 : x0 / (-dx) + 1);
+  const int64_t p0 = (int64_t)y0 * W + x0, step = (int64_t)dy * W + dx;
+  const uint32_t ring = smem_u32(ksm) + warp * kPrefetch * S::bytes;
+  const uint32_t lo_edge = lane == 0 ? 0xffffffffu : 0u;
+  const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
+  uint32_t pad[REGS];
+#pragma unroll
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? kPadCost : 0u;
+  const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
+  uint32_t* part = a.part + lane * REGS;
+
+  // Copies of pixel i into ring slot `slot`, one commit group (empty off the line).
+  auto fetch = [&](int slot, int i) {
+    if (i >= 0 && i < len) {
+      const int64_t p = p0 + i * step;
+      const uint32_t sl = ring + slot * S::bytes;
+      if (lane < 2 * CH) {
+        const int view = lane / CH, chunk = lane % CH;
+        cp_async16(sl + S::cost + view * Dp + chunk * 16,
+                   (view ? a.cost[1] : a.cost[0]) + p * Dp + chunk * 16);
+      }
+      if (lane == 31) cp_async4(sl + S::info, a.info + p);
+#pragma unroll
+      for (int c = lane; c < Dp / 4; c += 32) cp_async16(sl + S::part + c * 16, a.part + p * Dp + c * 4);
+    }
+    cp_async_commit();
+  };
+  // One pass: forward (back = false, pixel i after i - 1) or back (pixel i after i + 1).
+  auto pass = [&](bool back) {
+    PathState<REGS> cur;
+    zero_state(cur);
+    uint32_t prev_info = 0;
+    auto at = [&](int k) { return back ? len - 1 - k : k; };
+#pragma unroll
+    for (int k = 0; k < kPrefetch; k++) fetch(k, at(k));
+    for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+      for (int k = 0; k < kPrefetch; k++) {
+        if (base + k < len) {
+          const int i = at(base + k);
+          cp_async_wait<kPrefetch - 1>();
+          __syncwarp();
+          const uint32_t sl = ring + k * S::bytes;
+          uint32_t c[REGS], old[REGS];
+          widen_costs<REGS>(sl + S::cost + lane * REGS, sl + S::cost + Dp + lane * REGS, pad, c);
+          const uint32_t info = lds_u32(sl + S::info);
+          lds_words<REGS>(sl + S::part + lane * REGS * 4, old);
+          __syncwarp();  // every lane has read the slot before it is refilled
+          fetch(k, at(base + k + kPrefetch));
+          // The matching view's grays: left view in bits 0-7, right view in bits 8-15.  The first
+          // pixel has a zero state, so its penalty is never used.
+          const int dl = abs((int)(info & 0xffu) - (int)(prev_info & 0xffu));
+          const int dr = abs((int)((info >> 8) & 0xffu) - (int)((prev_info >> 8) & 0xffu));
+          const uint32_t q[1] = {cur.m + (step_p2[dl] | (step_p2[dr] << 16))};
+          PathState<REGS> prev[1] = {cur}, out[1];
+          paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+          uint32_t sum[REGS];
+#pragma unroll
+          for (int j = 0; j < REGS; j++) sum[j] = old[j] + out[0].v[j];
+          if (back)
+            store_words_cs<REGS>(part + (p0 + i * step) * Dp, sum);
+          else
+            store_words<REGS>(part + (p0 + i * step) * Dp, sum);
+          cur = out[0];
+          // Successors of an untextured pixel start afresh (CensusSgm.java:432-433).
+          const uint32_t keep = ((info >> 16) & 1u ? 0xffffu : 0u) | ((info >> 24) & 1u ? 0xffff0000u : 0u);
+          if (keep != 0xffffffffu) {
+#pragma unroll
+            for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+            cur.m &= keep;
+          }
+          prev_info = info;
+        }
+      }
+    }
+    cp_async_wait<0>();
+  };
+  pass(false);
+  // The return pass copies the forward pass's sums back from L2 (cp.async), some of them stored
+  // by other lanes just now: every lane's stores reach L2 before any lane copies.
+  __threadfence();
+  __syncwarp();
+  pass(true);
+}
+
+template <int REGS>
+cudaError_t launch_knights(KnightArgs a, cudaStream_t stream) {
+  const int shared = kLineWarps * kPrefetch * KnightSlot<REGS>::bytes;
+  cudaError_t e = cudaFuncSetAttribute(knight_kernel<REGS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, shared);
+  if (e != cudaSuccess) return e;
+  // The four families one after another: (1,2), (2,1), (-1,2), (-2,1).
+  const int family[4][2] = {{1, 2}, {2, 1}, {-1, 2}, {-2, 1}};
+  for (const auto& f : family) {
+    a.dx = f[0];
+    a.dy = f[1];
+    const int64_t lines = line_count(a.W, a.H, a.dx, a.dy);
+    knight_kernel<REGS><<<(int)((lines + kLineWarps - 1) / kLineWarps), kLineWarps * 32, shared,
+                           stream>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // One CTA = R row warps + a carry-in warp + a publisher warp (+ LW line warps), one row block of
@@ -1148,7 +1308,7 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
   const uint32_t hi_edge = lane == 31 ? 0xffffffffu : 0u;
   uint32_t pad[REGS];
 #pragma unroll
-  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? 0x10001000u : 0u;
+  for (int j = 0; j < REGS; j++) pad[j] = lane * REGS + j >= a.D ? kPadCost : 0u;
   const uint32_t p1x2 = (uint32_t)a.p1 * 0x10001u;
   PathState<REGS> horiz;  // (1,0) in stream coordinates
   zero_state(horiz);
@@ -1637,33 +1797,39 @@ cudaError_t launch_sweep_for(const SweepArgs& a, cudaStream_t stream, bool exclu
 }
 
 struct FusedLayout {
-  size_t cost, sum, pen, carry, flags, total;
+  size_t cost, sum, pen, info, carry, flags, total;
   int Dp, nb, vslot, rows;
   FusedLayout(const csgm_params& p, int w, int h) {
     Dp = padded_d(p.disparities);
     rows = rows_for(Dp / 32);
     nb = (h + rows - 1) / rows;
-    const int nv = p.directions == 8 ? 2 : 1;
+    const int nv = p.directions >= 8 ? 2 : 1;
     vslot = nv * Dp * 4;
     size_t n = (size_t)w * h;
     cost = n * Dp;
     sum = n * Dp * 4;
     pen = 2 * n * 16;
+    info = p.directions == 16 ? n * 4 : 0;
     carry = (size_t)2 * nb * w * vslot;
     flags = ((size_t)2 * nb + 8) * sizeof(int);
-    total = 2 * cost + (p.directions == 8 ? 3 : 2) * sum + pen + carry + flags + 7 * 256;
+    total = 2 * cost + (p.directions >= 8 ? 3 : 2) * sum + pen + info + carry + flags + 8 * 256;
   }
 };
 
 }  // namespace
 
 bool fused_supported(const csgm_params& p) {
-  if (p.disparities > 256 || p.aggregate_bytes != 2) return false;
-  if (p.directions != 4 && p.directions != 8) return false;
+  if (p.disparities > 256) return false;
+  if (p.directions != 4 && p.directions != 8 && p.directions != 16) return false;
   // Valid path costs stay below 512 (cost <= bits, penalty <= P2), which is what lets the
   // selection tell invalid cells by their totals.
   const int bits = p.window_x * p.window_y - 1;
   if (bits > 127 || p.p2 + bits >= 512) return false;
+  // The partial aggregates are packed uint16 pairs.  They hold every sum exactly when the proved
+  // bound directions x (512 + P2) fits 16 bits (StereoCost.aggregateBound, StereoCost.java:31-41),
+  // which P2 + bits < 512 guarantees for up to 16 paths; a uint32 aggregate then holds the same
+  // values, so aggregate_bytes 4 gives bit-identical results on these kernels.
+  if ((int64_t)p.directions * (512 + p.p2) > 65535) return false;
   return true;
 }
 
@@ -1685,9 +1851,14 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   uint32_t* sum_up = (uint32_t*)ctx.ws->get(kSumUp, F.sum, &status);
   if (!sum_up) return status;
   uint32_t* sum_lines = nullptr;
-  if (p.directions == 8) {
+  if (p.directions >= 8) {
     sum_lines = (uint32_t*)ctx.ws->get(kSumLines, F.sum, &status);
     if (!sum_lines) return status;
+  }
+  uint32_t* info = nullptr;
+  if (p.directions == 16) {
+    info = (uint32_t*)ctx.ws->get(kPixelInfo, F.info, &status);
+    if (!info) return status;
   }
   uint4* pen = (uint4*)ctx.ws->get(kPen, F.pen, &status);
   if (!pen) return status;
@@ -1731,7 +1902,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     ctx.prof->kernel_end("cost_pair");
   }
   {
-    PenaltyArgs pa{{v.gray_l, v.gray_r}, {v.tex_l, v.tex_r}, pen, w, h, p.p1, p.p2,
+    PenaltyArgs pa{{v.gray_l, v.gray_r}, {v.tex_l, v.tex_r}, pen, info, w, h, p.p1, p.p2,
                    p.edge_scale};
     ctx.prof->kernel_begin();
     penalty_kernel<<<dim3((w + 127) / 128, h, 2), 128, 0, ctx.stream>>>(pa);
@@ -1754,12 +1925,32 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
       default: return launch_lines<8>(la, stream);
     }
   };
+  // 16 paths: the knight-move line families add to the lines partial once the anti-diagonal
+  // lines have written it.
+  KnightArgs ka{{cost_l, cost_r}, info, sum_lines, w, h, p.disparities, p.p1, p.p2, p.edge_scale,
+                0, 0};
+  auto run_knights = [&](cudaStream_t stream) -> int {
+    if (!info) return CSGM_OK;
+    ctx.prof->kernel_begin();
+    cudaError_t ke;
+    switch (regs) {
+      case 2: ke = launch_knights<2>(ka, stream); break;
+      case 4: ke = launch_knights<4>(ka, stream); break;
+      case 6: ke = launch_knights<6>(ka, stream); break;
+      default: ke = launch_knights<8>(ka, stream); break;
+    }
+    if (ke != cudaSuccess) return cuda_fail(ke, "knight line kernel launch");
+    ctx.prof->kernel_end("knights");
+    return CSGM_OK;
+  };
   if (sum_lines && !line_warps) {
     cudaError_t le;
     ctx.prof->kernel_begin();
     le = run_lines(ctx.stream);
     if (le != cudaSuccess) return cuda_fail(le, "line kernel launch");
     ctx.prof->kernel_end("lines");
+    status = run_knights(ctx.stream);
+    if (status) return status;
   }
   cudaError_t e = cudaMemsetAsync(flags, 0, F.flags, ctx.stream);
   if (e != cudaSuccess) return cuda_fail(e, "flag clear");
@@ -1783,7 +1974,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.timeout = ctx.wait_limit > 0 ? ctx.wait_limit : kDefaultWaitLimit;
   a.line = la;
   a.line_slack = line_slack();
-  const bool eight = p.directions == 8;
+  const bool eight = p.directions >= 8;  // 16 paths: the 8-path sweep plus the knight lines
   // Batched pairs launch the sweep on a high-priority stream: its pending CTAs then take SMs ahead
   // of other pairs' bandwidth-bound kernels, so a pair's chain of row blocks is not held up.
   cudaStream_t sweep_stream = ctx.stream;
@@ -1814,6 +2005,8 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     e = run_lines(sweep_stream);
     if (e != cudaSuccess) return cuda_fail(e, "line kernel launch");
     ctx.prof->kernel_end("lines_rest");
+    status = run_knights(sweep_stream);
+    if (status) return status;
   }
   if (ctx.sweep_stream) {
     e = cudaEventRecord(ctx.sweep_done, ctx.sweep_stream);
