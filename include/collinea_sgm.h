@@ -155,10 +155,32 @@ void csgm_session_close(csgm_session* session);
  * (src/main/java/sgm/GpuSgm.java:629-633). */
 int csgm_session_set_budget(csgm_session* session, int64_t bytes);
 
-/* Device bytes csgm_pair needs for a w x h pair; CSGM_E_NOMEM if it exceeds the session budget.
- * Replaces the resident branch of GpuStereo.plan (src/main/java/sgm/GpuStereo.java:33-54). */
+/* How the views run: Options.gpuSgm (src/main/java/sgm/Options.java:32,780).  AUTO keeps the
+ * whole cost volume and aggregate in device memory when they fit the budget and streams otherwise;
+ * RESIDENT fails with CSGM_E_NOMEM when they do not fit; STREAMED always streams.  Streamed views
+ * run on the general kernels through strips of rows (GpuStereo.java:339-437): a down pass over
+ * the strips from the top aggregates the directions with dy >= 0, carrying path states across
+ * strip edges and parking the strip's partial aggregate in pinned host memory, and an up pass from
+ * the bottom adds the directions with dy < 0 to it and selects the strip's disparities.  Results
+ * are bit-identical to the resident views. */
+#define CSGM_SGM_AUTO 0
+#define CSGM_SGM_RESIDENT 1
+#define CSGM_SGM_STREAMED 2
+
+/* mode: CSGM_SGM_*; strip_rows: the largest strip height (Options.gpuStripRows, 0 = 64), halved
+ * until a strip fits the budget (GpuStereo.plan, src/main/java/sgm/GpuStereo.java:59-62). */
+int csgm_session_set_streaming(csgm_session* session, int32_t mode, int32_t strip_rows);
+
+/* Device bytes csgm_pair needs for a w x h pair under the session's budget and streaming mode;
+ * CSGM_E_NOMEM if no plan fits.  Replaces GpuStereo.plan (src/main/java/sgm/GpuStereo.java:33-84). */
 int csgm_plan(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
               int64_t* device_bytes);
+
+/* The same plan in detail, the reference's Plan record (GpuStereo.java:33-84): strip_rows = h for
+ * a resident plan, else the strip height; host_bytes = the pinned host memory a streamed plan
+ * parks its partial aggregate in (0 when resident).  Any output may be NULL. */
+int csgm_plan_detail(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
+                     int32_t* strip_rows, int64_t* device_bytes, int64_t* host_bytes);
 
 /* Largest disparity count whose plan fits the budget (0 if none):
  * GpuSgm.disparityLimit / GpuStereo.limit (src/main/java/sgm/GpuSgm.java:237-245,

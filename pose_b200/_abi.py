@@ -21,6 +21,12 @@ CSGM_E_TIMEOUT = -5
 CSGM_E_BUSY = -6
 CSGM_E_UNSUPPORTED = -7
 
+# csgm_session_set_streaming modes (Options.gpuSgm)
+CSGM_SGM_AUTO = 0
+CSGM_SGM_RESIDENT = 1
+CSGM_SGM_STREAMED = 2
+SGM_MODES = {"auto": CSGM_SGM_AUTO, "resident": CSGM_SGM_RESIDENT, "streamed": CSGM_SGM_STREAMED}
+
 STATUS_NAMES = {
     CSGM_E_INVALID: "CSGM_E_INVALID",
     CSGM_E_CUDA: "CSGM_E_CUDA",
@@ -153,6 +159,12 @@ SIGNATURES = {
     "csgm_session_open": (ctypes.c_int, [_I32, ctypes.POINTER(_P)]),
     "csgm_session_close": (None, [_P]),
     "csgm_session_set_budget": (ctypes.c_int, [_P, _I64]),
+    "csgm_session_set_streaming": (ctypes.c_int, [_P, _I32, _I32]),
+    "csgm_plan_detail": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I64),
+         ctypes.POINTER(_I64)],
+    ),
     "csgm_plan": (ctypes.c_int, [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(_I64)]),
     "csgm_disparity_limit": (
         ctypes.c_int,

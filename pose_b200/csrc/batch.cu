@@ -151,6 +151,8 @@ int csgm_batch_submit(csgm_session* s, const csgm_params* p, const uint8_t* left
   slot->ws.budget = s->batch_budget - held;
   Context ctx{slot->stream, s->sm_count, &slot->ws, &slot->prof, &slot->profile};
   ctx.wait_limit = s->wait_limit;
+  // Batch slots keep their pairs resident (admission counts whole volumes).
+  ctx.sgm_mode = CSGM_SGM_RESIDENT;
   ctx.sweep_stream = slot->sweep_stream ? slot->sweep_stream : slot->shared_sweep;
   ctx.sweep_ready = slot->sweep_ready;
   ctx.sweep_done = slot->sweep_done;

@@ -283,6 +283,7 @@ void csgm_session_close(csgm_session* s) {
   cudaStreamSynchronize(s->stream);
   release_batch_slots(s);
   s->workspace.release_all();
+  s->host_partial.release();
   cudaStreamDestroy(s->stream);
   delete s;  // destroys the profiler's events on the current device
 }
@@ -299,6 +300,15 @@ int csgm_session_set_wait_limit(csgm_session* s, int64_t cycles) {
   if (!s || cycles < 0) return fail(CSGM_E_INVALID, "invalid session or wait limit");
   std::lock_guard<std::mutex> guard(s->lock);
   s->wait_limit = cycles;
+  return CSGM_OK;
+}
+
+int csgm_session_set_streaming(csgm_session* s, int32_t mode, int32_t strip_rows) {
+  if (!s || mode < CSGM_SGM_AUTO || mode > CSGM_SGM_STREAMED || strip_rows < 0)
+    return fail(CSGM_E_INVALID, "invalid session, streaming mode or strip height");
+  std::lock_guard<std::mutex> guard(s->lock);
+  s->sgm_mode = mode;
+  s->strip_rows = strip_rows ? strip_rows : 64;  // Options.gpuStripRows default
   return CSGM_OK;
 }
 
@@ -346,29 +356,48 @@ int csgm_kernel_times(csgm_session* s, csgm_kernel_time* out, int32_t capacity, 
   return CSGM_OK;
 }
 
-int csgm_plan(csgm_session* s, const csgm_params* p, int32_t w, int32_t h, int64_t* bytes) {
-  if (!s || !bytes) return fail(CSGM_E_INVALID, "NULL argument");
+// A context with the session's budget and streaming settings, for planning only.
+static Context planning_context(csgm_session* s) {
+  Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
+  return ctx;
+}
+
+int csgm_plan_detail(csgm_session* s, const csgm_params* p, int32_t w, int32_t h,
+                     int32_t* strip_rows, int64_t* device_bytes, int64_t* host_bytes) {
+  if (!s) return fail(CSGM_E_INVALID, "NULL session");
   int rc = validate_params(p, w, h);
   if (rc) return rc;
-  *bytes = (int64_t)pair_workspace_bytes(*p, w, h, true);
-  if ((size_t)*bytes > s->workspace.budget)
-    return fail(CSGM_E_NOMEM,
-                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
-                *bytes / 1048576.0, s->workspace.budget / 1048576.0);
+  std::lock_guard<std::mutex> guard(s->lock);
+  ViewPlan plan;
+  rc = plan_pair(planning_context(s), *p, w, h, true, &plan);
+  if (rc) return rc;
+  if (strip_rows) *strip_rows = plan.rows;
+  if (device_bytes) *device_bytes = (int64_t)plan.device_bytes;
+  if (host_bytes) *host_bytes = (int64_t)plan.host_bytes;
   return CSGM_OK;
+}
+
+int csgm_plan(csgm_session* s, const csgm_params* p, int32_t w, int32_t h, int64_t* bytes) {
+  if (!s || !bytes) return fail(CSGM_E_INVALID, "NULL argument");
+  return csgm_plan_detail(s, p, w, h, nullptr, bytes, nullptr);
 }
 
 int csgm_disparity_limit(csgm_session* s, const csgm_params* p, int32_t w, int32_t h,
                          int32_t* limit) {
   // GpuStereo.limit (GpuStereo.java:86-94): binary search over the plan.
   if (!s || !p || !limit) return fail(CSGM_E_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> guard(s->lock);
+  const Context ctx = planning_context(s);
   int low = 2, high = 4096;
   while (low < high) {
     int mid = (low + high + 1) / 2;
     csgm_params q = *p;
     q.disparities = mid;
-    bool fits = validate_params(&q, w, h) == CSGM_OK &&
-                pair_workspace_bytes(q, w, h, true) <= s->workspace.budget;
+    ViewPlan plan;
+    bool fits = validate_params(&q, w, h) == CSGM_OK && plan_pair(ctx, q, w, h, true, &plan) == 0;
     if (fits)
       low = mid;
     else
@@ -394,6 +423,9 @@ int csgm_match(csgm_session* s, const csgm_params* p, const uint64_t* desc_a,
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
   ctx.wait_limit = s->wait_limit;
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
   ctx.twin = &s->twin;
   return run_match_host(ctx, *p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                         out_disp, out_summary, reasons, boundary, stats);
@@ -414,6 +446,9 @@ int csgm_pair(csgm_session* s, const csgm_params* p, const uint8_t* left, const 
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
   ctx.wait_limit = s->wait_limit;
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
   return run_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                        reasons, boundary, stats);
 }
@@ -434,6 +469,9 @@ int csgm_pair_device(csgm_session* s, const csgm_params* p, const uint8_t* left,
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
   ctx.wait_limit = s->wait_limit;
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
   return run_pair_device(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                          reasons, boundary, stats, sync != 0);
 }

@@ -3,6 +3,7 @@
 // A pair (CensusSgm.computeRecorded :56-201): census + texture of both images, the left view
 // (CensusSgm.match with reverse=false), the right view (reverse=true), the left-right check.
 // A view: cost volume, path aggregation, winner selection.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -29,19 +30,100 @@ static bool use_fused(const csgm_params& p) {
   return !(p.flags & CSGM_FLAG_GENERAL) && fused_supported(p);
 }
 
-size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
-  size_t n = (size_t)w * h, D = (size_t)p.disparities, words = (size_t)words_of(p);
+// Device bytes of a pair besides its cost volumes and aggregates: descriptors, masks, the views'
+// disparities, counters and (host_inputs) the upload / download buffers.
+static size_t pair_fixed_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
+  size_t n = (size_t)w * h, words = (size_t)words_of(p);
   size_t bytes = 0;
   bytes += 2 * n * words * 8;  // descriptors
   bytes += 2 * n;              // texture masks
   bytes += 2 * n * 4;          // raw view disparities
   bytes += sizeof(DeviceStats);
+  if (host_inputs) bytes += 4 * n + n * 4 + 2 * n;  // images, masks, checked, reasons, boundary
+  return bytes;
+}
+
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
+  size_t n = (size_t)w * h, D = (size_t)p.disparities;
+  size_t bytes = pair_fixed_bytes(p, w, h, host_inputs);
   if (use_fused(p))
     bytes += fused_workspace_bytes(p, w, h);
   else
     bytes += n * D * 2 + n * D * p.aggregate_bytes;  // one cost volume + one aggregate
-  if (host_inputs) bytes += 4 * n + n * 4 + 2 * n;  // images, masks, checked, reasons, boundary
   return bytes;
+}
+
+// Device bytes of one streamed strip of `rows` rows: its cost volume and partial aggregate, and
+// the path-state carries (two buffers of |dy| rows per direction that crosses strip edges).
+static size_t strip_bytes(const csgm_params& p, int w, int rows) {
+  const size_t D = (size_t)p.disparities, cells = (size_t)w * rows * D;
+  size_t carry = 0;
+  for (int d = 0; d < p.directions; d++) {
+    int dx, dy;
+    direction(d, dx, dy);
+    carry += 2 * (size_t)(dy < 0 ? -dy : dy) * w * D * 4;
+  }
+  return cells * (2 + p.aggregate_bytes) + carry + 4 * 256;
+}
+
+// GpuStereo.plan (GpuStereo.java:33-84): resident when the whole volume fits the budget (unless
+// streaming is forced), else strips whose height starts at the session's strip height and halves
+// until one fits.  Strips are at least two rows high with 16 paths, so that a (+-1,+-2) path's
+// predecessor always lies in the previous strip.
+static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
+                       size_t resident, ViewPlan* plan) {
+  const size_t budget = ctx.ws->budget;
+  if (ctx.sgm_mode != CSGM_SGM_STREAMED && resident <= budget) {
+    plan->streamed = false;
+    plan->rows = h;
+    plan->device_bytes = resident;
+    plan->host_bytes = 0;
+    return CSGM_OK;
+  }
+  if (ctx.sgm_mode == CSGM_SGM_RESIDENT || !ctx.host_partial)
+    return fail(CSGM_E_NOMEM,
+                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
+                resident / 1048576.0, budget / 1048576.0);
+  const int min_rows = p.directions == 16 ? 2 : 1;
+  for (int rows = std::min(h, std::max(ctx.strip_rows, min_rows)); rows >= min_rows; rows /= 2) {
+    const size_t bytes = fixed + strip_bytes(p, w, rows);
+    if (bytes <= budget) {
+      plan->streamed = true;
+      plan->rows = rows;
+      plan->device_bytes = bytes;
+      plan->host_bytes = (size_t)w * h * p.disparities * p.aggregate_bytes;
+      return CSGM_OK;
+    }
+  }
+  return fail(CSGM_E_NOMEM,
+              "GPU SGM search exceeds the device budget even in strips of %d rows: needs %.1f "
+              "MiB, budget %.1f MiB",
+              min_rows, (fixed + strip_bytes(p, w, min_rows)) / 1048576.0, budget / 1048576.0);
+}
+
+int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
+              ViewPlan* plan) {
+  return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs),
+                     pair_workspace_bytes(p, w, h, host_inputs), plan);
+}
+
+void* HostBuffer::get(size_t want, int* status) {
+  if (bytes >= want && ptr) return ptr;
+  release();
+  cudaError_t e = cudaMallocHost(&ptr, want);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    *status = cuda_fail(e, "pinned host buffer of the streamed aggregate");
+    return nullptr;
+  }
+  bytes = want;
+  return ptr;
+}
+
+void HostBuffer::release() {
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  bytes = 0;
 }
 
 // One view through the general kernels: cost volume, every path, selection.
@@ -78,6 +160,94 @@ static int run_view_general(Context& ctx, const csgm_params& p, const uint64_t* 
   return CSGM_OK;
 }
 
+// One view through strips of `rows` rows (GpuStereo.java:339-437, in two passes instead of one
+// per direction).  The down pass visits the strips from the top and aggregates every direction
+// with dy >= 0, each strip's lines starting from the path states its predecessor strip left in
+// the carries; the strip's partial aggregate goes to pinned host memory.  The up pass visits the
+// strips from the bottom, brings the partial back, adds the directions with dy < 0 and selects the
+// strip's disparities.  Cost volumes are recomputed per pass.  A pixel's aggregate is the same
+// sum of the same path costs as in the resident view (modular uint16 / exact int32 addition does
+// not depend on the order), so the results are identical.
+static int run_view_streamed(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
+                             const uint64_t* desc_b, const uint8_t* tex_a, const uint8_t* tex_b,
+                             const uint8_t* gray_a, const uint8_t* gray_b, int w, int h,
+                             int reverse, float* out, int32_t* summary, uint8_t* reasons,
+                             uint8_t* boundary, DeviceStats* dstats, int rows) {
+  int status = CSGM_OK;
+  const size_t D = (size_t)p.disparities, Sb = (size_t)p.aggregate_bytes;
+  const size_t strip_cells = (size_t)w * rows * D, row_cells = (size_t)w * D;
+  WS(cost, uint16_t, kCostL, strip_cells * 2);
+  WS(sum, uint8_t, kSum, strip_cells * Sb);
+  size_t carry_offset[kMaxDirections] = {}, carry_words = 0;
+  for (int d = 0; d < p.directions; d++) {
+    int dx, dy;
+    direction(d, dx, dy);
+    carry_offset[d] = carry_words;
+    carry_words += 2 * (size_t)(dy < 0 ? -dy : dy) * row_cells;
+  }
+  WS(carry, int32_t, kStripCarry, carry_words * 4);
+  uint8_t* host = (uint8_t*)ctx.host_partial->get((size_t)w * h * D * Sb, &status);
+  if (!host) return status;
+  const int strips = (h + rows - 1) / rows;
+  for (int pass = 0; pass < 2; pass++) {
+    for (int ord = 0; ord < strips; ord++) {
+      const int strip = pass == 0 ? ord : strips - 1 - ord;
+      const int y0 = strip * rows, actual = std::min(rows, h - y0);
+      const size_t cells = (size_t)w * actual * D;
+      CostArgs c{desc_a, desc_b, tex_a, tex_b, gray_a, gray_b, cost, w, h, p.disparities,
+                 p.min_disparity, reverse, p.window_x, p.window_y, words_of(p), p.cost_mode,
+                 p.census_weight_milli, p.ad_truncation, p.gradient_truncation,
+                 p.window_x * p.window_y - 1};
+      c.y0 = y0;
+      c.rows = actual;
+      ctx.prof->kernel_begin();
+      CK(launch_cost_volume(c, ctx.sm_count, ctx.stream), "cost kernel launch");
+      ctx.prof->kernel_end("cost_volume");
+      if (pass == 0)
+        CK(cudaMemsetAsync(sum, 0, cells * Sb, ctx.stream), "aggregate clear");
+      else
+        CK(cudaMemcpyAsync(sum, host + (size_t)y0 * row_cells * Sb, cells * Sb,
+                           cudaMemcpyHostToDevice, ctx.stream),
+           "partial aggregate upload");
+      for (int d = 0; d < p.directions; d++) {
+        int dx, dy;
+        direction(d, dx, dy);
+        if ((pass == 0) != (dy >= 0)) continue;
+        PathArgs a{cost, tex_a, gray_a, w, h, p.disparities, dx, dy, p.p1, p.p2, p.edge_scale};
+        a.y0 = y0;
+        a.rows = actual;
+        if (dy != 0) {
+          // Two carry buffers per direction, alternating: strip `ord` reads the one its
+          // predecessor in path order wrote and writes the other.
+          const size_t half = (size_t)(dy < 0 ? -dy : dy) * row_cells;
+          int32_t* base = carry + carry_offset[d];
+          a.carry_in = ord > 0 ? base + ((ord + 1) % 2) * half : nullptr;
+          a.carry_out = base + (ord % 2) * half;
+        }
+        ctx.prof->kernel_begin();
+        CK(launch_paths_line(a, sum, p.aggregate_bytes, ctx.sm_count, ctx.stream),
+           "paths kernel launch");
+        ctx.prof->kernel_end("paths_line");
+      }
+      if (pass == 0) {
+        CK(cudaMemcpyAsync(host + (size_t)y0 * row_cells * Sb, sum, cells * Sb,
+                           cudaMemcpyDeviceToHost, ctx.stream),
+           "partial aggregate download");
+      } else {
+        SelectArgs sa{cost, out, summary, reasons, boundary, dstats, w, h, p.disparities,
+                      p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+        sa.y0 = y0;
+        sa.rows = actual;
+        ctx.prof->kernel_begin();
+        CK(launch_winners(sa, sum, p.aggregate_bytes, ctx.sm_count, ctx.stream),
+           "winners kernel launch");
+        ctx.prof->kernel_end("winners");
+      }
+    }
+  }
+  return CSGM_OK;
+}
+
 void copy_stats(const DeviceStats& d, csgm_stats* out, bool add) {
   if (!add) memset(out, 0, sizeof *out);
   out->lower_boundary_rejected += (int64_t)d.lower_boundary_rejected;
@@ -100,11 +270,11 @@ static float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
 
 // The device part of a pair.  `own_call` = this is the whole call (csgm_pair_device), so it owns
 // the call-level timing; csgm_pair times its own copies around it.
-static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* left,
-                          const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
-                          int w, int h, float* lr_checked, float* disp_l, float* disp_r,
-                          uint8_t* reasons, uint8_t* boundary, csgm_stats* stats, bool sync,
-                          bool own_call) {
+static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& plan,
+                          const uint8_t* left, const uint8_t* right, const uint8_t* valid_l,
+                          const uint8_t* valid_r, int w, int h, float* lr_checked, float* disp_l,
+                          float* disp_r, uint8_t* reasons, uint8_t* boundary, csgm_stats* stats,
+                          bool sync, bool own_call) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
   int words = words_of(p);
@@ -143,7 +313,15 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const uint8_t* lef
   ctx.prof->kernel_begin();
   CK(launch_census_texture(ca, 2, ctx.stream), "census kernel launch");
   ctx.prof->kernel_end("census_texture");
-  if (use_fused(p)) {
+  if (plan.streamed) {
+    // Both views through strips (general kernels); the right view's counters are discarded.
+    status = run_view_streamed(ctx, p, desc_l, desc_r, tex_l, tex_r, left, right, w, h, 0, disp_l,
+                               nullptr, reasons, boundary, dstats, plan.rows);
+    if (status) return status;
+    status = run_view_streamed(ctx, p, desc_r, desc_l, tex_r, tex_l, right, left, w, h, 1, disp_r,
+                               nullptr, nullptr, nullptr, nullptr, plan.rows);
+    if (status) return status;
+  } else if (use_fused(p)) {
     // Both views in one pass structure (stereo_fused.cu).
     FusedViews v{desc_l,           desc_r,           tex_l,          tex_r,
                  left,             right,            disp_l,         disp_r,
@@ -189,8 +367,13 @@ int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, con
                     const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
                     float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
                     uint8_t* boundary, csgm_stats* stats, bool sync) {
-  return pair_on_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
-                        reasons, boundary, stats, sync, true);
+  ViewPlan plan;
+  int status = plan_pair(ctx, p, w, h, false, &plan);
+  if (status) return status;
+  if (plan.streamed && !sync)
+    return fail(CSGM_E_INVALID, "a streamed pair needs sync != 0 (its strips use host memory)");
+  return pair_on_device(ctx, p, plan, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
+                        disp_r, reasons, boundary, stats, sync, true);
 }
 
 // Uploads, device pipeline and downloads of a pair with host buffers, queued on ctx.stream.
@@ -203,12 +386,10 @@ static int queue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* le
                            cudaEvent_t* timing /* [4] or null */) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
-  // Reserve the pipeline's own buffers before the upload so a budget failure costs no copies.
-  int64_t needed = (int64_t)pair_workspace_bytes(p, w, h, true);
-  if ((size_t)needed > ctx.ws->budget)
-    return fail(CSGM_E_NOMEM,
-                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
-                needed / 1048576.0, ctx.ws->budget / 1048576.0);
+  // The plan is settled before the upload, so a budget failure costs no copies.
+  ViewPlan plan;
+  status = plan_pair(ctx, p, w, h, true, &plan);
+  if (status) return status;
   WS(d_left, uint8_t, kImgL, n);
   WS(d_right, uint8_t, kImgR, n);
   uint8_t *d_vl = nullptr, *d_vr = nullptr;
@@ -239,7 +420,7 @@ static int queue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* le
     CK(cudaMemcpyAsync(d_vr, valid_r, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
   }
   if (timing) CK(cudaEventRecord(timing[1], ctx.stream), "event record");
-  status = pair_on_device(ctx, p, d_left, d_right, d_vl, d_vr, w, h, d_checked, d_dl, d_dr,
+  status = pair_on_device(ctx, p, plan, d_left, d_right, d_vl, d_vr, w, h, d_checked, d_dl, d_dr,
                           d_reasons, d_boundary, nullptr, false, false);
   if (status) return status;
   if (timing) CK(cudaEventRecord(timing[2], ctx.stream), "event record");
@@ -463,20 +644,20 @@ static int run_match_fused(Context& ctx, const csgm_params& p, const uint64_t* d
 }
 
 // csgm_match through the general kernels: one view, any D, uint32 aggregates, 16 paths.
-static int run_match_general(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
-                             const uint64_t* desc_b, const uint8_t* gray_a,
+// Device bytes of csgm_match on the general kernels besides its cost volume and aggregate.
+static size_t match_fixed_bytes(const csgm_params& p, int w, int h, bool summary) {
+  const size_t n = (size_t)w * h;
+  return 2 * n * words_of(p) * 8 + 6 * n + n * 4 + (summary ? 24 * n : 0) + sizeof(DeviceStats);
+}
+
+static int run_match_general(Context& ctx, const csgm_params& p, const ViewPlan& plan,
+                             const uint64_t* desc_a, const uint64_t* desc_b, const uint8_t* gray_a,
                              const uint8_t* gray_b, const uint8_t* tex_a, const uint8_t* tex_b,
                              int w, int h, int reverse, float* out_disp, int32_t* out_summary,
                              uint8_t* reasons, uint8_t* boundary, csgm_stats* stats) {
   int status = CSGM_OK;
-  size_t n = (size_t)w * h, D = (size_t)p.disparities;
+  size_t n = (size_t)w * h;
   int words = words_of(p);
-  size_t needed = 2 * n * words * 8 + 6 * n + n * 4 + (out_summary ? 24 * n : 0) +
-                  n * D * (2 + p.aggregate_bytes);
-  if (needed > ctx.ws->budget)
-    return fail(CSGM_E_NOMEM,
-                "GPU SGM search exceeds the device budget: needs %.1f MiB, budget %.1f MiB",
-                needed / 1048576.0, ctx.ws->budget / 1048576.0);
   WS(d_a, uint64_t, kDescL, n * words * 8);
   WS(d_b, uint64_t, kDescR, n * words * 8);
   WS(d_ga, uint8_t, kImgL, n);
@@ -511,8 +692,12 @@ static int run_match_general(Context& ctx, const csgm_params& p, const uint64_t*
   if (boundary)
     CK(cudaMemcpyAsync(d_boundary, boundary, n, cudaMemcpyHostToDevice, ctx.stream), "upload");
   CK(cudaMemsetAsync(dstats, 0, sizeof(DeviceStats), ctx.stream), "stats clear");
-  status = run_view_general(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
-                            d_summary, d_reasons, d_boundary, dstats);
+  if (plan.streamed)
+    status = run_view_streamed(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
+                               d_summary, d_reasons, d_boundary, dstats, plan.rows);
+  else
+    status = run_view_general(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
+                              d_summary, d_reasons, d_boundary, dstats);
   if (status) return status;
   CK(cudaMemcpyAsync(out_disp, d_out, n * 4, cudaMemcpyDeviceToHost, ctx.stream), "readback");
   if (out_summary)
@@ -534,14 +719,21 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
                    const uint8_t* tex_a, const uint8_t* tex_b, int w, int h, int reverse,
                    float* out_disp, int32_t* out_summary, uint8_t* reasons, uint8_t* boundary,
                    csgm_stats* stats) {
-  // The fused kernels when they apply and their workspace fits the budget; else the general ones.
-  if (ctx.twin && use_fused(p) && h <= 65535 &&
-      match_fused_bytes(p, w, h, out_summary != nullptr) <= ctx.ws->budget)
+  // Resident on the fused kernels when they apply and their workspace fits the budget, else
+  // resident on the general ones, else streamed (as the session's mode allows).
+  const bool summary = out_summary != nullptr;
+  if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && use_fused(p) && h <= 65535 &&
+      match_fused_bytes(p, w, h, summary) <= ctx.ws->budget)
     return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                            out_disp, out_summary, reasons, boundary, stats);
   if (ctx.twin) ctx.twin->valid = false;
-  return run_match_general(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
-                           out_disp, out_summary, reasons, boundary, stats);
+  const size_t fixed = match_fixed_bytes(p, w, h, summary);
+  const size_t cells = (size_t)w * h * p.disparities;
+  ViewPlan plan;
+  int status = choose_plan(ctx, p, w, h, fixed, fixed + cells * (2 + p.aggregate_bytes), &plan);
+  if (status) return status;
+  return run_match_general(ctx, p, plan, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h,
+                           reverse, out_disp, out_summary, reasons, boundary, stats);
 }
 
 }  // namespace csgm

@@ -20,12 +20,30 @@ int validate_params(const csgm_params* p, int w, int h);
 enum Slot {
   kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
   kCostL, kCostR, kSum, kSumUp, kSumLines, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
-  kCarry, kFlags, kPixelInfo,
+  kCarry, kFlags, kPixelInfo, kStripCarry,
   // csgm_match on the fused kernels: two sets of view inputs (descriptors l/r, grays l/r, masks
   // l/r in the pair's order), per-view outputs, the comparison flag.
   kMatchIn0, kMatchIn1 = kMatchIn0 + 6, kMatchDisp = kMatchIn1 + 6, kMatchReasons = kMatchDisp + 2,
   kMatchBoundary = kMatchReasons + 2, kMatchSummary = kMatchBoundary + 2,
   kMatchStats = kMatchSummary + 2, kMatchEqual, kSlotCount
+};
+
+// Pinned host memory that a session grows on demand (the streamed down pass parks its partial
+// aggregate there, GpuStereo.java:339-437 keeps the reference's in host RAM).
+struct HostBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t want, int* status);
+  void release();
+};
+
+// How a pair's views run: resident (the whole volume in device memory: the fused kernels where
+// they apply, else the general ones) or streamed through strips of `rows` rows (general kernels).
+struct ViewPlan {
+  bool streamed = false;
+  int rows = 0;               // strip height (the image height when resident)
+  size_t device_bytes = 0;    // device memory of the plan
+  size_t host_bytes = 0;      // pinned host memory of the plan
 };
 
 // csgm_match runs both views of a pair whenever it runs the fused kernels: the reference always
@@ -103,6 +121,10 @@ struct Context {
   long long wait_limit = 0;
   // The session's held view of csgm_match (null: csgm_match is not the caller).
   MatchTwin* twin = nullptr;
+  // Options.gpuSgm (CSGM_SGM_*) and Options.gpuStripRows: resident or streamed views.
+  int sgm_mode = CSGM_SGM_AUTO;
+  int strip_rows = 64;
+  HostBuffer* host_partial = nullptr;  // null: streaming unavailable (batch slots)
 };
 
 // One batch slot: a pair in flight with its own stream and resident workspace.
@@ -122,6 +144,11 @@ struct BatchSlot {
 
 // Bytes of device workspace a pair needs (host_inputs: include the upload/download staging).
 size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs);
+
+// The plan of a pair (GpuStereo.plan, GpuStereo.java:33-84) under the context's budget, mode and
+// strip height; CSGM_E_NOMEM when no plan fits.
+int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
+              ViewPlan* plan);
 
 int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
                     const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
@@ -167,6 +194,9 @@ struct csgm_session {
   csgm_profile profile{};
   int64_t wait_limit = 0;  // csgm_session_set_wait_limit (0 = default)
   csgm::MatchTwin twin;    // csgm_match's held view
+  int sgm_mode = CSGM_SGM_AUTO;  // csgm_session_set_streaming
+  int strip_rows = 64;
+  csgm::HostBuffer host_partial;
   // Batched / served pairs (batch.cu).
   std::vector<csgm::BatchSlot> slots;
   size_t batch_budget = 0;

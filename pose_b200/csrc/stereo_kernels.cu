@@ -79,10 +79,12 @@ __global__ void cost_volume_kernel(CostArgs a) {
   int lane = threadIdx.x & 31;
   int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t p = warp; p < n; p += warps) {
+  const int64_t first = (int64_t)a.y0 * w, count = a.rows ? (int64_t)a.rows * w : n;
+  for (int64_t local = warp; local < count; local += warps) {
+    const int64_t p = first + local;
     int x = (int)(p % w), y = (int)(p / w);
     bool inside = x >= rx && x < w - rx && y >= ry && y < h - ry && a.tex_a[p];
-    uint16_t* out = a.out + p * D;
+    uint16_t* out = a.out + local * D;
     for (int k = lane; k < D; k += 32) {
       int value = kInvalidCost;
       if (inside) {
@@ -110,14 +112,29 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   int* prev = smem + (size_t)warp * 2 * D;
   int* cur = prev + D;
-  int64_t lines = line_count(w, h, a.dx, a.dy);
+  // Lines of the strip (y strip-local); the whole image is one strip when rows is 0.
+  const int rows = a.rows ? a.rows : h, y0 = a.y0;
+  const int ady = a.dy < 0 ? -a.dy : a.dy;
+  int64_t lines = line_count(w, rows, a.dx, a.dy);
   for (int64_t line = (int64_t)blockIdx.x * warps + warp; line < lines;
        line += (int64_t)gridDim.x * warps) {
     int x, y;
-    line_start(line, w, h, a.dx, a.dy, x, y);
+    line_start(line, w, rows, a.dx, a.dy, x, y);
     int64_t prev_p = -1;
-    while (x >= 0 && x < w && y >= 0 && y < h) {
-      int64_t p = (int64_t)y * w + x;
+    if (a.carry_in && y >= 0 && y < rows) {
+      // The line's first pixel follows a pixel of the previous strip in path order: its state
+      // is carry row j (the previous strip's rows that this strip's first |dy| rows follow).
+      const int px = x - a.dx, yp = y - a.dy, gy = y0 + yp;
+      if (px >= 0 && px < w && gy >= 0 && gy < h && (yp < 0 || yp >= rows)) {
+        const int j = yp < 0 ? yp + ady : yp - rows;
+        const int32_t* src = a.carry_in + ((int64_t)j * w + px) * D;
+        for (int k = lane; k < D; k += 32) prev[k] = src[k];
+        __syncwarp();
+        prev_p = (int64_t)gy * w + px;
+      }
+    }
+    while (x >= 0 && x < w && y >= 0 && y < rows) {
+      int64_t p = (int64_t)(y0 + y) * w + x;
       bool has = prev_p >= 0 && a.tex[prev_p];
       int minimum = 0, local_p2 = a.p2;
       if (has) {
@@ -126,8 +143,15 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
         minimum = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
         local_p2 = path_p2(a.p1, a.p2, a.edge_scale, a.gray[p], a.gray[prev_p]);
       }
-      const uint16_t* c = a.cost + p * D;
-      SumT* s = sum + p * D;
+      const int64_t local = (int64_t)y * w + x;
+      const uint16_t* c = a.cost + local * D;
+      SumT* s = sum + local * D;
+      // Rows the next strip in path order follows: the last |dy| (dy > 0) or first |dy| (dy < 0).
+      int32_t* out = nullptr;
+      if (a.carry_out && a.dy != 0) {
+        const int j = a.dy > 0 ? y - (rows - ady) : y;
+        if (j >= 0 && j < ady) out = a.carry_out + ((int64_t)j * w + x) * D;
+      }
       for (int k = lane; k < D; k += 32) {
         int v = c[k];
         if (has) {
@@ -138,6 +162,7 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
         }
         cur[k] = v;
         s[k] = (SumT)(s[k] + (SumT)v);
+        if (out) out[k] = v;
       }
       __syncwarp();
       int* swap = prev;
@@ -205,10 +230,12 @@ __global__ void winners_kernel(SelectArgs a, const SumT* __restrict__ sum) {
   int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long counts[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t p = warp; p < n; p += warps) {
+  const int64_t first = (int64_t)a.y0 * w, count = a.rows ? (int64_t)a.rows * w : n;
+  for (int64_t local = warp; local < count; local += warps) {
+    const int64_t p = first + local;
     int x = (int)(p % w), y = (int)(p / w);
-    const uint16_t* c = a.cost + p * D;
-    const SumT* s = sum + p * D;
+    const uint16_t* c = a.cost + local * D;
+    const SumT* s = sum + local * D;
     int flags = (c[0] != kInvalidCost ? 1 : 0) | (c[D - 1] != kInvalidCost ? 2 : 0);
     bool region = x >= rx && x < w - rx && y >= ry && y < h - ry;
     int best = -1, value = INT_MAX, second = INT_MAX, before = -1, after = -1;
@@ -322,7 +349,7 @@ cudaError_t launch_census_texture(const CensusArgs& a, int images, cudaStream_t 
 }
 
 cudaError_t launch_cost_volume(const CostArgs& a, int sm_count, cudaStream_t stream) {
-  int64_t n = (int64_t)a.w * a.h;
+  int64_t n = (int64_t)a.w * (a.rows ? a.rows : a.h);
   cost_volume_kernel<<<grid_for(n * 32, 256, sm_count * 32), 256, 0, stream>>>(a);
   return cudaGetLastError();
 }
@@ -331,7 +358,7 @@ cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int s
                               cudaStream_t stream) {
   const int warps = 4;
   size_t shared = (size_t)warps * 2 * a.D * sizeof(int);
-  int64_t lines = line_count(a.w, a.h, a.dx, a.dy);
+  int64_t lines = line_count(a.w, a.rows ? a.rows : a.h, a.dx, a.dy);
   int grid = grid_for(lines, warps, sm_count * 64);
   if (sum_bytes == 2) {
     if (shared > 48 * 1024)
@@ -349,7 +376,7 @@ cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int s
 
 cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, int sm_count,
                            cudaStream_t stream) {
-  int64_t n = (int64_t)a.w * a.h;
+  int64_t n = (int64_t)a.w * (a.rows ? a.rows : a.h);
   int grid = grid_for(n * 32, 256, sm_count * 16);
   if (sum_bytes == 2)
     winners_kernel<uint16_t><<<grid, 256, 0, stream>>>(a, (const uint16_t*)sum);

@@ -29,6 +29,8 @@ struct CostArgs {
   const uint8_t* gray_b;
   uint16_t* out;  // [n][D], 512 = invalid
   int w, h, D, min_disparity, reverse, wx, wy, words, mode, weight, ad_cap, grad_cap, bits;
+  // Strip of rows y0 .. y0+rows-1 (rows 0 = the whole image); out is indexed strip-locally.
+  int y0 = 0, rows = 0;
 };
 
 struct PathArgs {
@@ -36,6 +38,13 @@ struct PathArgs {
   const uint8_t* tex;    // predecessor must be textured
   const uint8_t* gray;   // edge-aware P2 of the matching view
   int w, h, D, dx, dy, p1, p2, edge_scale;
+  // Strip of rows y0 .. y0+rows-1 (rows 0 = the whole image); cost and sum are strip-local.
+  // Streamed strips carry path states across strip edges: carry_in holds the states of the |dy|
+  // rows of the previous strip in path order that this strip's first pixels follow, carry_out
+  // receives this strip's |dy| rows that the next strip follows, both [|dy|][w][D] int32.
+  int y0 = 0, rows = 0;
+  const int32_t* carry_in = nullptr;
+  int32_t* carry_out = nullptr;
 };
 
 struct SelectArgs {
@@ -47,6 +56,9 @@ struct SelectArgs {
   DeviceStats* stats;  // optional
   int w, h, D, wx, wy, min_disparity;
   double uniqueness;
+  // Strip of rows y0 .. y0+rows-1 (rows 0 = the whole image): cost and sum are strip-local, the
+  // outputs are indexed by image pixel.
+  int y0 = 0, rows = 0;
 };
 
 struct LrArgs {

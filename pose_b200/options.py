@@ -45,6 +45,9 @@ class Options:
     compute: str = "gpu"
     gpuDevice: int = 0
     gpuMemoryMb: int = 0
+    # resident or streamed views (Options.java:32,39; --gpu-sgm, --gpu-strip-rows)
+    gpuSgm: str = "auto"
+    gpuStripRows: int = 64
 
     def copy(self) -> "Options":
         return copy.copy(self)
@@ -93,6 +96,10 @@ class Options:
             raise ValueError("Require 0 <= p1 < p2, 0 <= uniqueness < 1")
         if self.directions not in (4, 8, 16):
             raise ValueError("Directions must be 4 or 8 (16 is this matcher's extension)")
+        if self.gpuSgm not in ("auto", "resident", "streamed"):
+            raise ValueError("--gpu-sgm must be auto, resident or streamed")
+        if self.gpuStripRows < 1:
+            raise ValueError("--gpu-strip-rows must be positive")
         if self.compute not in ("gpu", "auto"):
             raise ValueError("--compute must be gpu or auto for this backend (no CPU fallback)")
         from .stereo_cost import StereoCost

@@ -135,10 +135,25 @@ class GpuSgm:
     def set_budget(self, nbytes: int) -> None:
         check(self.lib.csgm_session_set_budget(self.handle, int(nbytes)))
 
+    def set_streaming(self, mode: str = "auto", strip_rows: int = 64) -> None:
+        """Options.gpuSgm ("auto", "resident", "streamed") and Options.gpuStripRows."""
+        check(self.lib.csgm_session_set_streaming(self.handle, _abi.SGM_MODES[mode],
+                                                  int(strip_rows)))
+
     def plan(self, params: CsgmParams, w: int, h: int) -> int:
         out = ctypes.c_int64()
         check(self.lib.csgm_plan(self.handle, ctypes.byref(params), w, h, ctypes.byref(out)))
         return out.value
+
+    def plan_detail(self, params: CsgmParams, w: int, h: int) -> dict:
+        """GpuStereo.plan's Plan (GpuStereo.java:33-84): streamed or resident, strip rows, device
+        and pinned host bytes."""
+        rows, dev, host = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        check(self.lib.csgm_plan_detail(self.handle, ctypes.byref(params), w, h,
+                                        ctypes.byref(rows), ctypes.byref(dev),
+                                        ctypes.byref(host)))
+        return {"streamed": rows.value < h, "rows": rows.value, "device_bytes": dev.value,
+                "host_bytes": host.value}
 
     def disparityLimit(self, params: CsgmParams, w: int, h: int) -> int:
         """GpuSgm.disparityLimit (GpuSgm.java:237-245)."""
@@ -282,6 +297,7 @@ class CensusSgm:
         self.options = options.validate()
         self._own = session is None
         self.session = session or GpuSgm(options.gpuDevice, options.gpuMemoryMb)
+        self.session.set_streaming(options.gpuSgm, options.gpuStripRows)
 
     def params(self) -> CsgmParams:
         return params_from_options(self.options)

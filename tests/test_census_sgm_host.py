@@ -21,6 +21,9 @@ from reference_cpu import compute_cpu, post_from_options
 class OracleSession:
     """The GpuSgm calls CensusSgm.compute makes, answered by the oracle."""
 
+    def set_streaming(self, mode="auto", strip_rows=64):
+        self.streaming = (mode, strip_rows)
+
     def pair(self, params, left, right, w, h, validLeft=None, validRight=None, want_views=False,
              want_reasons=False):
         r = orc.pair(params, left, right, w, h, validLeft, validRight, want_reasons=True)

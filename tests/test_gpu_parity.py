@@ -185,6 +185,7 @@ def test_budget_rejects_before_allocation():
     from pose_b200.sgm import GpuSgm
 
     with GpuSgm(0, memory_mb=1) as s:
+        s.set_streaming("resident")  # the reference test's --gpu-sgm resident
         w, h, a, b, _ = storage_gpu_pair()
         prm = params_from_options(Options())
         with pytest.raises(_abi.CsgmError) as e:
