@@ -264,6 +264,20 @@ int csgm_pair(csgm_session* session, const csgm_params* params, const uint8_t* l
               uint8_t* boundary, csgm_stats* stats);
 
 /*
+ * csgm_pair for --census-mode color-distance: the descriptors and texture masks come from the
+ * colour-distance census of the interleaved BGR images (CensusSgm.colorCensus,
+ * src/main/java/sgm/CensusSgm.java:108-120,302-332), the costs and penalties from the gray images,
+ * as CensusSgm.computeRecorded runs it up to the LR check (:56-201).
+ *   left_bgr/right_bgr : uint8[3*w*h] interleaved B, G, R; both required
+ * Other arguments and outputs as csgm_pair.  HOST pointers.
+ */
+int csgm_pair_color(csgm_session* session, const csgm_params* params, const uint8_t* left,
+                    const uint8_t* right, const uint8_t* left_bgr, const uint8_t* right_bgr,
+                    const uint8_t* valid_l, const uint8_t* valid_r, int32_t w, int32_t h,
+                    float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                    uint8_t* boundary, csgm_stats* stats);
+
+/*
  * csgm_pair on device-resident buffers: every image/mask/output pointer is a device pointer on the
  * session's device (outputs may be NULL except lr_checked).  For callers whose rectified images
  * are already in HBM (a GPU rectifier upstream, or a batch driver).  With sync == 0 the call only
@@ -353,6 +367,15 @@ typedef struct csgm_post {
 int csgm_postfilter(csgm_session* s, const csgm_post* post, const uint8_t* left,
                     const uint8_t* right, const float* disp_r, int32_t w, int32_t h,
                     float* checked, uint8_t* reasons, csgm_stats* stats);
+
+/* csgm_postfilter for --census-mode color-distance: the photometric gate correlates the three
+ * channels of the interleaved BGR images (CensusSgm.java:222-224,240-250, zncc :615-644 with
+ * channels = 3); the edge-preserving median still reads the gray left image (:208-214).
+ *   left_bgr/right_bgr : uint8[3*w*h]; other arguments as csgm_postfilter.  HOST pointers. */
+int csgm_postfilter_color(csgm_session* s, const csgm_post* post, const uint8_t* left,
+                          const uint8_t* right, const uint8_t* left_bgr, const uint8_t* right_bgr,
+                          const float* disp_r, int32_t w, int32_t h, float* checked,
+                          uint8_t* reasons, csgm_stats* stats);
 
 /* Page-locked host memory (cudaMallocHost) for batch inputs and outputs; csgm_host_free releases
  * it.  No counterpart in the reference (its FFM arenas are pageable). */

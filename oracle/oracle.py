@@ -53,6 +53,11 @@ def load() -> ctypes.CDLL:
         lib.oracle_postfilter.argtypes = [_P, _P, _P, _P, i32, i32, _P,
                                           ctypes.POINTER(CsgmStats), _P]
         lib.oracle_postfilter.restype = None
+        lib.oracle_pair_color.argtypes = [ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _P, _P, i32,
+                                          i32, _P, _P, _P, ctypes.POINTER(CsgmStats), _P, _P]
+        lib.oracle_postfilter_color.argtypes = [_P, _P, _P, _P, _P, _P, i32, i32, _P,
+                                                ctypes.POINTER(CsgmStats), _P]
+        lib.oracle_postfilter_color.restype = None
         lib.oracle_zncc.restype = f64
         lib.oracle_zncc.argtypes = [_P, _P, i32, i32, i32, i32, f64, i32, i32]
         lib.oracle_set_threads.argtypes = [i32]
@@ -149,8 +154,10 @@ def lr_check(dl, dr, w, h, rx, ry, threshold, reasons=None):
     return out, stats
 
 
-def pair(params: CsgmParams, left, right, w, h, valid_l=None, valid_r=None, want_reasons=False):
-    """Census + both views + LR check (CensusSgm.computeRecorded :56-201)."""
+def pair(params: CsgmParams, left, right, w, h, valid_l=None, valid_r=None, want_reasons=False,
+         left_bgr=None, right_bgr=None):
+    """Census + both views + LR check (CensusSgm.computeRecorded :56-201); with the BGR images,
+    the colour-distance census of --census-mode color-distance."""
     n = w * h
     left, right, valid_l, valid_r = _u8(left), _u8(right), _u8(valid_l), _u8(valid_r)
     checked = np.empty(n, np.float32)
@@ -159,17 +166,32 @@ def pair(params: CsgmParams, left, right, w, h, valid_l=None, valid_r=None, want
     reasons = np.empty(n, np.uint8) if want_reasons else None
     boundary = np.empty(n, np.uint8) if want_reasons else None
     stats = CsgmStats()
-    rc = load().oracle_pair(ctypes.byref(params), _ptr(left), _ptr(right), _ptr(valid_l),
-                            _ptr(valid_r), w, h, _ptr(checked), _ptr(dl), _ptr(dr),
-                            ctypes.byref(stats), _ptr(reasons), _ptr(boundary))
+    if left_bgr is not None:
+        lb, rb = _u8(left_bgr), _u8(right_bgr)
+        rc = load().oracle_pair_color(ctypes.byref(params), _ptr(left), _ptr(right), _ptr(lb),
+                                      _ptr(rb), _ptr(valid_l), _ptr(valid_r), w, h,
+                                      _ptr(checked), _ptr(dl), _ptr(dr), ctypes.byref(stats),
+                                      _ptr(reasons), _ptr(boundary))
+    else:
+        rc = load().oracle_pair(ctypes.byref(params), _ptr(left), _ptr(right), _ptr(valid_l),
+                                _ptr(valid_r), w, h, _ptr(checked), _ptr(dl), _ptr(dr),
+                                ctypes.byref(stats), _ptr(reasons), _ptr(boundary))
     if rc != 0:
         raise ValueError("oracle_pair rejected its arguments")
     return {"checked": checked, "dl": dl, "dr": dr, "stats": stats, "reasons": reasons,
             "boundary": boundary}
 
 
-def postfilter(post: OraclePost, left, right, dr, w, h, checked, stats: CsgmStats, reasons=None):
-    """Median, reciprocity, photometric gate, speckles and the valid count, in place."""
+def postfilter(post: OraclePost, left, right, dr, w, h, checked, stats: CsgmStats, reasons=None,
+               left_bgr=None, right_bgr=None):
+    """Median, reciprocity, photometric gate, speckles and the valid count, in place; with the
+    BGR images, the three-channel gate of --census-mode color-distance."""
+    if left_bgr is not None:
+        load().oracle_postfilter_color(ctypes.byref(post), _ptr(_u8(left)), _ptr(_u8(right)),
+                                       _ptr(_u8(left_bgr)), _ptr(_u8(right_bgr)),
+                                       _ptr(np.ascontiguousarray(dr, np.float32)), w, h,
+                                       _ptr(checked), ctypes.byref(stats), _ptr(reasons))
+        return
     load().oracle_postfilter(ctypes.byref(post), _ptr(_u8(left)), _ptr(_u8(right)),
                              _ptr(np.ascontiguousarray(dr, np.float32)), w, h, _ptr(checked),
                              ctypes.byref(stats), _ptr(reasons))

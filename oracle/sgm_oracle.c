@@ -414,10 +414,33 @@ void oracle_lr_check(const float* dl, const float* dr, int w, int h, int rx, int
     }
 }
 
+static int pair_impl(const csgm_params* prm, const uint8_t* left, const uint8_t* right,
+                     const uint8_t* left_bgr, const uint8_t* right_bgr, const uint8_t* valid_l,
+                     const uint8_t* valid_r, int w, int h, float* checked, float* dl, float* dr,
+                     csgm_stats* stats, uint8_t* reasons, uint8_t* boundary);
+
 int oracle_pair(const csgm_params* prm, const uint8_t* left, const uint8_t* right,
                 const uint8_t* valid_l, const uint8_t* valid_r, int w, int h, float* checked,
                 float* dl, float* dr, csgm_stats* stats, uint8_t* reasons, uint8_t* boundary) {
-  /* CensusSgm.computeRecorded, CensusSgm.java:56-201. */
+  return pair_impl(prm, left, right, 0, 0, valid_l, valid_r, w, h, checked, dl, dr, stats,
+                   reasons, boundary);
+}
+
+int oracle_pair_color(const csgm_params* prm, const uint8_t* left, const uint8_t* right,
+                      const uint8_t* left_bgr, const uint8_t* right_bgr, const uint8_t* valid_l,
+                      const uint8_t* valid_r, int w, int h, float* checked, float* dl, float* dr,
+                      csgm_stats* stats, uint8_t* reasons, uint8_t* boundary) {
+  if (!left_bgr || !right_bgr) return -1; /* :110-115 */
+  return pair_impl(prm, left, right, left_bgr, right_bgr, valid_l, valid_r, w, h, checked, dl, dr,
+                   stats, reasons, boundary);
+}
+
+static int pair_impl(const csgm_params* prm, const uint8_t* left, const uint8_t* right,
+                     const uint8_t* left_bgr, const uint8_t* right_bgr, const uint8_t* valid_l,
+                     const uint8_t* valid_r, int w, int h, float* checked, float* dl, float* dr,
+                     csgm_stats* stats, uint8_t* reasons, uint8_t* boundary) {
+  /* CensusSgm.computeRecorded, CensusSgm.java:56-201; colour-distance descriptors and texture
+   * (:108-120) when the BGR images are given, gray census otherwise (:121-126). */
   if (w < prm->window_x + 2 || h < prm->window_y + 2) return -1; /* :56-60 */
   long n = (long)w * h;
   int words = oracle_words(prm->window_x, prm->window_y);
@@ -431,10 +454,15 @@ int oracle_pair(const csgm_params* prm, const uint8_t* left, const uint8_t* righ
   memset(&local, 0, sizeof local);
   if (reasons) memset(reasons, 1, (size_t)n); /* :104-106 */
   if (boundary) memset(boundary, 0, (size_t)n);
-  oracle_census(left, w, h, prm->window_x, prm->window_y, a);   /* :122 */
-  oracle_census(right, w, h, prm->window_x, prm->window_y, b);  /* :123 */
-  oracle_texture(left, w, h, prm->window_x, prm->window_y, ta);  /* :124 */
-  oracle_texture(right, w, h, prm->window_x, prm->window_y, tb); /* :125 */
+  if (left_bgr) {
+    oracle_color_census(left_bgr, w, h, prm->window_x, prm->window_y, a, ta);  /* :116 */
+    oracle_color_census(right_bgr, w, h, prm->window_x, prm->window_y, b, tb); /* :117 */
+  } else {
+    oracle_census(left, w, h, prm->window_x, prm->window_y, a);   /* :122 */
+    oracle_census(right, w, h, prm->window_x, prm->window_y, b);  /* :123 */
+    oracle_texture(left, w, h, prm->window_x, prm->window_y, ta);  /* :124 */
+    oracle_texture(right, w, h, prm->window_x, prm->window_y, tb); /* :125 */
+  }
   if (valid_l && valid_r) /* :127-134 */
     for (long i = 0; i < n; i++) {
       ta[i] = ta[i] && valid_l[i];
@@ -594,10 +622,32 @@ int64_t oracle_remove_speckles(float* a, int w, int h, int minimum, double range
   return rejected;
 }
 
+static void postfilter_impl(const oracle_post* post, const uint8_t* left, const uint8_t* right,
+                            const uint8_t* photo_left, const uint8_t* photo_right, int channels,
+                            const float* dr, int w, int h, float* checked, csgm_stats* stats,
+                            uint8_t* reasons);
+
 void oracle_postfilter(const oracle_post* post, const uint8_t* left, const uint8_t* right,
                        const float* dr, int w, int h, float* checked, csgm_stats* stats,
                        uint8_t* reasons) {
-  /* CensusSgm.java:203-272 (gray census mode: one channel). */
+  /* Gray census mode: the photometric gate on the gray images, one channel (:222-224). */
+  postfilter_impl(post, left, right, left, right, 1, dr, w, h, checked, stats, reasons);
+}
+
+void oracle_postfilter_color(const oracle_post* post, const uint8_t* left, const uint8_t* right,
+                             const uint8_t* left_bgr, const uint8_t* right_bgr, const float* dr,
+                             int w, int h, float* checked, csgm_stats* stats, uint8_t* reasons) {
+  /* --census-mode color-distance: the gate on the interleaved BGR images, three channels
+   * (:222-224); the edge-preserving median still reads the gray left image (:208-214). */
+  postfilter_impl(post, left, right, left_bgr, right_bgr, 3, dr, w, h, checked, stats, reasons);
+}
+
+static void postfilter_impl(const oracle_post* post, const uint8_t* left, const uint8_t* right,
+                            const uint8_t* photo_left, const uint8_t* photo_right, int channels,
+                            const float* dr, int w, int h, float* checked, csgm_stats* stats,
+                            uint8_t* reasons) {
+  /* CensusSgm.java:203-272. */
+  (void)right;
   long n = (long)w * h;
   if (post->median > 1) { /* :203-214 */
     float* filtered = (float*)malloc(sizeof(float) * (size_t)n);
@@ -620,7 +670,8 @@ void oracle_postfilter(const oracle_post* post, const uint8_t* left, const uint8
         if (reasons) reasons[p] = 5;
         continue;
       }
-      double score = oracle_zncc(left, right, w, h, x, y, disparity, post->correlation_window / 2, 1);
+      double score = oracle_zncc(photo_left, photo_right, w, h, x, y, disparity,
+                                 post->correlation_window / 2, channels);
       if (score < post->correlation) {
         checked[p] = NAN;
         stats->photometric_rejected++;

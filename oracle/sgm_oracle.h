@@ -115,6 +115,19 @@ void oracle_postfilter(const oracle_post* post, const uint8_t* left, const uint8
                        const float* dr, int w, int h, float* checked, csgm_stats* stats,
                        uint8_t* reasons);
 
+/* --census-mode color-distance: the pair from colour-distance descriptors and texture of the
+ * interleaved BGR images (CensusSgm.java:108-120), the gray images for the costs and penalties. */
+int oracle_pair_color(const csgm_params* prm, const uint8_t* left, const uint8_t* right,
+                      const uint8_t* left_bgr, const uint8_t* right_bgr, const uint8_t* valid_l,
+                      const uint8_t* valid_r, int w, int h, float* checked, float* dl, float* dr,
+                      csgm_stats* stats, uint8_t* reasons, uint8_t* boundary);
+
+/* The post-filters in colour-distance mode: the photometric gate over three channels of the BGR
+ * images (CensusSgm.java:222-224,240-250). */
+void oracle_postfilter_color(const oracle_post* post, const uint8_t* left, const uint8_t* right,
+                             const uint8_t* left_bgr, const uint8_t* right_bgr, const float* dr,
+                             int w, int h, float* checked, csgm_stats* stats, uint8_t* reasons);
+
 /* Worker threads used by oracle_match/oracle_pair (1 = the reference's single thread). */
 void oracle_set_threads(int threads);
 int oracle_get_threads(void);

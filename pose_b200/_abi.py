@@ -194,6 +194,16 @@ SIGNATURES = {
          ctypes.POINTER(CsgmStats)],
     ),
     "csgm_color_census": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _P]),
+    "csgm_pair_color": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,
+         ctypes.POINTER(CsgmStats)],
+    ),
+    "csgm_postfilter_color": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmPost), _P, _P, _P, _P, _P, _I32, _I32, _P, _P,
+         ctypes.POINTER(CsgmStats)],
+    ),
     "csgm_postfilter": (
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmPost), _P, _P, _P, _I32, _I32, _P, _P, ctypes.POINTER(CsgmStats)],

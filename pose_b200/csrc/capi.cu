@@ -453,6 +453,31 @@ int csgm_pair(csgm_session* s, const csgm_params* p, const uint8_t* left, const 
                        reasons, boundary, stats);
 }
 
+int csgm_pair_color(csgm_session* s, const csgm_params* p, const uint8_t* left,
+                    const uint8_t* right, const uint8_t* left_bgr, const uint8_t* right_bgr,
+                    const uint8_t* valid_l, const uint8_t* valid_r, int32_t w, int32_t h,
+                    float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
+                    uint8_t* boundary, csgm_stats* stats) {
+  if (!s) return fail(CSGM_E_INVALID, "NULL session");
+  if (!left || !right || !lr_checked) return fail(CSGM_E_INVALID, "NULL image or output buffer");
+  if (!left_bgr || !right_bgr)
+    return fail(CSGM_E_INVALID, "Color-distance census requires interleaved BGR inputs");
+  if ((valid_l == nullptr) != (valid_r == nullptr))
+    return fail(CSGM_E_INVALID, "Invalid stereo mask dimensions");
+  int rc = validate_params(p, w, h);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> guard(s->lock);
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) return cuda_fail(e, "Device selection");
+  Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
+  ctx.wait_limit = s->wait_limit;
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
+  return run_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
+                       reasons, boundary, stats, left_bgr, right_bgr);
+}
+
 int csgm_pair_device(csgm_session* s, const csgm_params* p, const uint8_t* left,
                      const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
                      int32_t w, int32_t h, float* lr_checked, float* disp_l, float* disp_r,

@@ -16,6 +16,7 @@
 
 #include "collinea_sgm.h"
 #include "pipeline.h"
+#include "stereo_kernels.h"
 
 namespace csgm {
 namespace {
@@ -30,8 +31,9 @@ __device__ __forceinline__ double bgr_distance(const uint8_t* bgr, int64_t q, in
   return __dsqrt_rn(squared);
 }
 
-__global__ void color_census_kernel(const uint8_t* bgr, int w, int h, int wx, int wy, int words,
-                                    uint64_t* desc, uint8_t* tex) {
+// valid (optional): the pair's validity mask, ANDed into the texture mask (CensusSgm.java:127-134).
+__global__ void color_census_kernel(const uint8_t* bgr, const uint8_t* valid, int w, int h, int wx,
+                                    int wy, int words, uint64_t* desc, uint8_t* tex) {
   const int rx = wx / 2, ry = wy / 2;
   const int64_t n = (int64_t)w * h;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
@@ -61,11 +63,22 @@ __global__ void color_census_kernel(const uint8_t* bgr, int w, int h, int wx, in
         }
     }
     for (int j = 0; j < words; j++) desc[(int64_t)j * n + p] = bits[j];
-    tex[p] = textured;
+    tex[p] = textured && (valid == nullptr || valid[p] != 0);
   }
 }
 
 }  // namespace
+
+cudaError_t launch_color_census(const uint8_t* bgr, const uint8_t* valid, int w, int h, int wx,
+                                int wy, uint64_t* desc, uint8_t* tex, int sm_count,
+                                cudaStream_t stream) {
+  const int64_t n = (int64_t)w * h, blocks = (n + 255) / 256;
+  const int grid = (int)(blocks < (int64_t)sm_count * 16 ? blocks : (int64_t)sm_count * 16);
+  color_census_kernel<<<grid, 256, 0, stream>>>(bgr, valid, w, h, wx, wy, (wx * wy - 1 + 63) / 64,
+                                               desc, tex);
+  return cudaGetLastError();
+}
+
 }  // namespace csgm
 
 using namespace csgm;
@@ -93,10 +106,7 @@ extern "C" int csgm_color_census(csgm_session* s, const uint8_t* bgr, int32_t w,
   cudaStream_t st = s->stream;
   e = cudaMemcpyAsync(d_bgr, bgr, 3 * n, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_fail(e, "colour census upload");
-  const int64_t blocks = (n + 255) / 256;
-  const int grid = (int)(blocks < (int64_t)s->sm_count * 16 ? blocks : (int64_t)s->sm_count * 16);
-  color_census_kernel<<<grid, 256, 0, st>>>(d_bgr, w, h, window_x, window_y, words, d_desc, d_tex);
-  e = cudaGetLastError();
+  e = launch_color_census(d_bgr, nullptr, w, h, window_x, window_y, d_desc, d_tex, s->sm_count, st);
   if (e != cudaSuccess) return cuda_fail(e, "colour census launch");
   s->profiler.launches++;
   e = cudaMemcpyAsync(descriptors, d_desc, 8 * n * words, cudaMemcpyDeviceToHost, st);

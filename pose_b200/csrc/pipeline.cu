@@ -32,9 +32,10 @@ static bool use_fused(const csgm_params& p) {
 
 // Device bytes of a pair besides its cost volumes and aggregates: descriptors, masks, the views'
 // disparities, counters and (host_inputs) the upload / download buffers.
-static size_t pair_fixed_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
+static size_t pair_fixed_bytes(const csgm_params& p, int w, int h, bool host_inputs,
+                               bool color) {
   size_t n = (size_t)w * h, words = (size_t)words_of(p);
-  size_t bytes = 0;
+  size_t bytes = color ? 6 * n : 0;  // BGR images
   bytes += 2 * n * words * 8;  // descriptors
   bytes += 2 * n;              // texture masks
   bytes += 2 * n * 4;          // raw view disparities
@@ -43,9 +44,9 @@ static size_t pair_fixed_bytes(const csgm_params& p, int w, int h, bool host_inp
   return bytes;
 }
 
-size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs) {
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs, bool color) {
   size_t n = (size_t)w * h, D = (size_t)p.disparities;
-  size_t bytes = pair_fixed_bytes(p, w, h, host_inputs);
+  size_t bytes = pair_fixed_bytes(p, w, h, host_inputs, color);
   if (use_fused(p))
     bytes += fused_workspace_bytes(p, w, h);
   else
@@ -102,9 +103,9 @@ static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, s
 }
 
 int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
-              ViewPlan* plan) {
-  return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs),
-                     pair_workspace_bytes(p, w, h, host_inputs), plan);
+              ViewPlan* plan, bool color) {
+  return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs, color),
+                     pair_workspace_bytes(p, w, h, host_inputs, color), plan);
 }
 
 void* HostBuffer::get(size_t want, int* status) {
@@ -274,7 +275,8 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
                           const uint8_t* left, const uint8_t* right, const uint8_t* valid_l,
                           const uint8_t* valid_r, int w, int h, float* lr_checked, float* disp_l,
                           float* disp_r, uint8_t* reasons, uint8_t* boundary, csgm_stats* stats,
-                          bool sync, bool own_call) {
+                          bool sync, bool own_call, const uint8_t* bgr_l = nullptr,
+                          const uint8_t* bgr_r = nullptr) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
   int words = words_of(p);
@@ -301,18 +303,31 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
   CK(cudaMemsetAsync(dstats, 0, sizeof(DeviceStats), ctx.stream), "stats clear");
   if (reasons) CK(cudaMemsetAsync(reasons, 1, n, ctx.stream), "reasons init");
   if (boundary) CK(cudaMemsetAsync(boundary, 0, n, ctx.stream), "boundary init");
-  // CensusSgm.java:122-134: descriptors, texture masks, AND with the validity masks.
-  CensusArgs ca{};
-  ca.image[0] = {left, valid_l, desc_l, tex_l};
-  ca.image[1] = {right, valid_r, desc_r, tex_r};
-  ca.w = w;
-  ca.h = h;
-  ca.wx = p.window_x;
-  ca.wy = p.window_y;
-  ca.words = words;
-  ctx.prof->kernel_begin();
-  CK(launch_census_texture(ca, 2, ctx.stream), "census kernel launch");
-  ctx.prof->kernel_end("census_texture");
+  if (bgr_l) {
+    // CensusSgm.java:108-120,127-134: colour-distance descriptors and texture of the BGR images,
+    // AND with the validity masks.
+    ctx.prof->kernel_begin();
+    CK(launch_color_census(bgr_l, valid_l, w, h, p.window_x, p.window_y, desc_l, tex_l,
+                           ctx.sm_count, ctx.stream),
+       "colour census launch");
+    CK(launch_color_census(bgr_r, valid_r, w, h, p.window_x, p.window_y, desc_r, tex_r,
+                           ctx.sm_count, ctx.stream),
+       "colour census launch");
+    ctx.prof->kernel_end("color_census");
+  } else {
+    // CensusSgm.java:122-134: descriptors, texture masks, AND with the validity masks.
+    CensusArgs ca{};
+    ca.image[0] = {left, valid_l, desc_l, tex_l};
+    ca.image[1] = {right, valid_r, desc_r, tex_r};
+    ca.w = w;
+    ca.h = h;
+    ca.wx = p.window_x;
+    ca.wy = p.window_y;
+    ca.words = words;
+    ctx.prof->kernel_begin();
+    CK(launch_census_texture(ca, 2, ctx.stream), "census kernel launch");
+    ctx.prof->kernel_end("census_texture");
+  }
   if (plan.streamed) {
     // Both views through strips (general kernels); the right view's counters are discarded.
     status = run_view_streamed(ctx, p, desc_l, desc_r, tex_l, tex_r, left, right, w, h, 0, disp_l,
@@ -383,13 +398,21 @@ static int queue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* le
                            const uint8_t* right, const uint8_t* valid_l, const uint8_t* valid_r,
                            int w, int h, float* lr_checked, float* disp_l, float* disp_r,
                            uint8_t* reasons, uint8_t* boundary, DeviceStats* stats_dst,
-                           cudaEvent_t* timing /* [4] or null */) {
+                           cudaEvent_t* timing /* [4] or null */,
+                           const uint8_t* bgr_l = nullptr, const uint8_t* bgr_r = nullptr) {
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
   // The plan is settled before the upload, so a budget failure costs no copies.
   ViewPlan plan;
-  status = plan_pair(ctx, p, w, h, true, &plan);
+  status = plan_pair(ctx, p, w, h, true, &plan, bgr_l != nullptr);
   if (status) return status;
+  uint8_t *d_bgr_l = nullptr, *d_bgr_r = nullptr;
+  if (bgr_l) {
+    WS(a, uint8_t, kBgrL, 3 * n);
+    WS(b, uint8_t, kBgrR, 3 * n);
+    d_bgr_l = a;
+    d_bgr_r = b;
+  }
   WS(d_left, uint8_t, kImgL, n);
   WS(d_right, uint8_t, kImgR, n);
   uint8_t *d_vl = nullptr, *d_vr = nullptr;
@@ -419,9 +442,13 @@ static int queue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* le
     CK(cudaMemcpyAsync(d_vl, valid_l, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
     CK(cudaMemcpyAsync(d_vr, valid_r, n, cudaMemcpyHostToDevice, ctx.stream), "mask upload");
   }
+  if (bgr_l) {
+    CK(cudaMemcpyAsync(d_bgr_l, bgr_l, 3 * n, cudaMemcpyHostToDevice, ctx.stream), "BGR upload");
+    CK(cudaMemcpyAsync(d_bgr_r, bgr_r, 3 * n, cudaMemcpyHostToDevice, ctx.stream), "BGR upload");
+  }
   if (timing) CK(cudaEventRecord(timing[1], ctx.stream), "event record");
   status = pair_on_device(ctx, p, plan, d_left, d_right, d_vl, d_vr, w, h, d_checked, d_dl, d_dr,
-                          d_reasons, d_boundary, nullptr, false, false);
+                          d_reasons, d_boundary, nullptr, false, false, d_bgr_l, d_bgr_r);
   if (status) return status;
   if (timing) CK(cudaEventRecord(timing[2], ctx.stream), "event record");
   CK(cudaMemcpyAsync(lr_checked, d_checked, n * 4, cudaMemcpyDeviceToHost, ctx.stream),
@@ -453,7 +480,8 @@ int enqueue_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left,
 int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
                   const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
                   float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
-                  uint8_t* boundary, csgm_stats* stats) {
+                  uint8_t* boundary, csgm_stats* stats, const uint8_t* bgr_l,
+                  const uint8_t* bgr_r) {
   size_t n = (size_t)w * h;
   bool timed = ctx.prof->level >= 1;
   ctx.prof->begin_call(ctx.stream);
@@ -462,7 +490,8 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
     for (auto& e : ev) e = ctx.prof->event();
   DeviceStats host{};
   int status = queue_pair_host(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
-                               disp_r, reasons, boundary, &host, timed ? ev : nullptr);
+                               disp_r, reasons, boundary, &host, timed ? ev : nullptr, bgr_l,
+                               bgr_r);
   if (status) return status;
   CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
   if (host.pad) return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host.pad);
@@ -471,7 +500,7 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
     ctx.profile->upload_ns += (int64_t)(elapsed_ms(ev[0], ev[1]) * 1e6);
     ctx.profile->kernel_ns += (int64_t)(elapsed_ms(ev[1], ev[2]) * 1e6);
     ctx.profile->download_ns += (int64_t)(elapsed_ms(ev[2], ev[3]) * 1e6);
-    ctx.profile->uploaded_bytes += (int64_t)(valid_l ? 4 * n : 2 * n);
+    ctx.profile->uploaded_bytes += (int64_t)((valid_l ? 4 * n : 2 * n) + (bgr_l ? 6 * n : 0));
     ctx.profile->downloaded_bytes += (int64_t)(n * 4 * (1 + (disp_l != 0) + (disp_r != 0)) +
                                                (reasons ? n : 0) + (boundary ? n : 0));
     ctx.profile->calls++;

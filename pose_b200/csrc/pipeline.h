@@ -20,7 +20,7 @@ int validate_params(const csgm_params* p, int w, int h);
 enum Slot {
   kImgL, kImgR, kValidL, kValidR, kDescL, kDescR, kTexL, kTexR,
   kCostL, kCostR, kSum, kSumUp, kSumLines, kPen, kDispL, kDispR, kChecked, kReasons, kBoundary, kSummary, kStats,
-  kCarry, kFlags, kPixelInfo, kStripCarry,
+  kCarry, kFlags, kPixelInfo, kStripCarry, kBgrL, kBgrR,
   // csgm_match on the fused kernels: two sets of view inputs (descriptors l/r, grays l/r, masks
   // l/r in the pair's order), per-view outputs, the comparison flag.
   kMatchIn0, kMatchIn1 = kMatchIn0 + 6, kMatchDisp = kMatchIn1 + 6, kMatchReasons = kMatchDisp + 2,
@@ -142,23 +142,28 @@ struct BatchSlot {
   size_t reserved = 0;                // bytes admitted for it
 };
 
-// Bytes of device workspace a pair needs (host_inputs: include the upload/download staging).
-size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs);
+// Bytes of device workspace a pair needs (host_inputs: include the upload/download staging;
+// color: the two interleaved BGR images of --census-mode color-distance).
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs,
+                            bool color = false);
 
 // The plan of a pair (GpuStereo.plan, GpuStereo.java:33-84) under the context's budget, mode and
 // strip height; CSGM_E_NOMEM when no plan fits.
 int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
-              ViewPlan* plan);
+              ViewPlan* plan, bool color = false);
 
 int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
                     const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
                     float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
                     uint8_t* boundary, csgm_stats* stats, bool sync);
 
+// bgr_l / bgr_r (optional, both or neither): the interleaved BGR images whose colour-distance
+// census gives the descriptors and texture (--census-mode color-distance).
 int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
                   const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
                   float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
-                  uint8_t* boundary, csgm_stats* stats);
+                  uint8_t* boundary, csgm_stats* stats, const uint8_t* bgr_l = nullptr,
+                  const uint8_t* bgr_r = nullptr);
 
 int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
                    const uint64_t* desc_b, const uint8_t* gray_a, const uint8_t* gray_b,

@@ -96,10 +96,11 @@ __global__ void median_kernel(const float* a, const uint8_t* gray, int w, int h,
   }
 }
 
-// ZNCC of the left window at (x, y) and the right window at x - disparity, one gray channel
-// (CensusSgm.java:615-644); -1 where a window leaves the image or is too flat.
+// ZNCC of the left window at (x, y) and the right window at x - disparity over `channels`
+// interleaved channels (CensusSgm.java:615-644: one gray channel, or B, G, R in colour-distance
+// mode); -1 where a window leaves the image or is too flat.
 __device__ double zncc_score(const uint8_t* a, const uint8_t* b, int w, int h, int x, int y,
-                             double disparity, int r) {
+                             double disparity, int r, int channels) {
   const double target = __dsub_rn((double)x, disparity);
   const int bx = (int)floor(target);
   const double fraction = __dsub_rn(target, (double)bx);
@@ -107,30 +108,34 @@ __device__ double zncc_score(const uint8_t* a, const uint8_t* b, int w, int h, i
     return -1;
   const int n = (2 * r + 1) * (2 * r + 1);
   const double keep = __dsub_rn(1.0, fraction);
-  double sa = 0, sb = 0, saa = 0, sbb = 0, sab = 0;
-  for (int dy = -r; dy <= r; dy++)
-    for (int dx = -r; dx <= r; dx++) {
-      const int64_t ai = (int64_t)(y + dy) * w + x + dx;
-      const int64_t bi = (int64_t)(y + dy) * w + bx + dx;
-      const double av = (double)a[ai];
-      const double bv = __dadd_rn(__dmul_rn(keep, (double)b[bi]), __dmul_rn(fraction, (double)b[bi + 1]));
-      sa = __dadd_rn(sa, av);
-      sb = __dadd_rn(sb, bv);
-      saa = __dadd_rn(saa, __dmul_rn(av, av));
-      sbb = __dadd_rn(sbb, __dmul_rn(bv, bv));
-      sab = __dadd_rn(sab, __dmul_rn(av, bv));
-    }
   const double dn = (double)n;
-  const double covariance = __dadd_rn(0.0, __dsub_rn(sab, __ddiv_rn(__dmul_rn(sa, sb), dn)));
-  const double var_a = __dadd_rn(0.0, __dsub_rn(saa, __ddiv_rn(__dmul_rn(sa, sa), dn)));
-  const double var_b = __dadd_rn(0.0, __dsub_rn(sbb, __ddiv_rn(__dmul_rn(sb, sb), dn)));
-  if (var_a < n * 4 || var_b < n * 4) return -1;
+  double covariance = 0, var_a = 0, var_b = 0;
+  for (int channel = 0; channel < channels; channel++) {
+    double sa = 0, sb = 0, saa = 0, sbb = 0, sab = 0;
+    for (int dy = -r; dy <= r; dy++)
+      for (int dx = -r; dx <= r; dx++) {
+        const int64_t ai = ((int64_t)(y + dy) * w + x + dx) * channels + channel;
+        const int64_t bi = ((int64_t)(y + dy) * w + bx + dx) * channels + channel;
+        const double av = (double)a[ai];
+        const double bv = __dadd_rn(__dmul_rn(keep, (double)b[bi]),
+                                    __dmul_rn(fraction, (double)b[bi + channels]));
+        sa = __dadd_rn(sa, av);
+        sb = __dadd_rn(sb, bv);
+        saa = __dadd_rn(saa, __dmul_rn(av, av));
+        sbb = __dadd_rn(sbb, __dmul_rn(bv, bv));
+        sab = __dadd_rn(sab, __dmul_rn(av, bv));
+      }
+    covariance = __dadd_rn(covariance, __dsub_rn(sab, __ddiv_rn(__dmul_rn(sa, sb), dn)));
+    var_a = __dadd_rn(var_a, __dsub_rn(saa, __ddiv_rn(__dmul_rn(sa, sa), dn)));
+    var_b = __dadd_rn(var_b, __dsub_rn(sbb, __ddiv_rn(__dmul_rn(sb, sb), dn)));
+  }
+  if (var_a < channels * n * 4 || var_b < channels * n * 4) return -1;
   const double product = __dmul_rn(var_a, var_b);
   return __ddiv_rn(covariance, __dsqrt_rn(product > 1e-12 ? product : 1e-12));
 }
 
 struct GateArgs {
-  const uint8_t* left;
+  const uint8_t* left;   // images the gate correlates: gray, or interleaved BGR
   const uint8_t* right;
   const float* dr;
   float* checked;
@@ -138,6 +143,7 @@ struct GateArgs {
   PostCounts* counts;
   int w, h, border, radius;
   double tolerance, correlation;
+  int channels;  // 1 gray, 3 BGR
 };
 
 // Reciprocity (CensusSgm.java:604-612), then the photometric gate (:240-257).
@@ -164,7 +170,8 @@ __global__ void gate_kernel(const GateArgs g) {
       if (g.reasons) g.reasons[p] = 5;
       continue;
     }
-    const double score = zncc_score(g.left, g.right, g.w, g.h, x, y, (double)d, g.radius);
+    const double score =
+        zncc_score(g.left, g.right, g.w, g.h, x, y, (double)d, g.radius, g.channels);
     if (score < g.correlation) {
       g.checked[p] = __int_as_float(0x7fc00000);
       photometric++;
@@ -301,9 +308,12 @@ void launch_median(const float* a, const uint8_t* gray, int w, int h, const csgm
 
 using namespace csgm;
 
-extern "C" int csgm_postfilter(csgm_session* s, const csgm_post* post, const uint8_t* left,
-                               const uint8_t* right, const float* disp_r, int32_t w, int32_t h,
-                               float* checked, uint8_t* reasons, csgm_stats* stats) {
+// The post-filters; with left_bgr / right_bgr the photometric gate correlates the three BGR
+// channels (CensusSgm.java:222-224), while the edge-preserving median reads the gray left image.
+static int postfilter_impl(csgm_session* s, const csgm_post* post, const uint8_t* left,
+                           const uint8_t* right, const uint8_t* left_bgr,
+                           const uint8_t* right_bgr, const float* disp_r, int32_t w, int32_t h,
+                           float* checked, uint8_t* reasons, csgm_stats* stats) {
   if (!s) return fail(CSGM_E_INVALID, "NULL session");
   if (!left || !right || !disp_r || !checked)
     return fail(CSGM_E_INVALID, "NULL image, right-view or checked buffer");
@@ -329,6 +339,19 @@ extern "C" int csgm_postfilter(csgm_session* s, const csgm_post* post, const uin
   PostCounts* d_counts = d_size ? (PostCounts*)ws.get(kStats, sizeof(PostCounts), &status)
                                 : nullptr;
   if (!d_counts) return status ? status : fail(CSGM_E_NOMEM, "post-filter workspace");
+  const int channels = left_bgr ? 3 : 1;
+  const uint8_t* photo_l = d_left;
+  const uint8_t* photo_r = d_right;
+  if (left_bgr) {
+    uint8_t* bl = (uint8_t*)ws.get(kBgrL, 3 * n, &status);
+    uint8_t* br = bl ? (uint8_t*)ws.get(kBgrR, 3 * n, &status) : nullptr;
+    if (!br) return status;
+    e = cudaMemcpyAsync(bl, left_bgr, 3 * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(br, right_bgr, 3 * n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "post-filter BGR upload");
+    photo_l = bl;
+    photo_r = br;
+  }
 
   e = cudaMemcpyAsync(d_left, left, n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_right, right, n, cudaMemcpyHostToDevice, st);
@@ -351,8 +374,8 @@ extern "C" int csgm_postfilter(csgm_session* s, const csgm_post* post, const uin
     }
     map = d_median;
   }
-  GateArgs g{d_left, d_right, d_dr, map, d_reasons, d_counts, w, h, post->border,
-             post->correlation_window / 2, post->lr_threshold, post->correlation};
+  GateArgs g{photo_l, photo_r, d_dr, map, d_reasons, d_counts, w, h, post->border,
+             post->correlation_window / 2, post->lr_threshold, post->correlation, channels};
   gate_kernel<<<grid, 256, 0, st>>>(g);
   const int minimum = post->speckle_size;
   speckle_init_kernel<<<grid, 256, 0, st>>>(map, n, d_parent, d_size);
@@ -381,4 +404,22 @@ extern "C" int csgm_postfilter(csgm_session* s, const csgm_post* post, const uin
     stats->valid += (int64_t)host.valid;
   }
   return CSGM_OK;
+}
+
+extern "C" int csgm_postfilter(csgm_session* s, const csgm_post* post, const uint8_t* left,
+                               const uint8_t* right, const float* disp_r, int32_t w, int32_t h,
+                               float* checked, uint8_t* reasons, csgm_stats* stats) {
+  return postfilter_impl(s, post, left, right, nullptr, nullptr, disp_r, w, h, checked, reasons,
+                         stats);
+}
+
+extern "C" int csgm_postfilter_color(csgm_session* s, const csgm_post* post, const uint8_t* left,
+                                     const uint8_t* right, const uint8_t* left_bgr,
+                                     const uint8_t* right_bgr, const float* disp_r, int32_t w,
+                                     int32_t h, float* checked, uint8_t* reasons,
+                                     csgm_stats* stats) {
+  if (!left_bgr || !right_bgr)
+    return fail(CSGM_E_INVALID, "Color-distance census requires interleaved BGR inputs");
+  return postfilter_impl(s, post, left, right, left_bgr, right_bgr, disp_r, w, h, checked,
+                         reasons, stats);
 }

@@ -117,6 +117,10 @@ __device__ __forceinline__ int cell_cost(const CostArgs& a, int64_t p, int64_t q
 
 
 cudaError_t launch_census_texture(const CensusArgs& a, int images, cudaStream_t stream);
+// CensusSgm.colorCensus of an interleaved BGR image (color_census.cu), texture ANDed with valid.
+cudaError_t launch_color_census(const uint8_t* bgr, const uint8_t* valid, int w, int h, int wx,
+                                int wy, uint64_t* desc, uint8_t* tex, int sm_count,
+                                cudaStream_t stream);
 cudaError_t launch_cost_volume(const CostArgs& a, int sm_count, cudaStream_t stream);
 cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int sm_count,
                               cudaStream_t stream);

@@ -217,8 +217,11 @@ class GpuSgm:
         return (out, rec) if summary else out
 
     def pair(self, params: CsgmParams, left, right, w: int, h: int, validLeft=None,
-             validRight=None, want_views: bool = False, want_reasons: bool = False) -> Result:
-        """Census, both views and the LR check on the GPU (CensusSgm.computeRecorded :56-201)."""
+             validRight=None, want_views: bool = False, want_reasons: bool = False,
+             leftBgr=None, rightBgr=None) -> Result:
+        """Census, both views and the LR check on the GPU (CensusSgm.computeRecorded :56-201);
+        with the interleaved BGR images, the colour-distance census (--census-mode
+        color-distance, :108-120)."""
         n = w * h
         left, right = _u8(left, n), _u8(right, n)
         validLeft, validRight = _u8(validLeft, n), _u8(validRight, n)
@@ -230,9 +233,20 @@ class GpuSgm:
         reasons = np.empty(n, np.uint8) if want_reasons else None
         boundary = np.empty(n, np.uint8) if want_reasons else None
         cstats = CsgmStats()
-        check(self.lib.csgm_pair(self.handle, ctypes.byref(params), _ptr(left), _ptr(right),
-                                 _ptr(validLeft), _ptr(validRight), w, h, _ptr(checked), _ptr(dl),
-                                 _ptr(dr), _ptr(reasons), _ptr(boundary), ctypes.byref(cstats)))
+        if leftBgr is not None or rightBgr is not None:
+            if leftBgr is None or rightBgr is None:
+                raise ValueError("Color-distance census requires interleaved BGR inputs")
+            lb, rb = _u8(leftBgr, 3 * n), _u8(rightBgr, 3 * n)
+            check(self.lib.csgm_pair_color(self.handle, ctypes.byref(params), _ptr(left),
+                                           _ptr(right), _ptr(lb), _ptr(rb), _ptr(validLeft),
+                                           _ptr(validRight), w, h, _ptr(checked), _ptr(dl),
+                                           _ptr(dr), _ptr(reasons), _ptr(boundary),
+                                           ctypes.byref(cstats)))
+        else:
+            check(self.lib.csgm_pair(self.handle, ctypes.byref(params), _ptr(left), _ptr(right),
+                                     _ptr(validLeft), _ptr(validRight), w, h, _ptr(checked),
+                                     _ptr(dl), _ptr(dr), _ptr(reasons), _ptr(boundary),
+                                     ctypes.byref(cstats)))
         return Result(w, h, checked, Stats.from_c(cstats), dl, dr, reasons, boundary)
 
     def color_census(self, bgr, w: int, h: int, window_x: int, window_y: int):
@@ -250,11 +264,11 @@ class GpuSgm:
         return desc, tex
 
     def postfilter(self, post: CsgmPost, left, right, disp_r, w: int, h: int, checked,
-                   reasons=None, stats: CsgmStats | None = None):
+                   reasons=None, stats: CsgmStats | None = None, leftBgr=None, rightBgr=None):
         """The post-filters of CensusSgm.computeRecorded (:203-272) on the GPU: median,
         post-median reciprocity, photometric gate, speckles.  `checked` (float32) and `reasons`
         (uint8) are numpy arrays updated in place; `stats` (CsgmStats) is updated like the
-        reference's Stats."""
+        reference's Stats.  With the BGR images the gate correlates their three channels."""
         n = w * h
         left, right = _u8(left, n), _u8(right, n)
         disp_r = np.ascontiguousarray(disp_r, np.float32)
@@ -265,9 +279,18 @@ class GpuSgm:
             raise ValueError("reasons must be a contiguous uint8 array of w*h values")
         if disp_r.size != n:
             raise ValueError("disp_r must hold w*h values")
-        check(self.lib.csgm_postfilter(self.handle, ctypes.byref(post), _ptr(left), _ptr(right),
-                                       _ptr(disp_r), w, h, _ptr(checked), _ptr(reasons),
-                                       ctypes.byref(stats) if stats is not None else None))
+        st = ctypes.byref(stats) if stats is not None else None
+        if leftBgr is not None or rightBgr is not None:
+            if leftBgr is None or rightBgr is None:
+                raise ValueError("Color-distance census requires interleaved BGR inputs")
+            lb, rb = _u8(leftBgr, 3 * n), _u8(rightBgr, 3 * n)
+            check(self.lib.csgm_postfilter_color(self.handle, ctypes.byref(post), _ptr(left),
+                                                 _ptr(right), _ptr(lb), _ptr(rb), _ptr(disp_r),
+                                                 w, h, _ptr(checked), _ptr(reasons), st))
+        else:
+            check(self.lib.csgm_postfilter(self.handle, ctypes.byref(post), _ptr(left),
+                                           _ptr(right), _ptr(disp_r), w, h, _ptr(checked),
+                                           _ptr(reasons), st))
         return checked
 
 
@@ -302,27 +325,38 @@ class CensusSgm:
     def params(self) -> CsgmParams:
         return params_from_options(self.options)
 
+    def _bgr(self, leftBgr, rightBgr):
+        """The BGR images of --census-mode color-distance (CensusSgm.java:108-115)."""
+        if self.options.censusMode != "color-distance":
+            return None, None
+        if leftBgr is None or rightBgr is None:
+            raise ValueError("Color-distance census requires interleaved BGR inputs")
+        return leftBgr, rightBgr
+
     def match_pair(self, left, right, width: int, height: int, validLeft=None, validRight=None,
-                   want_views=False, want_reasons=False) -> Result:
+                   want_views=False, want_reasons=False, leftBgr=None, rightBgr=None) -> Result:
         """The matcher up to the LR check (CensusSgm.java:56-201)."""
         o = self.options
         if width < o.window_x + 2 or height < o.window_y + 2:
             raise ValueError("Invalid stereo image dimensions")
-        if o.censusMode != "gray":
-            raise NotImplementedError("color-distance census is not on the GPU path yet")
+        lb, rb = self._bgr(leftBgr, rightBgr)
         return self.session.pair(self.params(), left, right, width, height, validLeft,
-                                 validRight, want_views, want_reasons)
+                                 validRight, want_views, want_reasons, leftBgr=lb, rightBgr=rb)
 
     def compute(self, left, right, width: int, height: int, validLeft=None, validRight=None,
-                want_reasons=False) -> Result:
+                want_reasons=False, leftBgr=None, rightBgr=None) -> Result:
         """CensusSgm.computeRecorded (CensusSgm.java:56-272): the matcher and the LR check, then
         the median, post-median reciprocity, photometric gate and speckle removal, with the
-        Stats counters of both stages."""
+        Stats counters of both stages (colour-distance mode: BGR descriptors and a three-channel
+        gate)."""
+        lb, rb = self._bgr(leftBgr, rightBgr)
         res = self.match_pair(left, right, width, height, validLeft, validRight,
-                              want_views=True, want_reasons=want_reasons)
+                              want_views=True, want_reasons=want_reasons, leftBgr=lb,
+                              rightBgr=rb)
         cstats = res.stats.to_c()
         self.session.postfilter(post_settings(self.options), left, right, res.right, width,
-                                height, res.disparity, res.reasons, cstats)
+                                height, res.disparity, res.reasons, cstats, leftBgr=lb,
+                                rightBgr=rb)
         res.stats = Stats.from_c(cstats)
         return res
 

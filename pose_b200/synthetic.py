@@ -104,6 +104,41 @@ def make_pair(spec: PairSpec):
             d.astype(np.float32).reshape(-1))
 
 
+def make_color_pair(spec: PairSpec):
+    """A rectified colour pair for --census-mode color-distance: three independently textured
+    channels, warped by one disparity field as in make_pair, interleaved BGR, with the gray images
+    the matcher's costs and penalties read ((29 B + 150 G + 77 R + 128) >> 8).  Returns
+    (left gray, right gray, left BGR uint8[h*w*3], right BGR, disparity float32[h*w])."""
+    rng = np.random.default_rng(spec.seed)
+    h, w = spec.height, spec.width
+    left = np.stack([_texture(rng, h, w, spec.blur_sigma) for _ in range(3)], axis=-1)
+    d = disparity_field(spec, rng)
+    xs = np.arange(w)[None, :].repeat(h, 0)
+    target = np.rint(xs - d).astype(np.int64)
+    ok = (target >= 0) & (target < w)
+    rows = np.arange(h)[:, None].repeat(w, 1)
+    key = np.full(h * w, -1, np.int64)
+    dq = np.rint(d * 256).astype(np.int64)
+    flat = (rows * w + np.clip(target, 0, w - 1))[ok]
+    np.maximum.at(key, flat, (dq << 13 | xs)[ok])
+    hit = key >= 0
+    src = (np.arange(h * w) // w) * w + (key & 8191)
+    right = np.stack([_texture(rng, h, w, spec.blur_sigma) for _ in range(3)], axis=-1)
+    right = right.reshape(-1, 3)
+    right[hit] = left.reshape(-1, 3)[src[hit]]
+    right = right.reshape(h, w, 3)
+    left = np.clip(np.rint(left + rng.normal(0, spec.sensor_sigma, size=left.shape)), 0, 255)
+    right = np.clip(np.rint(right + rng.normal(0, spec.sensor_sigma, size=right.shape)), 0, 255)
+    left, right = left.astype(np.uint8), right.astype(np.uint8)
+
+    def gray(bgr):
+        b, g, r = (bgr[..., i].astype(np.int32) for i in range(3))
+        return ((29 * b + 150 * g + 77 * r + 128) >> 8).astype(np.uint8).reshape(-1)
+
+    return (gray(left), gray(right), left.reshape(-1), right.reshape(-1),
+            d.astype(np.float32).reshape(-1))
+
+
 def spec_for(name: str, seed_offset: int = 0) -> PairSpec:
     base = {"cfg0": CFG0, "cfg1": CFG1, "cfg2": CFG2}[name]
     return PairSpec(**{**base.__dict__, "seed": base.seed + seed_offset})

@@ -73,28 +73,30 @@ def reciprocal(right, w, h, x, y, d, tolerance, border):
     return math.isfinite(other) and abs(_fsub(d, other)) <= tolerance
 
 
-def zncc(a, b, w, h, x, y, d, r):
+def zncc(a, b, w, h, x, y, d, r, channels=1):
     target = x - float(d)
     bx = math.floor(target)
     fraction = target - bx
     if x - r < 0 or x + r >= w or y - r < 0 or y + r >= h or bx - r < 0 or bx + r + 1 >= w:
         return -1.0
     n = (2 * r + 1) * (2 * r + 1)
-    sa = sb = saa = sbb = sab = 0.0
-    for dy in range(-r, r + 1):
-        for dx in range(-r, r + 1):
-            av = float(a[(y + dy) * w + x + dx])
-            bi = (y + dy) * w + bx + dx
-            bv = (1 - fraction) * float(b[bi]) + fraction * float(b[bi + 1])
-            sa += av
-            sb += bv
-            saa += av * av
-            sbb += bv * bv
-            sab += av * bv
-    covariance = 0.0 + (sab - sa * sb / n)
-    var_a = 0.0 + (saa - sa * sa / n)
-    var_b = 0.0 + (sbb - sb * sb / n)
-    if var_a < n * 4 or var_b < n * 4:
+    covariance = var_a = var_b = 0.0
+    for channel in range(channels):
+        sa = sb = saa = sbb = sab = 0.0
+        for dy in range(-r, r + 1):
+            for dx in range(-r, r + 1):
+                av = float(a[((y + dy) * w + x + dx) * channels + channel])
+                bi = ((y + dy) * w + bx + dx) * channels + channel
+                bv = (1 - fraction) * float(b[bi]) + fraction * float(b[bi + channels])
+                sa += av
+                sb += bv
+                saa += av * av
+                sbb += bv * bv
+                sab += av * bv
+        covariance += sab - sa * sb / n
+        var_a += saa - sa * sa / n
+        var_b += sbb - sb * sb / n
+    if var_a < channels * n * 4 or var_b < channels * n * 4:
         return -1.0
     product = var_a * var_b
     return covariance / math.sqrt(product if product > 1e-12 else 1e-12)
@@ -133,10 +135,12 @@ def remove_speckles(a, w, h, minimum, rng, connectivity):
     return rejected
 
 
-def postfilter(post, left, right, dr, w, h, checked, counts, reasons):
+def postfilter(post, left, right, dr, w, h, checked, counts, reasons, left_bgr=None,
+               right_bgr=None):
     """In place on checked (float32) and reasons (uint8); counts is a dict with the four
     counters (postMedianLrRejected and photometricRejected added to, speckleRejected set, valid
-    added to)."""
+    added to).  With the BGR images the gate correlates their three channels."""
+    photo_l, photo_r, channels = (left, right, 1) if left_bgr is None else (left_bgr, right_bgr, 3)
     if post["median"] > 1:
         filtered = (median_valid(checked, w, h, post["median"]) if post["classic"] else
                     median_edge_preserving(checked, w, h, post["median"], post["max_change"], left,
@@ -153,7 +157,8 @@ def postfilter(post, left, right, dr, w, h, checked, counts, reasons):
                 counts["postMedianLrRejected"] += 1
                 reasons[p] = 5
                 continue
-            if zncc(left, right, w, h, x, y, d, post["window"] // 2) < post["correlation"]:
+            if zncc(photo_l, photo_r, w, h, x, y, d, post["window"] // 2,
+                    channels) < post["correlation"]:
                 checked[p] = np.nan
                 counts["photometricRejected"] += 1
                 reasons[p] = 6

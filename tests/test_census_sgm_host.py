@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes
 
 import numpy as np
+import pytest
 
 import oracle.oracle as orc
 from pose_b200.options import Options
@@ -25,16 +26,19 @@ class OracleSession:
         self.streaming = (mode, strip_rows)
 
     def pair(self, params, left, right, w, h, validLeft=None, validRight=None, want_views=False,
-             want_reasons=False):
-        r = orc.pair(params, left, right, w, h, validLeft, validRight, want_reasons=True)
+             want_reasons=False, leftBgr=None, rightBgr=None):
+        r = orc.pair(params, left, right, w, h, validLeft, validRight, want_reasons=True,
+                     left_bgr=leftBgr, right_bgr=rightBgr)
         return Result(w, h, r["checked"], Stats.from_c(r["stats"]), r["dl"], r["dr"],
                       r["reasons"] if want_reasons else None,
                       r["boundary"] if want_reasons else None)
 
-    def postfilter(self, post, left, right, disp_r, w, h, checked, reasons=None, stats=None):
+    def postfilter(self, post, left, right, disp_r, w, h, checked, reasons=None, stats=None,
+                   leftBgr=None, rightBgr=None):
         opost = orc.OraclePost()
         ctypes.memmove(ctypes.byref(opost), ctypes.byref(post), ctypes.sizeof(opost))
-        orc.postfilter(opost, left, right, disp_r, w, h, checked, stats, reasons)
+        orc.postfilter(opost, left, right, disp_r, w, h, checked, stats, reasons,
+                       left_bgr=leftBgr, right_bgr=rightBgr)
         return checked
 
 
@@ -58,3 +62,29 @@ def test_compute_equals_compute_recorded(oracle_lib):
     assert np.array_equal(got.reasons, want_res["reasons"])
     for c_name, name in Stats._C_NAMES.items():
         assert getattr(got.stats, name) == getattr(want_stats, c_name), name
+
+
+def test_color_mode_routes_bgr_images(oracle_lib):
+    """--census-mode color-distance: CensusSgm.compute hands the BGR images to the pair and to
+    the post-filters (CensusSgm.java:108-120,222-224) and refuses to run without them."""
+    from pose_b200.synthetic import make_color_pair
+
+    w, h = 64, 40
+    left, right, lbgr, rbgr, _ = make_color_pair(PairSpec(w, h, planes=2, d_min=3, d_max=12,
+                                                          seed=5))
+    o = Options()
+    o.census, o.disparities, o.censusMode = 5, 16, "color-distance"
+    sgm = CensusSgm(o, session=OracleSession())
+    with pytest.raises(ValueError):
+        sgm.compute(left, right, w, h)
+    got = sgm.compute(left, right, w, h, leftBgr=lbgr, rightBgr=rbgr)
+    prm = sgm.params()
+    want = orc.pair(prm, left, right, w, h, want_reasons=True, left_bgr=lbgr, right_bgr=rbgr)
+    checked, st = want["checked"].copy(), want["stats"]
+    post = orc.OraclePost()
+    ctypes.memmove(ctypes.byref(post), ctypes.byref(post_settings(o)), ctypes.sizeof(post))
+    orc.postfilter(post, left, right, want["dr"], w, h, checked, st, left_bgr=lbgr,
+                   right_bgr=rbgr)
+    assert np.array_equal(got.disparity.view(np.uint32), checked.view(np.uint32))
+    assert got.stats.photometricRejected == st.photometric_rejected
+

@@ -131,6 +131,73 @@ def test_postfilter_restatement_bit_exact(oracle_lib, case):
     assert (np.isfinite(res["checked"]) & ~np.isfinite(want)).any(), case
 
 
+@pytest.mark.parametrize("case", ["edge", "classic", "gate_off"])
+def test_color_postfilter_restatement_bit_exact(oracle_lib, case):
+    """--census-mode color-distance: the oracle's post-filters with the three-channel photometric
+    gate on the BGR images (CensusSgm.java:222-224,240-250) equal the restatement bit for bit,
+    on the oracle's own colour-census pair."""
+    import postfilter_restatement as pr
+    from pose_b200.synthetic import PairSpec, make_color_pair
+    from reference_cpu import post_from_options
+
+    orc = oracle_lib
+    w, h = 72, 54
+    left, right, lbgr, rbgr, _ = make_color_pair(PairSpec(w, h, planes=3, d_min=3, d_max=14,
+                                                          seed=17))
+    o = Options()
+    o.census, o.disparities = 5, 16
+    o.correlation = 0.55 if case != "gate_off" else -1.0
+    if case == "classic":
+        o.medianMode = "classic"
+    res = orc.pair(params_from_options(o), left, right, w, h, want_reasons=True, left_bgr=lbgr,
+                   right_bgr=rbgr)
+    post = post_from_options(o)
+    want, want_reasons, stats = res["checked"].copy(), res["reasons"].copy(), res["stats"]
+    base = (stats.post_median_lr_rejected, stats.photometric_rejected, stats.valid)
+    orc.postfilter(post, left, right, res["dr"], w, h, want, stats, want_reasons,
+                   left_bgr=lbgr, right_bgr=rbgr)
+    mine, mine_reasons = res["checked"].copy(), res["reasons"].copy()
+    counts = {"postMedianLrRejected": base[0], "photometricRejected": base[1],
+              "speckleRejected": 0, "valid": base[2]}
+    settings = {"median": o.median, "classic": o.medianMode == "classic",
+                "max_change": o.medianMaxChange, "edge": o.medianEdgeThreshold,
+                "lr": o.lrThreshold, "border": o.census // 2, "window": o.correlationWindow,
+                "correlation": o.correlation, "speckle": o.speckleSize, "range": o.speckleRange,
+                "connectivity": o.speckleConnectivity}
+    pr.postfilter(settings, left, right, res["dr"], w, h, mine, counts, mine_reasons,
+                  left_bgr=lbgr, right_bgr=rbgr)
+    assert np.array_equal(mine.view(np.uint32), want.view(np.uint32)), case
+    assert np.array_equal(mine_reasons, want_reasons), case
+    assert counts["photometricRejected"] == stats.photometric_rejected
+    assert counts["valid"] == stats.valid
+    if case != "gate_off":
+        assert stats.photometric_rejected > base[1], "the colour gate rejected nothing"
+
+
+def test_color_pair_is_the_composition(oracle_lib):
+    """oracle_pair_color = colour census of both images + CensusSgm.match of both views + LR."""
+    from pose_b200.synthetic import PairSpec, make_color_pair
+
+    orc = oracle_lib
+    w, h = 64, 40
+    left, right, lbgr, rbgr, _ = make_color_pair(PairSpec(w, h, planes=2, d_min=3, d_max=12,
+                                                          seed=5))
+    o = Options()
+    o.census, o.disparities = 5, 16
+    prm = params_from_options(o)
+    res = orc.pair(prm, left, right, w, h, want_reasons=True, left_bgr=lbgr, right_bgr=rbgr)
+    da, ta = orc.color_census(lbgr, w, h, 5, 5)
+    db, tb = orc.color_census(rbgr, w, h, 5, 5)
+    dl = orc.match(prm, da, db, left, right, ta, tb, w, h, 0)["disp"]
+    dr = orc.match(prm, db, da, right, left, tb, ta, w, h, 1)["disp"]
+    checked, _ = orc.lr_check(dl, dr, w, h, 2, 2, prm.lr_threshold)
+    assert np.array_equal(res["dl"].view(np.uint32), dl.view(np.uint32))
+    assert np.array_equal(res["dr"].view(np.uint32), dr.view(np.uint32))
+    assert np.array_equal(res["checked"].view(np.uint32), checked.view(np.uint32))
+    gray = orc.pair(prm, left, right, w, h)
+    assert not np.array_equal(gray["dl"].view(np.uint32), dl.view(np.uint32))
+
+
 @pytest.mark.parametrize("wx,wy", [(3, 3), (5, 5), (9, 7), (11, 11)])
 def test_color_census_restatement_bit_exact(oracle_lib, wx, wy):
     """oracle_color_census equals the Python restatement of CensusSgm.colorCensus."""
