@@ -188,6 +188,42 @@ int csgm_plan_detail(csgm_session* session, const csgm_params* params, int32_t w
 int csgm_disparity_limit(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
                          int32_t* limit);
 
+/*
+ * Launch shape of the fused sweep, picked per shape bucket by an autotuner (no counterpart in the
+ * reference, whose OpenCL work-group size is a device property, src/main/java/sgm/GpuSgm.java:163-221).
+ * Buckets: disparities rounded up to 64, paths, width and height in half-octaves.  Tuning never
+ * changes results.
+ */
+typedef struct csgm_tuning {
+  int32_t rows_per_block;  /* row warps per sweep CTA: 4, 8 (12 at 65..128 disparities) */
+  int32_t line_warps;      /* warps per sweep CTA walking the anti-diagonal lines: 0, 4, 8 */
+  int32_t line_slack;      /* percent of a block's remaining pixels a line may take: 10..1000 */
+  int32_t disparity_lanes; /* disparities per lane and register half (fixed: padded D / 32) */
+  double milliseconds;     /* measured pair time of this shape (0 when not measured) */
+} csgm_tuning;
+
+/* Times the candidate shapes on a synthetic w x h pair with these parameters, keeps the fastest
+ * for the bucket in the session and, when cache_path is not NULL, stores it in that cache file
+ * (text, one entry per line; other entries are kept).  CSGM_E_UNSUPPORTED when the fused kernels
+ * do not run the parameters.  best (optional) receives the chosen shape and its time. */
+int csgm_autotune(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
+                  const char* cache_path, csgm_tuning* best);
+
+/* Adds the entries of a tuning cache file to the session (a missing file adds nothing). */
+int csgm_session_load_tuning(csgm_session* session, const char* cache_path);
+
+/* Forces one shape for every call of the session (NULL: back to the tuned / default shapes). */
+int csgm_session_set_tuning(csgm_session* session, const csgm_tuning* tuning);
+
+/* The shape a call with these parameters and size would use now. */
+int csgm_tuning_get(csgm_session* session, const csgm_params* params, int32_t w, int32_t h,
+                    csgm_tuning* out);
+
+/* The cache file's entry for these parameters and size, without a session or device;
+ * out->rows_per_block is 0 when the file has none. */
+int csgm_tuning_cache_lookup(const char* cache_path, const csgm_params* params, int32_t w,
+                             int32_t h, csgm_tuning* out);
+
 /* Accumulated device timing since the last reset (reset != 0 clears it afterwards). */
 int csgm_profile_get(csgm_session* session, csgm_profile* out, int32_t reset);
 

@@ -127,6 +127,16 @@ class CsgmKernelTime(ctypes.Structure):
     ]
 
 
+class CsgmTuning(ctypes.Structure):
+    _fields_ = [
+        ("rows_per_block", ctypes.c_int32),
+        ("line_warps", ctypes.c_int32),
+        ("line_slack", ctypes.c_int32),
+        ("disparity_lanes", ctypes.c_int32),
+        ("milliseconds", ctypes.c_double),
+    ]
+
+
 class CsgmError(RuntimeError):
     """A non-zero status from the C ABI, with the library's thread-local message."""
 
@@ -177,6 +187,20 @@ SIGNATURES = {
         [_P, ctypes.POINTER(CsgmKernelTime), _I32, ctypes.POINTER(_I32), _I32],
     ),
     "csgm_session_synchronize": (ctypes.c_int, [_P]),
+    "csgm_autotune": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.c_char_p, ctypes.POINTER(CsgmTuning)],
+    ),
+    "csgm_session_load_tuning": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "csgm_session_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(CsgmTuning)]),
+    "csgm_tuning_get": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(CsgmTuning)],
+    ),
+    "csgm_tuning_cache_lookup": (
+        ctypes.c_int,
+        [ctypes.c_char_p, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(CsgmTuning)],
+    ),
     "csgm_session_set_wait_limit": (ctypes.c_int, [_P, _I64]),
     "csgm_pair_device": (
         ctypes.c_int,

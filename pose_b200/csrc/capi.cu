@@ -149,6 +149,17 @@ using namespace csgm;
 
 namespace csgm {
 
+void session_settings(Context& ctx, csgm_session* s, const csgm_params& p, int w, int h) {
+  ctx.wait_limit = s->wait_limit;
+  ctx.sgm_mode = s->sgm_mode;
+  ctx.strip_rows = s->strip_rows;
+  ctx.host_partial = &s->host_partial;
+  if (s->tuning_forced)
+    ctx.tuning = s->forced_tuning;
+  else if (const TuningTable::Entry* e = s->tuning.find(p, w, h))
+    ctx.tuning = e->t;
+}
+
 int validate_params(const csgm_params* p, int w, int h) {
   if (!p) return fail(CSGM_E_INVALID, "params is NULL");
   if (p->disparities < 3 || p->disparities > 4096)
@@ -356,12 +367,10 @@ int csgm_kernel_times(csgm_session* s, csgm_kernel_time* out, int32_t capacity, 
   return CSGM_OK;
 }
 
-// A context with the session's budget and streaming settings, for planning only.
-static Context planning_context(csgm_session* s) {
+// A context with the session's budget, streaming and tuning settings, for planning only.
+static Context planning_context(csgm_session* s, const csgm_params& p, int w, int h) {
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
-  ctx.sgm_mode = s->sgm_mode;
-  ctx.strip_rows = s->strip_rows;
-  ctx.host_partial = &s->host_partial;
+  session_settings(ctx, s, p, w, h);
   return ctx;
 }
 
@@ -372,7 +381,7 @@ int csgm_plan_detail(csgm_session* s, const csgm_params* p, int32_t w, int32_t h
   if (rc) return rc;
   std::lock_guard<std::mutex> guard(s->lock);
   ViewPlan plan;
-  rc = plan_pair(planning_context(s), *p, w, h, true, &plan);
+  rc = plan_pair(planning_context(s, *p, w, h), *p, w, h, true, &plan);
   if (rc) return rc;
   if (strip_rows) *strip_rows = plan.rows;
   if (device_bytes) *device_bytes = (int64_t)plan.device_bytes;
@@ -390,14 +399,14 @@ int csgm_disparity_limit(csgm_session* s, const csgm_params* p, int32_t w, int32
   // GpuStereo.limit (GpuStereo.java:86-94): binary search over the plan.
   if (!s || !p || !limit) return fail(CSGM_E_INVALID, "NULL argument");
   std::lock_guard<std::mutex> guard(s->lock);
-  const Context ctx = planning_context(s);
   int low = 2, high = 4096;
   while (low < high) {
     int mid = (low + high + 1) / 2;
     csgm_params q = *p;
     q.disparities = mid;
     ViewPlan plan;
-    bool fits = validate_params(&q, w, h) == CSGM_OK && plan_pair(ctx, q, w, h, true, &plan) == 0;
+    bool fits = validate_params(&q, w, h) == CSGM_OK &&
+                plan_pair(planning_context(s, q, w, h), q, w, h, true, &plan) == 0;
     if (fits)
       low = mid;
     else
@@ -422,10 +431,7 @@ int csgm_match(csgm_session* s, const csgm_params* p, const uint64_t* desc_a,
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
-  ctx.wait_limit = s->wait_limit;
-  ctx.sgm_mode = s->sgm_mode;
-  ctx.strip_rows = s->strip_rows;
-  ctx.host_partial = &s->host_partial;
+  session_settings(ctx, s, *p, w, h);
   ctx.twin = &s->twin;
   return run_match_host(ctx, *p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                         out_disp, out_summary, reasons, boundary, stats);
@@ -445,10 +451,7 @@ int csgm_pair(csgm_session* s, const csgm_params* p, const uint8_t* left, const 
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
-  ctx.wait_limit = s->wait_limit;
-  ctx.sgm_mode = s->sgm_mode;
-  ctx.strip_rows = s->strip_rows;
-  ctx.host_partial = &s->host_partial;
+  session_settings(ctx, s, *p, w, h);
   return run_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                        reasons, boundary, stats);
 }
@@ -470,10 +473,7 @@ int csgm_pair_color(csgm_session* s, const csgm_params* p, const uint8_t* left,
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
-  ctx.wait_limit = s->wait_limit;
-  ctx.sgm_mode = s->sgm_mode;
-  ctx.strip_rows = s->strip_rows;
-  ctx.host_partial = &s->host_partial;
+  session_settings(ctx, s, *p, w, h);
   return run_pair_host(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                        reasons, boundary, stats, left_bgr, right_bgr);
 }
@@ -493,10 +493,7 @@ int csgm_pair_device(csgm_session* s, const csgm_params* p, const uint8_t* left,
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
-  ctx.wait_limit = s->wait_limit;
-  ctx.sgm_mode = s->sgm_mode;
-  ctx.strip_rows = s->strip_rows;
-  ctx.host_partial = &s->host_partial;
+  session_settings(ctx, s, *p, w, h);
   return run_pair_device(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                          reasons, boundary, stats, sync != 0);
 }

@@ -44,11 +44,12 @@ static size_t pair_fixed_bytes(const csgm_params& p, int w, int h, bool host_inp
   return bytes;
 }
 
-size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs, bool color) {
+size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs, bool color,
+                            const SweepTuning& tuning) {
   size_t n = (size_t)w * h, D = (size_t)p.disparities;
   size_t bytes = pair_fixed_bytes(p, w, h, host_inputs, color);
   if (use_fused(p))
-    bytes += fused_workspace_bytes(p, w, h);
+    bytes += fused_workspace_bytes(p, w, h, tuning);
   else
     bytes += n * D * 2 + n * D * p.aggregate_bytes;  // one cost volume + one aggregate
   return bytes;
@@ -105,7 +106,7 @@ static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, s
 int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
               ViewPlan* plan, bool color) {
   return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs, color),
-                     pair_workspace_bytes(p, w, h, host_inputs, color), plan);
+                     pair_workspace_bytes(p, w, h, host_inputs, color, ctx.tuning), plan);
 }
 
 void* HostBuffer::get(size_t want, int* status) {
@@ -510,10 +511,11 @@ int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const
 }
 
 // Device bytes of csgm_match on the fused kernels (summary: winners records requested).
-static size_t match_fused_bytes(const csgm_params& p, int w, int h, bool summary) {
+static size_t match_fused_bytes(const csgm_params& p, int w, int h, bool summary,
+                                const SweepTuning& tuning) {
   const size_t n = (size_t)w * h, words = (size_t)words_of(p);
   const size_t inputs = 2 * n * words * 8 + 4 * n;  // one set: descriptors, grays, masks
-  return fused_workspace_bytes(p, w, h) + 2 * inputs +
+  return fused_workspace_bytes(p, w, h, tuning) + 2 * inputs +
          2 * (4 * n + 2 * n + (summary ? 24 * n : 0) + sizeof(DeviceStats)) + 16 * 256;
 }
 
@@ -752,7 +754,7 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
   // resident on the general ones, else streamed (as the session's mode allows).
   const bool summary = out_summary != nullptr;
   if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && use_fused(p) && h <= 65535 &&
-      match_fused_bytes(p, w, h, summary) <= ctx.ws->budget)
+      match_fused_bytes(p, w, h, summary, ctx.tuning) <= ctx.ws->budget)
     return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                            out_disp, out_summary, reasons, boundary, stats);
   if (ctx.twin) ctx.twin->valid = false;

@@ -13,6 +13,7 @@
 
 namespace csgm {
 
+struct Context;
 int fail(int status, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 int validate_params(const csgm_params* p, int w, int h);
@@ -35,6 +36,27 @@ struct HostBuffer {
   size_t bytes = 0;
   void* get(size_t want, int* status);
   void release();
+};
+
+// Launch shape of the fused sweep (the autotuner's knobs).  0 / -1 fields: the default.
+struct SweepTuning {
+  int rows = 0;         // rows per sweep CTA (row warps)
+  int line_warps = -1;  // line warps per sweep CTA walking the anti-diagonal lines
+  int line_slack = 0;   // percent of a block's remaining pixels a line may take
+};
+
+// Autotuned launch shapes per shape bucket (padded D, paths, half-octave width and height),
+// filled by csgm_autotune and loaded from its cache file.
+struct TuningTable {
+  struct Entry {
+    int dp, paths, wb, hb;
+    SweepTuning t;
+    double ms;
+  };
+  std::vector<Entry> entries;
+  static int bucket(int v);
+  const Entry* find(const csgm_params& p, int w, int h) const;
+  void put(const csgm_params& p, int w, int h, const SweepTuning& t, double ms);
 };
 
 // How a pair's views run: resident (the whole volume in device memory: the fused kernels where
@@ -125,6 +147,8 @@ struct Context {
   int sgm_mode = CSGM_SGM_AUTO;
   int strip_rows = 64;
   HostBuffer* host_partial = nullptr;  // null: streaming unavailable (batch slots)
+  // Launch shape of the fused sweep for this call (from the session's tuning table).
+  SweepTuning tuning;
 };
 
 // One batch slot: a pair in flight with its own stream and resident workspace.
@@ -145,7 +169,7 @@ struct BatchSlot {
 // Bytes of device workspace a pair needs (host_inputs: include the upload/download staging;
 // color: the two interleaved BGR images of --census-mode color-distance).
 size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs,
-                            bool color = false);
+                            bool color = false, const SweepTuning& tuning = SweepTuning{});
 
 // The plan of a pair (GpuStereo.plan, GpuStereo.java:33-84) under the context's budget, mode and
 // strip height; CSGM_E_NOMEM when no plan fits.
@@ -202,8 +226,17 @@ struct csgm_session {
   int sgm_mode = CSGM_SGM_AUTO;  // csgm_session_set_streaming
   int strip_rows = 64;
   csgm::HostBuffer host_partial;
+  csgm::TuningTable tuning;  // csgm_autotune / csgm_session_load_tuning
+  bool tuning_forced = false;  // csgm_session_set_tuning
+  csgm::SweepTuning forced_tuning;
   // Batched / served pairs (batch.cu).
   std::vector<csgm::BatchSlot> slots;
   size_t batch_budget = 0;
   int64_t next_request = 1;
 };
+
+namespace csgm {
+// Copies the session's wait limit, streaming mode and (for these parameters and size) sweep
+// tuning into a call's context.
+void session_settings(Context& ctx, csgm_session* s, const csgm_params& p, int w, int h);
+}  // namespace csgm

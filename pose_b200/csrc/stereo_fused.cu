@@ -1736,13 +1736,14 @@ constexpr int kMaxSharedPerBlock = 227 * 1024;
 template <int REGS, int R>
 int sweep_smem_with_lines(int lw) { return SweepLayout<REGS, 3, kChunk, R>::with_lines(lw); }
 
-int line_warps_for(int regs, int rows) {
+// `requested` (0, 4 or 8; -1 = none) takes precedence over the environment and the default.
+int line_warps_for(int regs, int rows, int requested) {
   static const int forced = [] {
     const char* e = getenv("CSGM_SWEEP_LINE_WARPS");
     const int v = e ? atoi(e) : -1;
     return v == 0 || v == 4 || v == 8 ? v : -1;
   }();
-  int lw = forced >= 0 ? forced : kSweepLineWarps;
+  int lw = requested >= 0 ? requested : forced >= 0 ? forced : kSweepLineWarps;
   auto smem = [&](int l) {
     switch (regs * 16 + rows) {
       case 2 * 16 + 4: return sweep_smem_with_lines<2, 4>(l);
@@ -1799,9 +1800,9 @@ cudaError_t launch_sweep_for(const SweepArgs& a, cudaStream_t stream, bool exclu
 struct FusedLayout {
   size_t cost, sum, pen, info, carry, flags, total;
   int Dp, nb, vslot, rows;
-  FusedLayout(const csgm_params& p, int w, int h) {
+  FusedLayout(const csgm_params& p, int w, int h, int rows_per_block) {
     Dp = padded_d(p.disparities);
-    rows = rows_for(Dp / 32);
+    rows = rows_per_block;
     nb = (h + rows - 1) / rows;
     const int nv = p.directions >= 8 ? 2 : 1;
     vslot = nv * Dp * 4;
@@ -1833,15 +1834,29 @@ bool fused_supported(const csgm_params& p) {
   return true;
 }
 
-size_t fused_workspace_bytes(const csgm_params& p, int w, int h) {
-  return FusedLayout(p, w, h).total;
+SweepTuning resolve_tuning(const csgm_params& p, const SweepTuning& want) {
+  const int regs = padded_d(p.disparities) / 32;
+  SweepTuning t;
+  const int r = want.rows;
+  t.rows = r == 4 || r == 8 || (r == 12 && regs == 4) ? r : rows_for(regs);
+  const int lw = want.line_warps == 0 || want.line_warps == 4 || want.line_warps == 8
+                     ? want.line_warps
+                     : -1;
+  t.line_warps = p.directions >= 8 ? line_warps_for(regs, t.rows, lw) : 0;
+  t.line_slack = want.line_slack >= 10 && want.line_slack <= 1000 ? want.line_slack : line_slack();
+  return t;
+}
+
+size_t fused_workspace_bytes(const csgm_params& p, int w, int h, const SweepTuning& tuning) {
+  return FusedLayout(p, w, h, resolve_tuning(p, tuning).rows).total;
 }
 
 int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h,
                     int** error_flag) {
   int status = CSGM_OK;
   if (h > 65535) return fail(CSGM_E_UNSUPPORTED, "fused path: image taller than 65535 rows");
-  FusedLayout F(p, w, h);
+  const SweepTuning T = resolve_tuning(p, ctx.tuning);
+  FusedLayout F(p, w, h, T.rows);
   uint8_t* cost_l = (uint8_t*)ctx.ws->get(kCostL, F.cost, &status);
   if (!cost_l) return status;
   uint8_t* cost_r = (uint8_t*)ctx.ws->get(kCostR, F.cost, &status);
@@ -1914,7 +1929,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   // The anti-diagonal lines: inside the sweep's CTAs (line warps), or as their own kernel on the
   // pair's stream before the sweep (beside the sweep on a second stream they slowed it by more
   // than their own run time: 4.63 ms per pair against 4.47 ms one after the other).
-  const int line_warps = sum_lines && ctx.lines_in_sweep ? line_warps_for(regs, F.rows) : 0;
+  const int line_warps = sum_lines && ctx.lines_in_sweep ? T.line_warps : 0;
   LineArgs la{{cost_l, cost_r}, pen, sum_lines, w, h, p.disparities, p.p1,
               line_warps ? flags + 2 * F.nb + 2 : nullptr};
   auto run_lines = [&](cudaStream_t stream) {
@@ -1973,7 +1988,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
   a.p1 = p.p1;
   a.timeout = ctx.wait_limit > 0 ? ctx.wait_limit : kDefaultWaitLimit;
   a.line = la;
-  a.line_slack = line_slack();
+  a.line_slack = T.line_slack;
   const bool eight = p.directions >= 8;  // 16 paths: the 8-path sweep plus the knight lines
   // Batched pairs launch the sweep on a high-priority stream: its pending CTAs then take SMs ahead
   // of other pairs' bandwidth-bound kernels, so a pair's chain of row blocks is not held up.

@@ -25,7 +25,11 @@ struct FusedViews {
 };
 
 bool fused_supported(const csgm_params& p);
-size_t fused_workspace_bytes(const csgm_params& p, int w, int h);
+// The tuning a fused run uses: the requested values where valid for these parameters (rows per
+// block 4, 8, or 12 at 65..128 disparities; line warps 0, 4 or 8 within the shared memory of a
+// CTA, 8/16 paths only; line slack 10..1000), otherwise the environment's or the defaults.
+SweepTuning resolve_tuning(const csgm_params& p, const SweepTuning& requested);
+size_t fused_workspace_bytes(const csgm_params& p, int w, int h, const SweepTuning& tuning);
 // Queues both views on ctx.stream; *error_flag receives the device address of the sweep's error
 // word (non-zero after a bounded wait ran out).
 int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int w, int h,

@@ -182,6 +182,38 @@ class GpuSgm:
     def synchronize(self) -> None:
         check(self.lib.csgm_session_synchronize(self.handle))
 
+    # -- autotuned launch shapes ----------------------------------------------------------
+    @staticmethod
+    def _tuning_dict(t) -> dict:
+        return {"rows_per_block": t.rows_per_block, "line_warps": t.line_warps,
+                "line_slack": t.line_slack, "disparity_lanes": t.disparity_lanes,
+                "milliseconds": t.milliseconds}
+
+    def autotune(self, params: CsgmParams, w: int, h: int, cache_path: str | None = None) -> dict:
+        """Time the sweep's launch shapes on a synthetic w x h pair and keep the fastest."""
+        t = _abi.CsgmTuning()
+        path = cache_path.encode() if cache_path else None
+        check(self.lib.csgm_autotune(self.handle, ctypes.byref(params), w, h, path,
+                                     ctypes.byref(t)))
+        return self._tuning_dict(t)
+
+    def load_tuning(self, cache_path: str) -> None:
+        check(self.lib.csgm_session_load_tuning(self.handle, cache_path.encode()))
+
+    def set_tuning(self, tuning: dict | None) -> None:
+        """Force one launch shape for every call (None: the tuned / default shapes)."""
+        if tuning is None:
+            check(self.lib.csgm_session_set_tuning(self.handle, None))
+            return
+        t = _abi.CsgmTuning(tuning.get("rows_per_block", 0), tuning.get("line_warps", -1),
+                            tuning.get("line_slack", 0), 0, 0.0)
+        check(self.lib.csgm_session_set_tuning(self.handle, ctypes.byref(t)))
+
+    def tuning(self, params: CsgmParams, w: int, h: int) -> dict:
+        t = _abi.CsgmTuning()
+        check(self.lib.csgm_tuning_get(self.handle, ctypes.byref(params), w, h, ctypes.byref(t)))
+        return self._tuning_dict(t)
+
     def set_wait_limit(self, cycles: int) -> None:
         """Watchdog of the device-side waits in SM clock cycles (0 = the default, ~2 s); a wait
         that runs out makes the call fail with CSGM_E_TIMEOUT and leaves the session usable."""
