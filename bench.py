@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate (max)")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graphs", action="store_true",
+                    help="replay the device pipeline as a CUDA graph in the timed steps")
     ap.add_argument("--profile-pairs", type=int, default=0,
                     help="run this many pairs through GpuSgm.pair and exit (an ncu target)")
     ap.add_argument("--rows", type=int, default=0,
@@ -333,7 +335,10 @@ def run_ours(args):
         flush.zero_()
         torch.cuda.synchronize()
 
-    session.set_profiling(2)
+    # Per-kernel events cannot sit inside a graph: with --graphs the timed steps record one event
+    # pair around each replay (level 1) and the per-kernel split comes from untimed plain steps.
+    session.set_profiling(1 if args.graphs else 2)
+    session.set_graphs(args.graphs)
     for _ in range(args.warmup):
         flush_l2()
         step_device()
@@ -355,6 +360,16 @@ def run_ours(args):
     clock_info = clocks.stop()
     prof = session.profile(reset=True)
     kernels = session.kernel_times(reset=True)
+    graph_stats = session.graph_stats() if args.graphs else None
+    if args.graphs:
+        session.set_graphs(False)
+        session.set_profiling(2)
+        for _ in range(3):
+            flush_l2()
+            step_device()
+        torch.cuda.synchronize()
+        kernels = session.kernel_times(reset=True)
+        session.profile(reset=True)
     device_s = prof["kernel_ns"] / 1e9
     launches = int(prof["launches"])
     device_s = max_over_ranks(device_s, dist, f"cuda:{local}")
@@ -424,7 +439,9 @@ def run_ours(args):
                    "pairs_per_step_per_gpu": 1,
                    "l2": "flushed before every step (256 MiB memset, untimed)",
                    "parallelism": f"replicas x{world}", "wall_ms_per_step": round(
-                       wall / args.steps * 1e3, 4)},
+                       wall / args.steps * 1e3, 4),
+                   "cuda_graphs": ({"captured": graph_stats[0], "replayed": graph_stats[1]}
+                                   if graph_stats else False)},
         "e2e": {"value": round(e2e_value, 3), "unit": "Gcells/s", "h2d_bytes_per_step": 2 * n,
                 "d2h_bytes_per_step": 4 * n + ctypes.sizeof(CsgmStats)},
         "e2e_match": e2e_match,

@@ -243,6 +243,16 @@ int csgm_session_set_profiling(csgm_session* session, int32_t level);
 int csgm_kernel_times(csgm_session* session, csgm_kernel_time* out, int32_t capacity,
                       int32_t* count, int32_t reset);
 
+/* CUDA graphs for csgm_pair_device (0 off, the default; 1 on): the first call with given
+ * parameters, size, device buffers and launch shape runs normally and captures its device work
+ * into a graph; calls that repeat it replay the graph (one launch instead of about a dozen).  A
+ * graph is dropped when the session's workspace is reallocated.  Streamed pairs and per-kernel
+ * profiling (level 2) run without graphs.  No counterpart in the reference. */
+int csgm_session_set_graphs(csgm_session* session, int32_t enabled);
+
+/* Graphs captured and replayed by the session so far. */
+int csgm_graph_stats(csgm_session* session, int64_t* captured, int64_t* replayed);
+
 /* Waits for all work queued on the session's stream. */
 int csgm_session_synchronize(csgm_session* session);
 

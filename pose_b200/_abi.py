@@ -202,6 +202,8 @@ SIGNATURES = {
         [ctypes.c_char_p, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(CsgmTuning)],
     ),
     "csgm_session_set_wait_limit": (ctypes.c_int, [_P, _I64]),
+    "csgm_session_set_graphs": (ctypes.c_int, [_P, _I32]),
+    "csgm_graph_stats": (ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "csgm_pair_device": (
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P,

@@ -63,6 +63,7 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
                    (allocated + bytes) / 1048576.0, budget / 1048576.0);
     return nullptr;
   }
+  generation++;
   cudaError_t e = async_stream ? cudaMallocAsync(&b.ptr, bytes, async_stream) : cudaMalloc(&b.ptr, bytes);
   if (e != cudaSuccess) {
     *status = cuda_fail(e, "GPU buffer allocation");
@@ -75,6 +76,7 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
 }
 
 void Workspace::release_all() {
+  generation++;
   for (auto& b : buffers)
     if (b.ptr) {
       if (async_stream)
@@ -293,6 +295,7 @@ void csgm_session_close(csgm_session* s) {
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
   release_batch_slots(s);
+  s->graph_cache.clear();
   s->workspace.release_all();
   s->host_partial.release();
   cudaStreamDestroy(s->stream);
@@ -320,6 +323,23 @@ int csgm_session_set_streaming(csgm_session* s, int32_t mode, int32_t strip_rows
   std::lock_guard<std::mutex> guard(s->lock);
   s->sgm_mode = mode;
   s->strip_rows = strip_rows ? strip_rows : 64;  // Options.gpuStripRows default
+  return CSGM_OK;
+}
+
+int csgm_session_set_graphs(csgm_session* s, int32_t enabled) {
+  if (!s || (enabled != 0 && enabled != 1)) return fail(CSGM_E_INVALID, "invalid session or flag");
+  std::lock_guard<std::mutex> guard(s->lock);
+  cudaSetDevice(s->device);
+  s->graphs = enabled != 0;
+  if (!s->graphs) s->graph_cache.clear();
+  return CSGM_OK;
+}
+
+int csgm_graph_stats(csgm_session* s, int64_t* captured, int64_t* replayed) {
+  if (!s) return fail(CSGM_E_INVALID, "NULL session");
+  std::lock_guard<std::mutex> guard(s->lock);
+  if (captured) *captured = s->graph_cache.captured;
+  if (replayed) *replayed = s->graph_cache.replayed;
   return CSGM_OK;
 }
 
@@ -494,6 +514,9 @@ int csgm_pair_device(csgm_session* s, const csgm_params* p, const uint8_t* left,
   if (e != cudaSuccess) return cuda_fail(e, "Device selection");
   Context ctx{s->stream, s->sm_count, &s->workspace, &s->profiler, &s->profile};
   session_settings(ctx, s, *p, w, h);
+  if (s->graphs && s->profiler.level < 2)
+    return run_pair_device_graph(ctx, s->graph_cache, *p, left, right, valid_l, valid_r, w, h,
+                                 lr_checked, disp_l, disp_r, reasons, boundary, stats, sync != 0);
   return run_pair_device(ctx, *p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l, disp_r,
                          reasons, boundary, stats, sync != 0);
 }

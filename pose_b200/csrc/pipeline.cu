@@ -392,6 +392,112 @@ int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, con
                         disp_r, reasons, boundary, stats, sync, true);
 }
 
+void GraphCache::clear() {
+  for (auto& e : entries)
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+  entries.clear();
+}
+
+int run_pair_device_graph(Context& ctx, GraphCache& cache, const csgm_params& p,
+                          const uint8_t* left, const uint8_t* right, const uint8_t* valid_l,
+                          const uint8_t* valid_r, int w, int h, float* lr_checked, float* disp_l,
+                          float* disp_r, uint8_t* reasons, uint8_t* boundary, csgm_stats* stats,
+                          bool sync) {
+  ViewPlan plan;
+  int status = plan_pair(ctx, p, w, h, false, &plan);
+  if (status) return status;
+  if (plan.streamed)  // strips copy through host memory: not captured
+    return run_pair_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
+                           disp_r, reasons, boundary, stats, sync);
+  // The key: everything the captured work depends on.
+  struct Key {
+    csgm_params p;
+    int w, h;
+    const void* ptr[9];
+    SweepTuning tuning;
+    long long wait_limit;
+  } key{};
+  key.p = p;
+  key.w = w;
+  key.h = h;
+  const void* ptrs[9] = {left, right, valid_l, valid_r, lr_checked, disp_l, disp_r, reasons,
+                         boundary};
+  memcpy(key.ptr, ptrs, sizeof ptrs);
+  key.tuning = ctx.tuning;
+  key.wait_limit = ctx.wait_limit;
+  std::vector<uint8_t> bytes((const uint8_t*)&key, (const uint8_t*)&key + sizeof key);
+  GraphCache::Entry* hit = nullptr;
+  for (auto& e : cache.entries)
+    if (e.key == bytes && e.generation == ctx.ws->generation) hit = &e;
+  if (!hit) {
+    // The plain run allocates what the pipeline needs and gives this call's results; the same
+    // work is then captured for the calls that repeat it.
+    status = run_pair_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
+                             disp_r, reasons, boundary, stats, sync);
+    if (status) return status;
+    const uint64_t generation = ctx.ws->generation;
+    CK(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    const int level = ctx.prof->level;
+    ctx.prof->level = 0;
+    const int64_t launches = ctx.prof->launches;
+    const int captured = pair_on_device(ctx, p, plan, left, right, valid_l, valid_r, w, h,
+                                        lr_checked, disp_l, disp_r, reasons, boundary, nullptr,
+                                        false, false);
+    ctx.prof->level = level;
+    const int64_t in_graph = ctx.prof->launches - launches;
+    ctx.prof->launches = launches;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(ctx.stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = captured == CSGM_OK && end == cudaSuccess && graph &&
+                    ctx.ws->generation == generation &&
+                    cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();  // a capture that did not work leaves the plain run's results
+    if (cache.entries.size() >= GraphCache::kCapacity) {
+      auto oldest = std::min_element(cache.entries.begin(), cache.entries.end(),
+                                     [](const GraphCache::Entry& a, const GraphCache::Entry& b) {
+                                       return a.used < b.used;
+                                     });
+      if (oldest->exec) cudaGraphExecDestroy(oldest->exec);
+      cache.entries.erase(oldest);
+    }
+    // A key whose work could not be captured is remembered too, so it runs plainly from now on.
+    cache.entries.push_back({bytes, ok ? exec : nullptr, generation, ++cache.clock, in_graph});
+    if (ok) cache.captured++;
+    return CSGM_OK;
+  }
+  if (!hit->exec)
+    return run_pair_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
+                           disp_r, reasons, boundary, stats, sync);
+  // Replay.
+  hit->used = ++cache.clock;
+  cache.replayed++;
+  ctx.prof->begin_call(ctx.stream);
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (ctx.prof->level >= 1) {
+    t0 = ctx.prof->event();
+    t1 = ctx.prof->event();
+    CK(cudaEventRecord(t0, ctx.stream), "event record");
+  }
+  CK(cudaGraphLaunch(hit->exec, ctx.stream), "graph launch");
+  if (t1) CK(cudaEventRecord(t1, ctx.stream), "event record");
+  ctx.prof->launches += hit->launches;
+  if (!sync) return CSGM_OK;
+  DeviceStats host{};
+  CK(cudaMemcpyAsync(&host, ctx.ws->buffers[kStats].ptr, sizeof host, cudaMemcpyDeviceToHost,
+                     ctx.stream),
+     "stats readback");
+  CK(cudaStreamSynchronize(ctx.stream), "GPU SGM execution");
+  if (host.pad) return fail(CSGM_E_TIMEOUT, "a bounded device wait expired (code %llu)", host.pad);
+  if (stats) copy_stats(host, stats, false);
+  if (t1) {
+    ctx.profile->kernel_ns += (int64_t)(elapsed_ms(t0, t1) * 1e6);
+    ctx.profile->calls++;
+  }
+  return CSGM_OK;
+}
+
 // Uploads, device pipeline and downloads of a pair with host buffers, queued on ctx.stream.
 // pinned_stats (may be null) receives the selection counters; *host_d2h_stats says whether it was
 // queued.  Returns before the GPU has finished.

@@ -38,6 +38,24 @@ struct HostBuffer {
   void release();
 };
 
+// Captured device pipelines of csgm_pair_device, replayed when a call repeats one (same
+// parameters, size, buffers and launch shape) and the workspace has not been reallocated since.
+struct GraphCache {
+  struct Entry {
+    std::vector<uint8_t> key;
+    cudaGraphExec_t exec = nullptr;  // null: the work could not be captured; run it plainly
+    uint64_t generation = 0;
+    uint64_t used = 0;
+    int64_t launches = 0;  // kernels in the graph
+  };
+  static constexpr size_t kCapacity = 8;
+  std::vector<Entry> entries;
+  uint64_t clock = 0;
+  int64_t captured = 0, replayed = 0;
+  void clear();
+  ~GraphCache() { clear(); }
+};
+
 // Launch shape of the fused sweep (the autotuner's knobs).  0 / -1 fields: the default.
 struct SweepTuning {
   int rows = 0;         // rows per sweep CTA (row warps)
@@ -91,6 +109,9 @@ struct Workspace {
   Buffer buffers[kSlotCount];
   size_t allocated = 0;
   size_t budget = 0;
+  // Advances whenever a buffer is allocated again or released: a captured graph that refers to
+  // the buffers is valid only for the generation it was captured in.
+  uint64_t generation = 0;
   // When set, buffers are allocated and freed stream-ordered on this stream (no device-wide
   // synchronisation while other streams' kernels run).
   cudaStream_t async_stream = nullptr;
@@ -183,6 +204,13 @@ int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, con
 
 // bgr_l / bgr_r (optional, both or neither): the interleaved BGR images whose colour-distance
 // census gives the descriptors and texture (--census-mode color-distance).
+// run_pair_device through the graph cache (device buffers; replays a captured pipeline).
+int run_pair_device_graph(Context& ctx, GraphCache& cache, const csgm_params& p,
+                          const uint8_t* left, const uint8_t* right, const uint8_t* valid_l,
+                          const uint8_t* valid_r, int w, int h, float* lr_checked, float* disp_l,
+                          float* disp_r, uint8_t* reasons, uint8_t* boundary, csgm_stats* stats,
+                          bool sync);
+
 int run_pair_host(Context& ctx, const csgm_params& p, const uint8_t* left, const uint8_t* right,
                   const uint8_t* valid_l, const uint8_t* valid_r, int w, int h,
                   float* lr_checked, float* disp_l, float* disp_r, uint8_t* reasons,
@@ -227,6 +255,8 @@ struct csgm_session {
   int strip_rows = 64;
   csgm::HostBuffer host_partial;
   csgm::TuningTable tuning;  // csgm_autotune / csgm_session_load_tuning
+  bool graphs = false;       // csgm_session_set_graphs
+  csgm::GraphCache graph_cache;
   bool tuning_forced = false;  // csgm_session_set_tuning
   csgm::SweepTuning forced_tuning;
   // Batched / served pairs (batch.cu).

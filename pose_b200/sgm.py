@@ -214,6 +214,15 @@ class GpuSgm:
         check(self.lib.csgm_tuning_get(self.handle, ctypes.byref(params), w, h, ctypes.byref(t)))
         return self._tuning_dict(t)
 
+    def set_graphs(self, enabled: bool) -> None:
+        """Capture csgm_pair_device's device pipeline as a CUDA graph and replay it."""
+        check(self.lib.csgm_session_set_graphs(self.handle, int(bool(enabled))))
+
+    def graph_stats(self) -> tuple:
+        cap, rep = ctypes.c_int64(), ctypes.c_int64()
+        check(self.lib.csgm_graph_stats(self.handle, ctypes.byref(cap), ctypes.byref(rep)))
+        return cap.value, rep.value
+
     def set_wait_limit(self, cycles: int) -> None:
         """Watchdog of the device-side waits in SM clock cycles (0 = the default, ~2 s); a wait
         that runs out makes the call fail with CSGM_E_TIMEOUT and leaves the session usable."""
