@@ -53,7 +53,9 @@ def parse_args():
     ap.add_argument("--slots", type=int, default=4, help="cfg3/cfg4: batch slots")
     ap.add_argument("--pairs", type=int, default=48, help="cfg3: pairs in the batch")
     ap.add_argument("--rates", default="10,25,50,100,200,400", help="cfg4: offered pairs/s")
-    ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate (max)")
+    ap.add_argument("--requests", type=int, default=2000, help="cfg4: requests per rate")
+    ap.add_argument("--pool", type=int, default=200,
+                    help="cfg4: distinct synthetic pairs the requests are drawn from")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graphs", action="store_true",
@@ -700,7 +702,7 @@ def run_served(args):
     from pose_b200.batch import PairBatch, PinnedArray
     from pose_b200.sgm import GpuSgm
 
-    pool_items = mixed_pair_specs(24, 4000, mpix=(0.3, 6.0))
+    pool_items = mixed_pair_specs(args.pool, 4000, mpix=(0.3, 6.0))
     images = generate_mixed(pool_items)
     session = GpuSgm(0)
     lib = session.lib
@@ -715,7 +717,9 @@ def run_served(args):
     max_n = max(it["w"] * it["h"] for it in pool_items)
     outputs = [PinnedArray(lib, max_n, np.float32) for _ in range(args.slots)]
     batch = PairBatch(session, slots=args.slots, budget_bytes=120 << 30)
-    for i in range(len(pool_items)):  # warm: kernels, resident workspaces of both servers
+    # Warm: kernels and the per-pair session's workspace (its largest pairs).
+    for i in sorted(range(len(pool_items)), key=lambda i: -pool_items[i]["w"] * pool_items[i]["h"]
+                    * pool_items[i]["D"])[:8]:
         session.pair(params[i], inputs[i]["left"].array, inputs[i]["right"].array,
                      pool_items[i]["w"], pool_items[i]["h"])
     order = sorted(range(len(pool_items)), key=lambda i: -pool_items[i]["w"] * pool_items[i]["h"]
@@ -782,7 +786,7 @@ def run_served(args):
 
     rows = []
     for rate in [float(x) for x in args.rates.split(",")]:
-        count = int(min(args.requests, max(40, rate * 4)))
+        count = args.requests
         times, which = arrivals(rate, count, int(rate * 7))
         lb, tb = serve_batched(times, which)
         lp, tp = serve_per_pair(times, which)
@@ -802,7 +806,8 @@ def run_served(args):
         "dtype": "u16", "data": "synthetic",
         "config": {"workload": "cfg4 Poisson open loop, sizes log-uniform 0.3-6 Mpix, aspect "
                                "3:2/4:3, D in {64,128,192,256}, census/AD-census, 8 paths, "
-                               "24 distinct pairs drawn at random",
+                               f"{len(pool_items)} distinct pairs drawn at random, "
+                               f"{args.requests} requests per rate",
                    "slots": args.slots, "budget_gib": 120, "host_buffers": "pinned"},
         "rates": rows,
     }

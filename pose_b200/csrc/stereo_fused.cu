@@ -423,6 +423,12 @@ struct PenaltyArgs {
 };
 
 __global__ void penalty_kernel(const PenaltyArgs a) {
+  // StereoCost.pathP2 depends on the gray difference only: a table of its 256 values replaces the
+  // 64-bit division per path, view and pixel.
+  __shared__ int step_p2[256];
+  for (int d = threadIdx.x; d < 256; d += blockDim.x)
+    step_p2[d] = path_p2(a.p1, a.p2, a.edge_scale, d, 0);
+  __syncthreads();
   const int xs = blockIdx.x * blockDim.x + threadIdx.x;
   const int yp = blockIdx.y, s = blockIdx.z;
   const int W = a.W, H = a.H;
@@ -440,7 +446,7 @@ __global__ void penalty_kernel(const PenaltyArgs a) {
     for (int i = 0; i < 4; i++) {
       int value = a.p2;
       if (px[i] >= 0 && px[i] < W && py[i] >= 0 && py[i] < H)
-        value = path_p2(a.p1, a.p2, a.edge_scale, center, g[(int64_t)py[i] * W + px[i]]);
+        value = step_p2[abs(center - (int)g[(int64_t)py[i] * W + px[i]])];
       word[i] |= (uint32_t)(value - a.p1) << (16 * v);
     }
     if (a.tex[v][(int64_t)y * W + x]) word[0] |= 0x8000u << (16 * v);
