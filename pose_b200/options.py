@@ -48,6 +48,12 @@ class Options:
     # resident or streamed views (Options.java:32,39; --gpu-sgm, --gpu-strip-rows)
     gpuSgm: str = "auto"
     gpuStripRows: int = 64
+    # pyramid matcher (Options.java:28,85-86; DenseMatcher.java)
+    pyramidLevels: int = 1  # 0 = automatic
+    pyramidRadius: int = 16
+    tileSize: int = 512
+    tileOverlap: int = 32
+    memoryMb: int = 2048
 
     def copy(self) -> "Options":
         return copy.copy(self)
@@ -100,6 +106,10 @@ class Options:
             raise ValueError("--gpu-sgm must be auto, resident or streamed")
         if self.gpuStripRows < 1:
             raise ValueError("--gpu-strip-rows must be positive")
+        if (self.tileSize < 32 or self.tileOverlap < 2 or self.tileOverlap > self.tileSize
+                or self.pyramidLevels < 0 or self.pyramidLevels > 6 or self.pyramidRadius < 4
+                or self.memoryMb < 16):
+            raise ValueError("Invalid tiling / pyramid settings")
         if self.compute not in ("gpu", "auto"):
             raise ValueError("--compute must be gpu or auto for this backend (no CPU fallback)")
         from .stereo_cost import StereoCost

@@ -45,6 +45,10 @@ class Stats:
     photometricRejected: int = 0
     speckleRejected: int = 0
     valid: int = 0
+    # the pyramid matcher's coarse level (DenseMatcher.java:84-88)
+    coarseLowerBoundaryRejected: int = 0
+    coarseUpperBoundaryRejected: int = 0
+    coarseFullIntervalPixels: int = 0
 
     _C_NAMES = dict(zip(_abi.STATS_FIELDS, [
         "lowerBoundaryRejected", "fullIntervalPixels", "boundaryRejected",

@@ -49,3 +49,18 @@ def stats_csv(stats) -> str:
 
 def finite_count(d: np.ndarray) -> int:
     return int(np.isfinite(d).sum())
+
+
+def compute_recorded_cpu(o, a, b, ca, cb, w, h, ma, mb):
+    """CensusSgm.computeRecorded with compute=cpu and a collecting observer, as the pyramid
+    matcher's tiles call it (DenseMatcher.java:306-318): a Result with reasons and flags."""
+    from pose_b200.sgm import Result, Stats
+
+    prm = params_from_options(o)
+    res = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True, left_bgr=ca, right_bgr=cb)
+    disp, stats, reasons = res["checked"].copy(), res["stats"], res["reasons"].copy()
+    orc.postfilter(post_from_options(o), a, b, res["dr"], w, h, disp, stats, reasons,
+                   left_bgr=ca, right_bgr=cb)
+    return Result(w, h, disp, Stats.from_c(stats), res["dl"], res["dr"], reasons,
+                  res["boundary"])
+
