@@ -267,7 +267,10 @@ def run_reference(args):
     left, right, _ = make_pair(spec)
     w, h = spec.width, spec.height
     threads = os.cpu_count() or 1
-    rows = args.cpu_rows or default_cpu_rows(prm, h)
+    # The whole pair where one takes seconds on all host threads (640x480 and 1600x1067 pairs);
+    # a full-width band of the 16-path 3000x2000 D256 pair, sized to the same amount of work.
+    work = w * h * prm.disparities * max(1, prm.directions // 8)
+    rows = args.cpu_rows or (h if work <= 3e8 else max(prm.window_y + 2, int(h * 3e8 / work)))
     values = []
     for i in range(args.warmup + args.steps):
         v, _ = cpu_baseline(prm, left, right, w, h, rows, threads)
@@ -281,9 +284,12 @@ def run_reference(args):
         "ms_per_step": cells / (value * 1e9) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": args.workload + " " + workload_desc(args.workload, prm),
-                   "sample": f"{w}x{rows} full-width band of the pair"},
+                   "sample": ("the whole pair" if rows == h else
+                              f"{w}x{rows} full-width band of the pair")},
         "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
-                         "sample": f"{w}x{rows} band, census+both views+LR, {threads} threads"},
+                         "sample": (f"whole {w}x{h} pair" if rows == h else
+                                    f"{w}x{rows} band") +
+                                   f", census+both views+LR, {threads} threads"},
         "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
