@@ -26,8 +26,10 @@ namespace csgm {
 
 static int words_of(const csgm_params& p) { return (p.window_x * p.window_y - 1 + 63) / 64; }
 
-static bool use_fused(const csgm_params& p) {
-  return !(p.flags & CSGM_FLAG_GENERAL) && fused_supported(p);
+// The fused kernels run the pair when its parameters allow them and it is at most 65535 rows
+// tall (the sweep's row-block indices); otherwise the general kernels do.
+static bool use_fused(const csgm_params& p, int h) {
+  return !(p.flags & CSGM_FLAG_GENERAL) && fused_supported(p) && h <= 65535;
 }
 
 // Device bytes of a pair besides its cost volumes and aggregates: descriptors, masks, the views'
@@ -48,7 +50,7 @@ size_t pair_workspace_bytes(const csgm_params& p, int w, int h, bool host_inputs
                             const SweepTuning& tuning) {
   size_t n = (size_t)w * h, D = (size_t)p.disparities;
   size_t bytes = pair_fixed_bytes(p, w, h, host_inputs, color);
-  if (use_fused(p))
+  if (use_fused(p, h))
     bytes += fused_workspace_bytes(p, w, h, tuning);
   else
     bytes += n * D * 2 + n * D * p.aggregate_bytes;  // one cost volume + one aggregate
@@ -337,7 +339,7 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
     status = run_view_streamed(ctx, p, desc_r, desc_l, tex_r, tex_l, right, left, w, h, 1, disp_r,
                                nullptr, nullptr, nullptr, nullptr, plan.rows);
     if (status) return status;
-  } else if (use_fused(p)) {
+  } else if (use_fused(p, h)) {
     // Both views in one pass structure (stereo_fused.cu).
     FusedViews v{desc_l,           desc_r,           tex_l,          tex_r,
                  left,             right,            disp_l,         disp_r,
@@ -859,7 +861,7 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
   // Resident on the fused kernels when they apply and their workspace fits the budget, else
   // resident on the general ones, else streamed (as the session's mode allows).
   const bool summary = out_summary != nullptr;
-  if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && use_fused(p) && h <= 65535 &&
+  if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && use_fused(p, h) &&
       match_fused_bytes(p, w, h, summary, ctx.tuning) <= ctx.ws->budget)
     return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                            out_disp, out_summary, reasons, boundary, stats);
