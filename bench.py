@@ -157,6 +157,17 @@ def pair_model_bytes_per_cell(prm) -> int:
     return 5 + 4 * prm.aggregate_bytes
 
 
+def model_bytes_per_launch(kernel: str, prm, w: int, h: int):
+    """A kernel's share of the pair model's 5 + 4 Sb bytes per cell (SURVEY 8(d) accounting):
+    the sweeps read both views' cost volumes (2 streams x 2 views x 1 B) and one stream's partial
+    aggregate is written and read by the other (2 views x 2 Sb); the cost kernel writes the volume
+    once (1 B).  None for kernels the model does not count."""
+    cells = w * h * prm.disparities
+    sb = prm.aggregate_bytes
+    table = {"sweep": 4 + 4 * sb, "cost_pair": 1, "cost_volume": 1}
+    return table[kernel] * cells if kernel in table else None
+
+
 def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int, lines_in_sweep=False):
     """Algorithmic HBM bytes of one launch of `kernel`, from the bytes each kernel must move per
     cell (uint8 costs, Sb-byte partial aggregates, both views).  None for per-pixel kernels and
@@ -414,10 +425,12 @@ def run_ours(args):
     roofline = None
     if kernels:
         name, (count, total_ns) = max(kernels.items(), key=lambda kv: kv[1][1])
-        per_launch = algorithmic_bytes_per_launch(name, prm, w, h, "lines_rest" in kernels)
+        per_launch = model_bytes_per_launch(name, prm, w, h)
+        impl = algorithmic_bytes_per_launch(name, prm, w, h, "lines_rest" in kernels)
         peak, peak_kind = measured_peak_gbs()
         if per_launch and count:
-            achieved = per_launch / (total_ns / count / 1e9) / 1e9
+            launch_s = total_ns / count / 1e9
+            achieved = per_launch / launch_s / 1e9
             roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1),
                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                         "frac": round(achieved / peak, 4),
@@ -427,7 +440,11 @@ def run_ours(args):
                         "share": round(total_ns / max(1, sum(v[1] for v in kernels.values())), 3),
                         "pair_model_frac": round(
                             pair_model_bytes_per_cell(prm) * cells / (ms_per_step / 1e3) / 1e9
-                            / peak, 4)}
+                            / peak, 4),
+                        # the bytes the implementation's own passes move (its intermediates
+                        # included: the third partial, the line walks' forward costs)
+                        "impl_bytes_per_launch": impl,
+                        "impl_frac": round(impl / launch_s / 1e9 / peak, 4) if impl else None}
 
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
