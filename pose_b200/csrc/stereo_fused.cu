@@ -1719,7 +1719,8 @@ cudaError_t launch_sweep(const SweepArgs& a, cudaStream_t stream, bool exclusive
 // an SM (one CTA per SM: at D = 128, 1067 rows, 12 rows per CTA measured 2.84 ms per sweep
 // against 2.93 with 8 and 3.04 with 16).
 constexpr int kChunk = 2;  // pixels per cost chunk and per carry publication
-constexpr int rows_default(int regs) { return regs >= 8 ? 4 : regs == 4 ? 12 : 8; }
+// 193..256 disparities: 8 rows (3000x2000 D256, 16 paths: 46-48 ms per pair against 50 with 4).
+constexpr int rows_default(int regs) { return regs == 4 ? 12 : 8; }
 
 // Rows per sweep CTA: the default, or CSGM_SWEEP_ROWS (4, 8, or 12 at D <= 128) for tuning runs.
 int rows_for(int regs) {

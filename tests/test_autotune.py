@@ -47,7 +47,8 @@ def test_autotune_caches_and_reloads(tmp_path):
         assert again == best
 
 
-def test_every_launch_shape_gives_the_same_bits():
+@pytest.mark.parametrize("D,directions", [(128, 8), (256, 8), (256, 16), (192, 4)])
+def test_every_launch_shape_gives_the_same_bits(D, directions):
     """A pair under each shape the autotuner tries, forced, against the oracle."""
     from pose_b200.sgm import GpuSgm
     from pose_b200.synthetic import PairSpec, make_pair
@@ -55,16 +56,22 @@ def test_every_launch_shape_gives_the_same_bits():
     spec = PairSpec(400, 140, planes=3, d_min=4, d_max=100, seed=9)
     left, right, _ = make_pair(spec)
     w, h = spec.width, spec.height
-    prm = params(D=128)
+    prm = params(D=D, directions=directions)
     want = orc.pair(prm, left, right, w, h, want_reasons=True)
+    regs = (D + 63) // 64 * 2
     with GpuSgm(0) as s:
-        for rows in (4, 8, 12):
+        for rows in (4, 8, 12) if regs == 4 else (4, 8):
             for lw in (0, 4, 8):
                 for slack in (10, 100, 400):
                     s.set_tuning({"rows_per_block": rows, "line_warps": lw, "line_slack": slack})
                     t = s.tuning(prm, w, h)
-                    assert (t["rows_per_block"], t["line_warps"], t["line_slack"]) == (
-                        rows, lw, slack)
+                    if directions < 8 or (lw and t["line_warps"] != lw):
+                        # no line warps in 4-path mode; shapes whose line rings exceed a CTA's
+                        # shared memory run with fewer line warps
+                        assert t["line_warps"] < max(lw, 1)
+                    else:
+                        assert (t["rows_per_block"], t["line_warps"], t["line_slack"]) == (
+                            rows, lw, slack)
                     got = s.pair(prm, left, right, w, h, want_views=True, want_reasons=True)
                     assert np.array_equal(got.disparity.view(np.uint32),
                                           want["checked"].view(np.uint32)), (rows, lw, slack)
