@@ -483,6 +483,14 @@ constexpr int kPrefetch = 8;
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
+// The same copy under a predicate (no branch around it; `src` is not read when `on` is false).
+__device__ __forceinline__ void cp_async16_if(uint32_t dst, const void* src, bool on) {
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q cp.async.cg.shared.global [%0], [%1], 16;\n}\n" ::
+          "r"(dst),
+      "l"(src), "r"((int)on)
+      : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -541,9 +549,11 @@ struct SweepLayout {
   static constexpr int RING = 4;        // ring slots between consecutive row warps
   static constexpr int NB = 4;          // cost chunk slots per row warp
   static constexpr int CS = 16 / K;     // carry chunk slots (16 pixels)
-  // One pixel's vertical path states, normalised (L - min L, so the successor needs no
-  // minimum): NV x Dp u16x2.
-  static constexpr int vslot = NV * Dp * 4;
+  // One pixel's vertical path states as computed (NV x Dp u16x2), then their row minima (NV
+  // words, padded to 16 bytes): the successor subtracts the minimum itself, as the (1,0) path
+  // does with its state in registers.
+  static constexpr int vmins = NV * Dp * 4;
+  static constexpr int vslot = vmins + 16;
   // One cost chunk: K x Dp cost bytes of the left view, of the right view, K penalty records.
   static constexpr int cslot = K * (2 * Dp + 16);
   static constexpr int bars = 0;                            // cost_full[R][NB], carry_full[CS]
@@ -711,19 +721,13 @@ __device__ __forceinline__ void zero_state(PathState<REGS>& s) {
   s.m = 0;
 }
 
-// Path `path` of one pixel slot (vslot layout) for this lane (`lane_slot` = the pixel slot's
-// shared address plus this lane's offset): a normalised state (minimum 0).
+// Path `path` of the pixel slot at shared address `slot` (vslot layout with the minima at byte
+// `vmins`) for the lane whose words start `lane_off` bytes in: its state and its row minimum.
 template <int REGS>
-__device__ __forceinline__ void load_path(uint32_t lane_slot, int path, PathState<REGS>& s) {
-  lds_words<REGS>(lane_slot + path * (32 * REGS * 4), s.v);
-  s.m = 0;
-}
-// L - min L of state s (no borrow: every half is at least its minimum), ANDed with keep.
-template <int REGS>
-__device__ __forceinline__ void normalise(const PathState<REGS>& s, uint32_t keep,
-                                          uint32_t (&d)[REGS]) {
-#pragma unroll
-  for (int j = 0; j < REGS; j++) d[j] = (s.v[j] - s.m) & keep;
+__device__ __forceinline__ void load_path(uint32_t slot, uint32_t lane_off, int vmins, int path,
+                                          PathState<REGS>& s) {
+  lds_words<REGS>(slot + lane_off + path * (32 * REGS * 4), s.v);
+  s.m = lds_u32(slot + vmins + 4 * path);
 }
 
 // Cost of the pad disparities D..Dp-1 in both halves.  A pad lane's path cost is at least 1536,
@@ -802,10 +806,12 @@ __device__ __forceinline__ void paths_step(const PathState<REGS> (&prev)[NP],
           __viaddmin_u16x2(__vimin3_u16x2(dn, up, q[i]), p1x2, prev[i].v[j]);
       out[i].v[j] = t + c[j] - prev[i].m;  // t >= minLp in both halves: no borrow
     }
+    // Warp minima of both halves: the high 16 bits of a 32-bit minimum are the minimum of the
+    // high halves, so one reduction of mm and one of mm << 16 give both.
     const uint32_t mm = lane_min<REGS>(out[i].v);
-    const uint32_t r0 = __reduce_min_sync(0xffffffffu, mm & 0xffffu);
-    const uint32_t r1 = __reduce_min_sync(0xffffffffu, mm >> 16);
-    out[i].m = __byte_perm(r0, r1, 0x5410);
+    const uint32_t hi = __reduce_min_sync(0xffffffffu, mm);
+    const uint32_t lo = __reduce_min_sync(0xffffffffu, mm << 16);
+    out[i].m = __byte_perm(lo, hi, 0x7632);
   }
 }
 
@@ -827,29 +833,27 @@ __device__ __forceinline__ void walk_line(const LineArgs& a, int line, uint32_t 
   uint32_t* part = a.part + lane * REGS;
   const int64_t step = (int64_t)W - 1;  // pixel-index step along the line (down-left)
   const int64_t p0 = (int64_t)y0 * W + x0;
+  // Per lane, once per line: lanes 0 .. 2 CH - 1 copy one 16-byte chunk of a view's costs, lane
+  // 31 the penalty record.  The up stream's record of pixel i sits at pen_up0 - i * step (its
+  // stream coordinates mirror the image in x and y).
+  const bool cost_lane = lane < 2 * CH;
+  const uint32_t cost_dst = S::cost + (cost_lane ? (lane / CH) * Dp + (lane % CH) * 16 : 0);
+  const uint8_t* cost_src =
+      (cost_lane && lane >= CH ? a.cost[1] : a.cost[0]) + (cost_lane ? (lane % CH) * 16 : 0);
+  const int64_t pen_up0 = ((int64_t)2 * H - 1 - y0) * W + (W - 1 - x0);
 
   // Issues the copies of pixel i into ring slot `slot` as one commit group (empty if i is off
   // the line, so the group count stays in step).
   auto fetch = [&](int slot, int i, bool back) {
-    if (i >= 0 && i < len) {
-      const int64_t p = p0 + i * step;
-      const uint32_t s = ring + slot * S::bytes;
-      if (lane < 2 * CH) {
-        const int view = lane / CH, chunk = lane % CH;
-        cp_async16(s + S::cost + view * Dp + chunk * 16,
-                   (view ? a.cost[1] : a.cost[0]) + p * Dp + chunk * 16);
-      }
-      if (lane == 31) {
-        const int y = y0 + i, x = x0 - i;
-        const uint4* rec = back ? &a.pen[((int64_t)H + (H - 1 - y)) * W + (W - 1 - x)]
-                                : &a.pen[p];
-        cp_async16(s + S::pen, rec);
-      }
-      if (back) {
+    const bool on = i >= 0 && i < len;
+    const int64_t p = p0 + i * step;
+    const uint32_t s = ring + slot * S::bytes;
+    cp_async16_if(s + cost_dst, cost_src + p * Dp, on && cost_lane);
+    cp_async16_if(s + S::pen, &a.pen[back ? pen_up0 - i * step : p], on && lane == 31);
+    if (back) {
 #pragma unroll
-        for (int c = lane; c < Dp / 4; c += 32)
-          cp_async16(s + S::part + c * 16, a.part + p * Dp + c * 4);
-      }
+      for (int c = lane; c < Dp / 4; c += 32)
+        cp_async16_if(s + S::part + c * 16, a.part + p * Dp + c * 4, on);
     }
     cp_async_commit();
   };
@@ -1268,14 +1272,13 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
   const uint32_t sm0 = smem_u32(smem);
   const uint32_t lane_off = lane * REGS * 4;
   const uint32_t slots_a = sm0 + L::cost + w * NB * L::cslot;
-  const uint32_t ring_a = sm0 + L::ring + w * RING * L::vslot + lane_off;
-  const uint32_t zero_a = sm0 + L::zero + lane_off;
+  const uint32_t ring_a = sm0 + L::ring + w * RING * L::vslot;
+  const uint32_t zero_a = sm0 + L::zero;
   // Predecessor row: the ring of the warp above, the carry buffer, or (first image row) the zero
   // slot for every pixel.
-  const uint32_t up_a = (yp == 0     ? sm0 + L::zero
-                         : use_carry ? sm0 + L::carry
-                                     : sm0 + L::ring + (w - 1) * RING * L::vslot) +
-                        lane_off;
+  const uint32_t up_a = yp == 0     ? sm0 + L::zero
+                        : use_carry ? sm0 + L::carry
+                                    : sm0 + L::ring + (w - 1) * RING * L::vslot;
   const int up_mask = yp == 0 ? 0 : use_carry ? CS * K - 1 : RING - 1;
   uint8_t* carry_out = a.carry + (int64_t)(stream * a.nb + b) * W * L::vslot;
   const uint8_t* cost_row0 = a.cost[0] + (int64_t)y * W * Dp;
@@ -1288,7 +1291,7 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
   // Cost bytes of chunk pixel `off` sit at slot + cost_first + off * cost_step (image order).
   const int cost_first_full = (mirror ? (K - 1) * Dp : 0) + lane * REGS;
   const int cost_step = mirror ? -Dp : Dp;
-  uint8_t* carry_ptr = carry_out + lane_off;  // this row's carry slot of the current pixel
+  uint8_t* carry_ptr = carry_out;  // this row's carry slot of the current pixel
 
   auto issue_chunk = [&](int c) {  // lane 0
     const int n = chunk_n(c);
@@ -1343,15 +1346,15 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
       const uint4 pw = lds_v4(pb);
       PathState<REGS> prev[NPATH];
       prev[0] = horiz;
-      load_path<REGS>(up_a + (xs & up_mask) * L::vslot, 0, prev[1]);
+      load_path<REGS>(up_a + (xs & up_mask) * L::vslot, lane_off, L::vmins, 0, prev[1]);
       if constexpr (NPATH > 2) {
         const uint32_t pd = xs > 0 ? up_a + ((xs - 1) & up_mask) * L::vslot : zero_a;
-        load_path<REGS>(pd, 1, prev[2]);
+        load_path<REGS>(pd, lane_off, L::vmins, 1, prev[2]);
       }
       uint32_t q[NPATH];
       q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
-      q[1] = pw.y;  // normalised predecessors: minimum 0
-      if constexpr (NPATH > 2) q[2] = pw.z;
+      q[1] = prev[1].m + pw.y;
+      if constexpr (NPATH > 2) q[2] = prev[2].m + pw.z;
       PathState<REGS> out[NPATH];
       paths_step<REGS, NPATH>(prev, q, p1x2, cst, lo_edge, hi_edge, out);
       // Partial aggregate of this stream's paths.
@@ -1365,30 +1368,31 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
       }
       store_words_cs<REGS>(sum_ptr, s);
       sum_ptr += sum_step;
-      // The row below gets normalised states; successors of an untextured pixel start afresh
-      // (CensusSgm.java:432-433): they see zeros.
+      // The row below gets the states and their minima; successors of an untextured pixel start
+      // afresh (CensusSgm.java:432-433): they see zeros.
       const uint32_t keep = prmt(pw.x, 0, 0xbb99u);
       const uint32_t o = ring_a + (xs & (RING - 1)) * L::vslot;
-      if (keep == 0xffffffffu) {
+      if (keep != 0xffffffffu) {
 #pragma unroll
-        for (int i = 0; i < NV; i++) {
-          uint32_t d[REGS];
+        for (int i = 0; i < NPATH; i++) {
 #pragma unroll
-          for (int j = 0; j < REGS; j++) d[j] = out[i + 1].v[j] - out[i + 1].m;
-          sts_words<REGS>(o + i * (Dp * 4), d);
-          if constexpr (PUBLISH) store_words<REGS>(carry_ptr + i * (Dp * 4), d);
+          for (int j = 0; j < REGS; j++) out[i].v[j] &= keep;
+          out[i].m &= keep;
         }
-      } else {
+      }
 #pragma unroll
-        for (int i = 0; i < NV; i++) {
-          uint32_t d[REGS];
-          normalise<REGS>(out[i + 1], keep, d);
-          sts_words<REGS>(o + i * (Dp * 4), d);
-          if constexpr (PUBLISH) store_words<REGS>(carry_ptr + i * (Dp * 4), d);
+      for (int i = 0; i < NV; i++) {
+        sts_words<REGS>(o + lane_off + i * (Dp * 4), out[i + 1].v);
+        if constexpr (PUBLISH) store_words<REGS>(carry_ptr + lane_off + i * (Dp * 4), out[i + 1].v);
+      }
+      if (lane == 0) {
+        if constexpr (NV == 2) {
+          sts_v2(o + L::vmins, out[1].m, out[2].m);
+          if constexpr (PUBLISH) *(uint2*)(carry_ptr + L::vmins) = make_uint2(out[1].m, out[2].m);
+        } else {
+          asm volatile("st.shared.u32 [%0], %1;" ::"r"(o + L::vmins), "r"(out[1].m));
+          if constexpr (PUBLISH) *(uint32_t*)(carry_ptr + L::vmins) = out[1].m;
         }
-#pragma unroll
-        for (int j = 0; j < REGS; j++) out[0].v[j] &= keep;
-        out[0].m &= keep;
       }
       if constexpr (PUBLISH) carry_ptr += L::vslot;
       horiz = out[0];
@@ -1812,7 +1816,7 @@ struct FusedLayout {
     rows = rows_per_block;
     nb = (h + rows - 1) / rows;
     const int nv = p.directions >= 8 ? 2 : 1;
-    vslot = nv * Dp * 4;
+    vslot = nv * Dp * 4 + 16;  // the states and their minima (16 bytes)
     size_t n = (size_t)w * h;
     cost = n * Dp;
     sum = n * Dp * 4;
