@@ -1323,14 +1323,20 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
   zero_state(horiz);
   int carry_ready = 0;
 
-  // Idle steps before this row starts (the 1-pixel lag behind the row above).
-  for (int step = 0; step < w; step++) rows_barrier(R * 32);
-
   // The sweep of one row.  CARRY_IN: the row above is the previous block's carry row (waited for
   // chunk by chunk); PUBLISH: this row's vertical states are also stored as this block's carry.
+  // The (1,0) path of a pixel depends on this warp's registers alone, so it is computed one step
+  // ahead, with the pixel's costs and penalty record, before the step barrier: after the barrier
+  // only the paths whose predecessor lies in the row above remain.
+  struct Prepared {
+    uint32_t c[REGS];    // the pixel's widened costs
+    uint4 pw;            // its penalty record
+    PathState<REGS> h;   // its (1,0) path state
+  };
   auto sweep_row = [&](auto carry_tag, auto publish_tag) {
     constexpr bool CARRY_IN = decltype(carry_tag)::value;
     constexpr bool PUBLISH = decltype(publish_tag)::value;
+    constexpr int NU = NPATH - 1;  // paths from the row above
     auto wait_carry = [&](int need) {
       need = min(need, nchunks - 1);
       while (carry_ready <= need) {
@@ -1338,64 +1344,72 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
         carry_ready++;
       }
     };
-    // One pixel: xs (stream column); cb = shared address of this lane's left-view cost bytes,
-    // pb = shared address of the pixel's penalty record.
-    auto pixel = [&](int xs, uint32_t cb, uint32_t pb) {
-      uint32_t cst[REGS];
-      widen_costs<REGS>(cb, cb + K * Dp, pad, cst);
-      const uint4 pw = lds_v4(pb);
-      PathState<REGS> prev[NPATH];
-      prev[0] = horiz;
-      load_path<REGS>(up_a + (xs & up_mask) * L::vslot, lane_off, L::vmins, 0, prev[1]);
-      if constexpr (NPATH > 2) {
+    // Costs, record and (1,0) path of the next pixel: cb = shared address of this lane's
+    // left-view cost bytes, pb = shared address of the pixel's penalty record.
+    auto prepare = [&](uint32_t cb, uint32_t pb, Prepared& n) {
+      widen_costs<REGS>(cb, cb + K * Dp, pad, n.c);
+      n.pw = lds_v4(pb);
+      const uint32_t q[1] = {horiz.m + (n.pw.x & 0x7fff7fffu)};
+      PathState<REGS> prev[1] = {horiz}, out[1];
+      paths_step<REGS, 1>(prev, q, p1x2, n.c, lo_edge, hi_edge, out);
+      n.h = out[0];
+    };
+    // The rest of pixel xs (stream column) from its prepared part.
+    auto pixel = [&](int xs, const Prepared& n) {
+      PathState<REGS> prev[NU];
+      load_path<REGS>(up_a + (xs & up_mask) * L::vslot, lane_off, L::vmins, 0, prev[0]);
+      if constexpr (NU > 1) {
         const uint32_t pd = xs > 0 ? up_a + ((xs - 1) & up_mask) * L::vslot : zero_a;
-        load_path<REGS>(pd, lane_off, L::vmins, 1, prev[2]);
+        load_path<REGS>(pd, lane_off, L::vmins, 1, prev[1]);
       }
-      uint32_t q[NPATH];
-      q[0] = prev[0].m + (pw.x & 0x7fff7fffu);
-      q[1] = prev[1].m + pw.y;
-      if constexpr (NPATH > 2) q[2] = prev[2].m + pw.z;
-      PathState<REGS> out[NPATH];
-      paths_step<REGS, NPATH>(prev, q, p1x2, cst, lo_edge, hi_edge, out);
+      uint32_t q[NU];
+      q[0] = prev[0].m + n.pw.y;
+      if constexpr (NU > 1) q[1] = prev[1].m + n.pw.z;
+      PathState<REGS> out[NU];
+      paths_step<REGS, NU>(prev, q, p1x2, n.c, lo_edge, hi_edge, out);
       // Partial aggregate of this stream's paths.
       uint32_t s[REGS];
 #pragma unroll
       for (int j = 0; j < REGS; j++) {
-        uint32_t acc = out[0].v[j];
+        uint32_t acc = n.h.v[j];
 #pragma unroll
-        for (int i = 1; i < NPATH; i++) acc += out[i].v[j];
+        for (int i = 0; i < NU; i++) acc += out[i].v[j];
         s[j] = acc;
       }
       store_words_cs<REGS>(sum_ptr, s);
       sum_ptr += sum_step;
       // The row below gets the states and their minima; successors of an untextured pixel start
       // afresh (CensusSgm.java:432-433): they see zeros.
-      const uint32_t keep = prmt(pw.x, 0, 0xbb99u);
+      const uint32_t keep = prmt(n.pw.x, 0, 0xbb99u);
       const uint32_t o = ring_a + (xs & (RING - 1)) * L::vslot;
+      PathState<REGS> h = n.h;
       if (keep != 0xffffffffu) {
 #pragma unroll
-        for (int i = 0; i < NPATH; i++) {
+        for (int i = 0; i < NU; i++) {
 #pragma unroll
           for (int j = 0; j < REGS; j++) out[i].v[j] &= keep;
           out[i].m &= keep;
         }
+#pragma unroll
+        for (int j = 0; j < REGS; j++) h.v[j] &= keep;
+        h.m &= keep;
       }
 #pragma unroll
       for (int i = 0; i < NV; i++) {
-        sts_words<REGS>(o + lane_off + i * (Dp * 4), out[i + 1].v);
-        if constexpr (PUBLISH) store_words<REGS>(carry_ptr + lane_off + i * (Dp * 4), out[i + 1].v);
+        sts_words<REGS>(o + lane_off + i * (Dp * 4), out[i].v);
+        if constexpr (PUBLISH) store_words<REGS>(carry_ptr + lane_off + i * (Dp * 4), out[i].v);
       }
       if (lane == 0) {
         if constexpr (NV == 2) {
-          sts_v2(o + L::vmins, out[1].m, out[2].m);
-          if constexpr (PUBLISH) *(uint2*)(carry_ptr + L::vmins) = make_uint2(out[1].m, out[2].m);
+          sts_v2(o + L::vmins, out[0].m, out[1].m);
+          if constexpr (PUBLISH) *(uint2*)(carry_ptr + L::vmins) = make_uint2(out[0].m, out[1].m);
         } else {
-          asm volatile("st.shared.u32 [%0], %1;" ::"r"(o + L::vmins), "r"(out[1].m));
-          if constexpr (PUBLISH) *(uint32_t*)(carry_ptr + L::vmins) = out[1].m;
+          asm volatile("st.shared.u32 [%0], %1;" ::"r"(o + L::vmins), "r"(out[0].m));
+          if constexpr (PUBLISH) *(uint32_t*)(carry_ptr + L::vmins) = out[0].m;
         }
       }
       if constexpr (PUBLISH) carry_ptr += L::vslot;
-      horiz = out[0];
+      horiz = h;
     };
     // End of chunk c: refill its slot NB chunks ahead, report carry progress / release.
     auto end_chunk = [&](int c) {
@@ -1412,27 +1426,45 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
       }
       __syncwarp();
     };
+    // The first pixel of chunk c, once its copies have landed.
+    auto prepare_first = [&](int c, Prepared& n) {
+      if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
+      const uint32_t slot = slots_a + (c % NB) * L::cslot;
+      const int first = (mirror ? (chunk_n(c) - 1) * Dp : 0) + lane * REGS;
+      prepare(slot + first, slot + 2 * K * Dp, n);
+    };
+    Prepared nx;
+    prepare_first(0, nx);
+    // Idle steps before this row starts (the 1-pixel lag behind the row above).
+    for (int step = 0; step < w; step++) rows_barrier(R * 32);
     const int full_chunks = W / K;
     for (int c = 0; c < full_chunks; c++) {
-      if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
       if constexpr (CARRY_IN) wait_carry(c);
       const uint32_t slot = slots_a + (c % NB) * L::cslot;
 #pragma unroll
       for (int off = 0; off < K; off++) {
-        pixel(c * K + off, slot + cost_first_full + off * cost_step, slot + 2 * K * Dp + 16 * off);
+        const Prepared cur = nx;
+        pixel(c * K + off, cur);
+        if (off + 1 < K)
+          prepare(slot + cost_first_full + (off + 1) * cost_step, slot + 2 * K * Dp + 16 * (off + 1),
+                  nx);
+        else if (c + 1 < nchunks)
+          prepare_first(c + 1, nx);
         rows_barrier(R * 32);
       }
       end_chunk(c);
     }
     if (full_chunks < nchunks) {
-      // Partial last chunk.
+      // Partial last chunk (its first pixel is prepared).
       const int c = full_chunks, n = W - c * K;
-      if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
       if constexpr (CARRY_IN) wait_carry(c);
       const uint32_t slot = slots_a + (c % NB) * L::cslot;
       const int first = (mirror ? (n - 1) * Dp : 0) + lane * REGS;
       for (int off = 0; off < n; off++) {
-        pixel(c * K + off, slot + first + off * cost_step, slot + 2 * K * Dp + 16 * off);
+        const Prepared cur = nx;
+        pixel(c * K + off, cur);
+        if (off + 1 < n)
+          prepare(slot + first + (off + 1) * cost_step, slot + 2 * K * Dp + 16 * (off + 1), nx);
         rows_barrier(R * 32);
       }
       end_chunk(c);
