@@ -736,13 +736,18 @@ __device__ __forceinline__ void load_path(uint32_t slot, uint32_t lane_off, int 
 // paths a pad total stays below 16 x (1536 + 511) < 2^16, above the invalid threshold 16 x 512.
 constexpr uint32_t kPadCost = 0x06000600u;
 
-// This lane's costs of both views as packed u16 pairs: byte j of each view widened, 0x80 -> 512,
-// and pad[j] ORed in (disparities >= D are lifted to kPadCost so they never win a minimum).
+// This lane's costs of both views as packed u16 pairs (widen_costs = load_cost_words +
+// widen_words): byte j of each view widened, 0x80 -> 512, and pad[j] ORed in (disparities >= D
+// are lifted to kPadCost so they never win a minimum).
 template <int REGS>
-__device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint32_t (&pad)[REGS],
-                                            uint32_t (&c)[REGS]) {
-  constexpr int NW = (REGS + 3) / 4;
+struct CostWords {  // this lane's raw cost bytes of both views
+  static constexpr int NW = (REGS + 3) / 4;
   uint32_t a[NW], b[NW];
+};
+template <int REGS>
+__device__ __forceinline__ void load_cost_words(uint32_t c0, uint32_t c1, CostWords<REGS>& w) {
+  uint32_t(&a)[CostWords<REGS>::NW] = w.a;
+  uint32_t(&b)[CostWords<REGS>::NW] = w.b;
   if constexpr (REGS == 2) {
     a[0] = lds_u16(c0);
     b[0] = lds_u16(c1);
@@ -761,6 +766,12 @@ __device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint
     b[0] = t1.x;
     b[1] = t1.y;
   }
+}
+template <int REGS>
+__device__ __forceinline__ void widen_words(const CostWords<REGS>& w, const uint32_t (&pad)[REGS],
+                                            uint32_t (&c)[REGS]) {
+  const uint32_t(&a)[CostWords<REGS>::NW] = w.a;
+  const uint32_t(&b)[CostWords<REGS>::NW] = w.b;
 #pragma unroll
   for (int j = 0; j < REGS; j++) {
     const uint32_t i = j % 4;
@@ -768,6 +779,13 @@ __device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint
     const uint32_t sel = i | ((i | 8) << 4) | ((4 + i) << 8) | (((4 + i) | 8) << 12);
     c[j] = (prmt(a[j / 4], b[j / 4], sel) & 0x027f027fu) | pad[j];
   }
+}
+template <int REGS>
+__device__ __forceinline__ void widen_costs(uint32_t c0, uint32_t c1, const uint32_t (&pad)[REGS],
+                                            uint32_t (&c)[REGS]) {
+  CostWords<REGS> w;
+  load_cost_words<REGS>(c0, c1, w);
+  widen_words<REGS>(w, pad, c);
 }
 
 // Lane minimum of REGS packed pairs.
@@ -1326,12 +1344,13 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
   // The sweep of one row.  CARRY_IN: the row above is the previous block's carry row (waited for
   // chunk by chunk); PUBLISH: this row's vertical states are also stored as this block's carry.
   // The (1,0) path of a pixel depends on this warp's registers alone, so it is computed one step
-  // ahead, with the pixel's costs and penalty record, before the step barrier: after the barrier
-  // only the paths whose predecessor lies in the row above remain.
+  // ahead, before the step barrier: a step issues its loads first (the row above for pixel xs,
+  // the costs and record of pixel xs + 1), then the paths from the row above for xs and the (1,0)
+  // path of xs + 1 side by side, then its stores.
   struct Prepared {
-    uint32_t c[REGS];    // the pixel's widened costs
-    uint4 pw;            // its penalty record
-    PathState<REGS> h;   // its (1,0) path state
+    uint32_t c[REGS];   // the pixel's widened costs
+    uint4 pw;           // its penalty record
+    PathState<REGS> h;  // its (1,0) path state
   };
   auto sweep_row = [&](auto carry_tag, auto publish_tag) {
     constexpr bool CARRY_IN = decltype(carry_tag)::value;
@@ -1344,45 +1363,54 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
         carry_ready++;
       }
     };
-    // Costs, record and (1,0) path of the next pixel: cb = shared address of this lane's
-    // left-view cost bytes, pb = shared address of the pixel's penalty record.
-    auto prepare = [&](uint32_t cb, uint32_t pb, Prepared& n) {
-      widen_costs<REGS>(cb, cb + K * Dp, pad, n.c);
-      n.pw = lds_v4(pb);
-      const uint32_t q[1] = {horiz.m + (n.pw.x & 0x7fff7fffu)};
+    // The (1,0) path of the next pixel from its loaded cost words and record.
+    auto prepare = [&](const CostWords<REGS>& cw, const uint4& pw, Prepared& n) {
+      widen_words<REGS>(cw, pad, n.c);
+      n.pw = pw;
+      const uint32_t q[1] = {horiz.m + (pw.x & 0x7fff7fffu)};
       PathState<REGS> prev[1] = {horiz}, out[1];
       paths_step<REGS, 1>(prev, q, p1x2, n.c, lo_edge, hi_edge, out);
       n.h = out[0];
     };
-    // The rest of pixel xs (stream column) from its prepared part.
-    auto pixel = [&](int xs, const Prepared& n) {
+    // One step: pixel xs (stream column) from its prepared part `cur`, and the next pixel's
+    // prepared part from its cost bytes at ncb and record at npb (when xs + 1 < W; otherwise the
+    // addresses repeat a landed slot and the result is not used).
+    auto step = [&](int xs, const Prepared& cur, uint32_t ncb, uint32_t npb, Prepared& nx) {
       PathState<REGS> prev[NU];
       load_path<REGS>(up_a + (xs & up_mask) * L::vslot, lane_off, L::vmins, 0, prev[0]);
       if constexpr (NU > 1) {
         const uint32_t pd = xs > 0 ? up_a + ((xs - 1) & up_mask) * L::vslot : zero_a;
         load_path<REGS>(pd, lane_off, L::vmins, 1, prev[1]);
       }
+      CostWords<REGS> cw;
+      load_cost_words<REGS>(ncb, ncb + K * Dp, cw);
+      const uint4 npw = lds_v4(npb);
+      // Successors of an untextured pixel start afresh (CensusSgm.java:432-433): they see zeros.
+      const uint32_t keep = prmt(cur.pw.x, 0, 0xbb99u);
+      horiz = cur.h;
+      if (keep != 0xffffffffu) {
+#pragma unroll
+        for (int j = 0; j < REGS; j++) horiz.v[j] &= keep;
+        horiz.m &= keep;
+      }
+      prepare(cw, npw, nx);
       uint32_t q[NU];
-      q[0] = prev[0].m + n.pw.y;
-      if constexpr (NU > 1) q[1] = prev[1].m + n.pw.z;
+      q[0] = prev[0].m + cur.pw.y;
+      if constexpr (NU > 1) q[1] = prev[1].m + cur.pw.z;
       PathState<REGS> out[NU];
-      paths_step<REGS, NU>(prev, q, p1x2, n.c, lo_edge, hi_edge, out);
+      paths_step<REGS, NU>(prev, q, p1x2, cur.c, lo_edge, hi_edge, out);
       // Partial aggregate of this stream's paths.
       uint32_t s[REGS];
 #pragma unroll
       for (int j = 0; j < REGS; j++) {
-        uint32_t acc = n.h.v[j];
+        uint32_t acc = cur.h.v[j];
 #pragma unroll
         for (int i = 0; i < NU; i++) acc += out[i].v[j];
         s[j] = acc;
       }
       store_words_cs<REGS>(sum_ptr, s);
       sum_ptr += sum_step;
-      // The row below gets the states and their minima; successors of an untextured pixel start
-      // afresh (CensusSgm.java:432-433): they see zeros.
-      const uint32_t keep = prmt(n.pw.x, 0, 0xbb99u);
-      const uint32_t o = ring_a + (xs & (RING - 1)) * L::vslot;
-      PathState<REGS> h = n.h;
+      // The row below gets the states and their minima.
       if (keep != 0xffffffffu) {
 #pragma unroll
         for (int i = 0; i < NU; i++) {
@@ -1390,10 +1418,8 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
           for (int j = 0; j < REGS; j++) out[i].v[j] &= keep;
           out[i].m &= keep;
         }
-#pragma unroll
-        for (int j = 0; j < REGS; j++) h.v[j] &= keep;
-        h.m &= keep;
       }
+      const uint32_t o = ring_a + (xs & (RING - 1)) * L::vslot;
 #pragma unroll
       for (int i = 0; i < NV; i++) {
         sts_words<REGS>(o + lane_off + i * (Dp * 4), out[i].v);
@@ -1409,7 +1435,6 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
         }
       }
       if constexpr (PUBLISH) carry_ptr += L::vslot;
-      horiz = h;
     };
     // End of chunk c: refill its slot NB chunks ahead, report carry progress / release.
     auto end_chunk = [&](int c) {
@@ -1426,17 +1451,23 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
       }
       __syncwarp();
     };
-    // The first pixel of chunk c, once its copies have landed.
-    auto prepare_first = [&](int c, Prepared& n) {
+    auto wait_chunk = [&](int c) {
       if (!wait_bar(&my_full[c % NB], (c / NB) & 1, err, limit, 1)) aborted = true;
-      const uint32_t slot = slots_a + (c % NB) * L::cslot;
-      const int first = (mirror ? (chunk_n(c) - 1) * Dp : 0) + lane * REGS;
-      prepare(slot + first, slot + 2 * K * Dp, n);
     };
+    // Shared address of this lane's cost bytes of the first pixel of chunk c.
+    auto first_cost = [&](int c) {
+      return slots_a + (c % NB) * L::cslot + (mirror ? (chunk_n(c) - 1) * Dp : 0) + lane * REGS;
+    };
+    auto first_pen = [&](int c) { return slots_a + (c % NB) * L::cslot + 2 * K * Dp; };
     Prepared nx;
-    prepare_first(0, nx);
+    {
+      wait_chunk(0);
+      CostWords<REGS> cw;
+      load_cost_words<REGS>(first_cost(0), first_cost(0) + K * Dp, cw);
+      prepare(cw, lds_v4(first_pen(0)), nx);
+    }
     // Idle steps before this row starts (the 1-pixel lag behind the row above).
-    for (int step = 0; step < w; step++) rows_barrier(R * 32);
+    for (int st = 0; st < w; st++) rows_barrier(R * 32);
     const int full_chunks = W / K;
     for (int c = 0; c < full_chunks; c++) {
       if constexpr (CARRY_IN) wait_carry(c);
@@ -1444,12 +1475,19 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
 #pragma unroll
       for (int off = 0; off < K; off++) {
         const Prepared cur = nx;
-        pixel(c * K + off, cur);
-        if (off + 1 < K)
-          prepare(slot + cost_first_full + (off + 1) * cost_step, slot + 2 * K * Dp + 16 * (off + 1),
-                  nx);
-        else if (c + 1 < nchunks)
-          prepare_first(c + 1, nx);
+        uint32_t ncb, npb;
+        if (off + 1 < K) {
+          ncb = slot + cost_first_full + (off + 1) * cost_step;
+          npb = slot + 2 * K * Dp + 16 * (off + 1);
+        } else if (c + 1 < nchunks) {
+          wait_chunk(c + 1);
+          ncb = first_cost(c + 1);
+          npb = first_pen(c + 1);
+        } else {
+          ncb = slot + cost_first_full + off * cost_step;
+          npb = slot + 2 * K * Dp + 16 * off;
+        }
+        step(c * K + off, cur, ncb, npb, nx);
         rows_barrier(R * 32);
       }
       end_chunk(c);
@@ -1462,9 +1500,8 @@ __global__ void __launch_bounds__((R + 2 + LW) * 32, 1) sweep_kernel(const Sweep
       const int first = (mirror ? (n - 1) * Dp : 0) + lane * REGS;
       for (int off = 0; off < n; off++) {
         const Prepared cur = nx;
-        pixel(c * K + off, cur);
-        if (off + 1 < n)
-          prepare(slot + first + (off + 1) * cost_step, slot + 2 * K * Dp + 16 * (off + 1), nx);
+        const int nxt = off + 1 < n ? off + 1 : off;
+        step(c * K + off, cur, slot + first + nxt * cost_step, slot + 2 * K * Dp + 16 * nxt, nx);
         rows_barrier(R * 32);
       }
       end_chunk(c);
