@@ -96,18 +96,52 @@ def workload_desc(name: str, prm) -> str:
 
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region: NVML every
+    5 ms from a thread, so that even a short region has samples; nvidia-smi every 200 ms when
+    NVML cannot be loaded.  Only reads the GPU's state."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index: str):
         self.gpu = gpu_index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        if self.gpu.isdigit():
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(int(self.gpu))
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(self.gpu)
 
     def start(self):
+        try:
+            nv, handle = self._nvml_handle()
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            self.nvml = nv
+            self.stop_event = threading.Event()
+
+            def sample():
+                while not self.stop_event.is_set():
+                    sm = nv.nvmlDeviceGetClockInfo(handle, nv.NVML_CLOCK_SM)
+                    top = nv.nvmlDeviceGetMaxClockInfo(handle, nv.NVML_CLOCK_SM)
+                    reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    active = [n for n, b in zip(self.NAMES, bits) if reasons & b]
+                    self.samples.append((sm, top, active))
+                    self.stop_event.wait(0.005)
+
+            self.thread = threading.Thread(target=sample, daemon=True)
+            self.thread.start()
+            return
+        except Exception:  # NVML missing or refused: fall back to nvidia-smi
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -123,31 +157,40 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
+        if self.nvml is not None:
+            self.stop_event.set()
+            self.thread.join(timeout=2)
+            for s_mhz, top, names in self.samples:
+                sm.append(float(s_mhz))
+                smax.append(float(top))
+                reasons.update(names)
+            source = "nvml"
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower().startswith("active"):
-                    reasons.add(name)
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+            for line in self.lines:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, flag in zip(self.NAMES, parts[5:9]):
+                    if flag.lower().startswith("active"):
+                        reasons.add(name)
+            source = "nvidia-smi"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": source}
 
 
 # Bytes per cell (pixel x disparity of one pair) of the pair-level roofline model: a uint8 cost
