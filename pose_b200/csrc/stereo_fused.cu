@@ -853,25 +853,31 @@ __device__ __forceinline__ void walk_line(const LineArgs& a, int line, uint32_t 
   const int64_t p0 = (int64_t)y0 * W + x0;
   // Per lane, once per line: lanes 0 .. 2 CH - 1 copy one 16-byte chunk of a view's costs, lane
   // 31 the penalty record.  The up stream's record of pixel i sits at pen_up0 - i * step (its
-  // stream coordinates mirror the image in x and y).
+  // stream coordinates mirror the image in x and y).  Along the line every address advances by a
+  // fixed step per pixel, so the copies and stores use running pointers.
   const bool cost_lane = lane < 2 * CH;
   const uint32_t cost_dst = S::cost + (cost_lane ? (lane / CH) * Dp + (lane % CH) * 16 : 0);
   const uint8_t* cost_src =
       (cost_lane && lane >= CH ? a.cost[1] : a.cost[0]) + (cost_lane ? (lane % CH) * 16 : 0);
   const int64_t pen_up0 = ((int64_t)2 * H - 1 - y0) * W + (W - 1 - x0);
+  const int64_t cost_stride = step * Dp;  // bytes of a cost volume per pixel along the line
+  const int64_t part_stride = step * Dp;  // words of the partial per pixel along the line
 
-  // Issues the copies of pixel i into ring slot `slot` as one commit group (empty if i is off
-  // the line, so the group count stays in step).
-  auto fetch = [&](int slot, int i, bool back) {
-    const bool on = i >= 0 && i < len;
-    const int64_t p = p0 + i * step;
+  // Position of the next pixel to fetch (its copies' sources) and of the pixel being stored.
+  struct Cursor {
+    const uint8_t* cost;
+    const uint4* pen;
+    const uint32_t* part;
+  };
+  // Issues the copies of the cursor's pixel into ring slot `slot` as one commit group (empty if
+  // `on` is false, so the group count stays in step).
+  auto fetch = [&](int slot, const Cursor& f, bool on, bool back) {
     const uint32_t s = ring + slot * S::bytes;
-    cp_async16_if(s + cost_dst, cost_src + p * Dp, on && cost_lane);
-    cp_async16_if(s + S::pen, &a.pen[back ? pen_up0 - i * step : p], on && lane == 31);
+    cp_async16_if(s + cost_dst, f.cost, on && cost_lane);
+    cp_async16_if(s + S::pen, f.pen, on && lane == 31);
     if (back) {
 #pragma unroll
-      for (int c = lane; c < Dp / 4; c += 32)
-        cp_async16_if(s + S::part + c * 16, a.part + p * Dp + c * 4, on);
+      for (int c = lane; c < Dp / 4; c += 32) cp_async16_if(s + S::part + c * 16, f.part + c * 4, on);
     }
     cp_async_commit();
   };
@@ -886,70 +892,99 @@ __device__ __forceinline__ void walk_line(const LineArgs& a, int line, uint32_t 
 
   PathState<REGS> cur;
   // Forward: (-1,1), pixel i's predecessor is pixel i - 1.
-  zero_state(cur);
-#pragma unroll
-  for (int k = 0; k < kPrefetch; k++) fetch(k, k, false);
-  for (int base = 0; base < len; base += kPrefetch) {
+  {
+    zero_state(cur);
+    Cursor f{cost_src + p0 * Dp, a.pen + p0, nullptr};  // pixel 0
+    uint32_t* out_ptr = part + p0 * Dp;
+    auto advance = [&](Cursor& c) {
+      c.cost += cost_stride;
+      c.pen += step;
+    };
 #pragma unroll
     for (int k = 0; k < kPrefetch; k++) {
-      const int i = base + k;
-      if (i < len) {
-        cp_async_wait<kPrefetch - 1>();
-        __syncwarp();
-        uint32_t c[REGS], pq, pt;
-        take(k, c, pq, pt);
-        __syncwarp();  // every lane has read the slot before it is refilled
-        fetch(k, i + kPrefetch, false);
-        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
-        const uint32_t keep = prmt(pt, 0, 0xbb99u);
-        PathState<REGS> prev[1] = {cur}, out[1];
-        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
-        store_words<REGS>(part + (p0 + i * step) * Dp, out[0].v);
-        cur = out[0];
-        if (keep != 0xffffffffu) {
-#pragma unroll
-          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
-          cur.m &= keep;
-        }
-      }
+      fetch(k, f, k < len, false);
+      advance(f);
     }
+    // One pixel (ring slot k) while `i < len`.
+    auto pixel = [&](int k, int i, auto guarded) {
+      if (decltype(guarded)::value && i >= len) return;
+      cp_async_wait<kPrefetch - 1>();
+      __syncwarp();
+      uint32_t c[REGS], pq, pt;
+      take(k, c, pq, pt);
+      __syncwarp();  // every lane has read the slot before it is refilled
+      fetch(k, f, i + kPrefetch < len, false);
+      advance(f);
+      const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+      const uint32_t keep = prmt(pt, 0, 0xbb99u);
+      PathState<REGS> prev[1] = {cur}, out[1];
+      paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+      store_words<REGS>(out_ptr, out[0].v);
+      out_ptr += part_stride;
+      cur = out[0];
+      if (keep != 0xffffffffu) {
+#pragma unroll
+        for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+        cur.m &= keep;
+      }
+    };
+    for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+      for (int k = 0; k < kPrefetch; k++) pixel(k, base + k, std::true_type{});
+    }
+    cp_async_wait<0>();
   }
-  cp_async_wait<0>();
   // The return pass copies the stored forward costs back from L2 (cp.async.cg), some of them
   // written by other lanes just now: every lane's stores reach L2 before any lane copies.
   __threadfence();
   __syncwarp();
   // Backward: (1,-1), pixel i's predecessor is pixel i + 1; adds to the stored forward costs.
-  zero_state(cur);
-#pragma unroll
-  for (int k = 0; k < kPrefetch; k++) fetch(k, len - 1 - k, true);
-  for (int base = 0; base < len; base += kPrefetch) {
+  {
+    zero_state(cur);
+    const int64_t pl = p0 + (int64_t)(len - 1) * step;  // pixel len - 1
+    Cursor f{cost_src + pl * Dp, a.pen + (pen_up0 - (int64_t)(len - 1) * step),
+             a.part + pl * Dp};
+    uint32_t* out_ptr = part + pl * Dp;
+    auto advance = [&](Cursor& c) {
+      c.cost -= cost_stride;
+      c.pen += step;
+      c.part -= part_stride;
+    };
 #pragma unroll
     for (int k = 0; k < kPrefetch; k++) {
-      const int i = len - 1 - (base + k);
-      if (i >= 0) {
-        cp_async_wait<kPrefetch - 1>();
-        __syncwarp();
-        uint32_t c[REGS], pq, pt, fwd[REGS];
-        take(k, c, pq, pt);
-        lds_words<REGS>(ring + k * S::bytes + S::part + lane * REGS * 4, fwd);
-        __syncwarp();
-        fetch(k, i - kPrefetch, true);
-        const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
-        const uint32_t keep = prmt(pt, 0, 0xbb99u);
-        PathState<REGS> prev[1] = {cur}, out[1];
-        paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
-        uint32_t sum[REGS];
+      fetch(k, f, k < len, true);
+      advance(f);
+    }
+    // Pixel len - 1 - n (ring slot k), the n-th of the pass.
+    auto pixel = [&](int k, int n, auto guarded) {
+      if (decltype(guarded)::value && n >= len) return;
+      cp_async_wait<kPrefetch - 1>();
+      __syncwarp();
+      uint32_t c[REGS], pq, pt, fwd[REGS];
+      take(k, c, pq, pt);
+      lds_words<REGS>(ring + k * S::bytes + S::part + lane * REGS * 4, fwd);
+      __syncwarp();
+      fetch(k, f, n + kPrefetch < len, true);
+      advance(f);
+      const uint32_t q[1] = {cur.m + (pq & 0x7fff7fffu)};
+      const uint32_t keep = prmt(pt, 0, 0xbb99u);
+      PathState<REGS> prev[1] = {cur}, out[1];
+      paths_step<REGS, 1>(prev, q, p1x2, c, lo_edge, hi_edge, out);
+      uint32_t sum[REGS];
 #pragma unroll
-        for (int j = 0; j < REGS; j++) sum[j] = fwd[j] + out[0].v[j];
-        store_words_cs<REGS>(part + (p0 + i * step) * Dp, sum);
-        cur = out[0];
-        if (keep != 0xffffffffu) {
+      for (int j = 0; j < REGS; j++) sum[j] = fwd[j] + out[0].v[j];
+      store_words_cs<REGS>(out_ptr, sum);
+      out_ptr -= part_stride;
+      cur = out[0];
+      if (keep != 0xffffffffu) {
 #pragma unroll
-          for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
-          cur.m &= keep;
-        }
+        for (int j = 0; j < REGS; j++) cur.v[j] &= keep;
+        cur.m &= keep;
       }
+    };
+    for (int base = 0; base < len; base += kPrefetch) {
+#pragma unroll
+      for (int k = 0; k < kPrefetch; k++) pixel(k, base + k, std::true_type{});
     }
   }
   cp_async_wait<0>();
