@@ -166,10 +166,28 @@ int csgm_session_set_budget(csgm_session* session, int64_t bytes);
 #define CSGM_SGM_AUTO 0
 #define CSGM_SGM_RESIDENT 1
 #define CSGM_SGM_STREAMED 2
+/* Compact SGM, the reference's --gpu-sgm esgm (src/main/java/sgm/GpuCandidateStereo.java:53-167):
+ * grayscale Census with 16-bit aggregates, no cost volume and no aggregate volume.  Every path
+ * proposes a few separated disparities per pixel (csgm_session_set_candidates); the exact
+ * aggregate at each proposal and its two neighbours and a lower bound of it elsewhere certify most
+ * pixels' outcomes, and the others are aggregated exactly over every disparity.  Results are
+ * bit-identical to the resident views; the winners records of certified pixels hold the best
+ * known second value instead of the exact one. */
+#define CSGM_SGM_COMPACT 3
 
 /* mode: CSGM_SGM_*; strip_rows: the largest strip height (Options.gpuStripRows, 0 = 64), halved
  * until a strip fits the budget (GpuStereo.plan, src/main/java/sgm/GpuStereo.java:59-62). */
 int csgm_session_set_streaming(csgm_session* session, int32_t mode, int32_t strip_rows);
+
+/* Options.esgmCandidates (src/main/java/sgm/Options.java:35,244,781): the separated proposals each
+ * path keeps per pixel in compact SGM, 1..4 (default 2); the plan lowers it until it fits. */
+int csgm_session_set_candidates(csgm_session* session, int32_t per_path);
+
+/* Compact SGM's outcome for the session's last view of each side (reverse 0 = left, 1 = right):
+ * the pixels its proposals certified and those it aggregated exactly (the reference's
+ * esgm_left/right report, GpuCandidateStereo.java:106-131). */
+int csgm_session_compact_report(csgm_session* session, int32_t reverse, int64_t* certified,
+                                int64_t* verified);
 
 /* Device bytes csgm_pair needs for a w x h pair under the session's budget and streaming mode;
  * CSGM_E_NOMEM if no plan fits.  Replaces GpuStereo.plan (src/main/java/sgm/GpuStereo.java:33-84). */

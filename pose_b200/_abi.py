@@ -25,7 +25,9 @@ CSGM_E_UNSUPPORTED = -7
 CSGM_SGM_AUTO = 0
 CSGM_SGM_RESIDENT = 1
 CSGM_SGM_STREAMED = 2
-SGM_MODES = {"auto": CSGM_SGM_AUTO, "resident": CSGM_SGM_RESIDENT, "streamed": CSGM_SGM_STREAMED}
+CSGM_SGM_COMPACT = 3
+SGM_MODES = {"auto": CSGM_SGM_AUTO, "resident": CSGM_SGM_RESIDENT, "streamed": CSGM_SGM_STREAMED,
+             "esgm": CSGM_SGM_COMPACT}
 
 STATUS_NAMES = {
     CSGM_E_INVALID: "CSGM_E_INVALID",
@@ -170,6 +172,9 @@ SIGNATURES = {
     "csgm_session_close": (None, [_P]),
     "csgm_session_set_budget": (ctypes.c_int, [_P, _I64]),
     "csgm_session_set_streaming": (ctypes.c_int, [_P, _I32, _I32]),
+    "csgm_session_set_candidates": (ctypes.c_int, [_P, _I32]),
+    "csgm_session_compact_report": (
+        ctypes.c_int, [_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "csgm_plan_detail": (
         ctypes.c_int,
         [_P, ctypes.POINTER(CsgmParams), _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I64),

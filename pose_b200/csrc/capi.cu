@@ -155,6 +155,8 @@ void session_settings(Context& ctx, csgm_session* s, const csgm_params& p, int w
   ctx.wait_limit = s->wait_limit;
   ctx.sgm_mode = s->sgm_mode;
   ctx.strip_rows = s->strip_rows;
+  ctx.candidates = s->candidates;
+  ctx.compact_report = s->compact_report;
   ctx.host_partial = &s->host_partial;
   if (s->tuning_forced)
     ctx.tuning = s->forced_tuning;
@@ -318,11 +320,29 @@ int csgm_session_set_wait_limit(csgm_session* s, int64_t cycles) {
 }
 
 int csgm_session_set_streaming(csgm_session* s, int32_t mode, int32_t strip_rows) {
-  if (!s || mode < CSGM_SGM_AUTO || mode > CSGM_SGM_STREAMED || strip_rows < 0)
+  if (!s || mode < CSGM_SGM_AUTO || mode > CSGM_SGM_COMPACT || strip_rows < 0)
     return fail(CSGM_E_INVALID, "invalid session, streaming mode or strip height");
   std::lock_guard<std::mutex> guard(s->lock);
   s->sgm_mode = mode;
   s->strip_rows = strip_rows ? strip_rows : 64;  // Options.gpuStripRows default
+  return CSGM_OK;
+}
+
+int csgm_session_set_candidates(csgm_session* s, int32_t per_path) {
+  // Options.java:781-782.
+  if (!s) return fail(CSGM_E_INVALID, "NULL session");
+  if (per_path < 1 || per_path > 4) return fail(CSGM_E_INVALID, "--esgm-candidates must be 1..4");
+  std::lock_guard<std::mutex> guard(s->lock);
+  s->candidates = per_path;
+  return CSGM_OK;
+}
+
+int csgm_session_compact_report(csgm_session* s, int32_t reverse, int64_t* certified,
+                                int64_t* verified) {
+  if (!s || (reverse != 0 && reverse != 1)) return fail(CSGM_E_INVALID, "invalid session or view");
+  std::lock_guard<std::mutex> guard(s->lock);
+  if (certified) *certified = s->compact_report[2 * reverse];
+  if (verified) *verified = s->compact_report[2 * reverse + 1];
   return CSGM_OK;
 }
 

@@ -70,12 +70,45 @@ static size_t strip_bytes(const csgm_params& p, int w, int rows) {
   return cells * (2 + p.aggregate_bytes) + carry + 4 * 256;
 }
 
+// Device bytes of compact SGM besides `fixed`: proposals and compact aggregates (8 bytes per
+// proposal and pixel), the lower bounds, the unresolved slots and list, and one image row of exact
+// aggregates and cost rows (the least chunk of the exact pass).
+static size_t compact_bytes(const csgm_params& p, int w, int h, int pool) {
+  const size_t n = (size_t)w * h, C = (size_t)p.directions * pool;
+  return n * (C * 8 + 2 + 8) + 16 + (size_t)w * p.disparities * 4;
+}
+
+// GpuCandidateStereo.plan (GpuCandidateStereo.java:20-47): grayscale Census with 16-bit
+// aggregates only; the proposals per path start at the session's count and drop until the
+// compact buffers fit the budget.
+static int compact_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
+                        ViewPlan* plan) {
+  if (p.cost_mode != CSGM_COST_CENSUS || p.aggregate_bytes != 2)
+    return fail(CSGM_E_INVALID, "compact SGM needs grayscale Census with 16-bit aggregates");
+  for (int pool = ctx.candidates; pool >= 1; pool--) {
+    const size_t bytes = fixed + compact_bytes(p, w, h, pool);
+    if (bytes <= ctx.ws->budget) {
+      plan->streamed = false;
+      plan->compact = true;
+      plan->pool = pool;
+      plan->rows = h;
+      plan->device_bytes = bytes;
+      plan->host_bytes = 0;
+      return CSGM_OK;
+    }
+  }
+  return fail(CSGM_E_NOMEM,
+              "No compact Census/16-bit GPU plan fits: needs %.1f MiB, budget %.1f MiB",
+              (fixed + compact_bytes(p, w, h, 1)) / 1048576.0, ctx.ws->budget / 1048576.0);
+}
+
 // GpuStereo.plan (GpuStereo.java:33-84): resident when the whole volume fits the budget (unless
 // streaming is forced), else strips whose height starts at the session's strip height and halves
 // until one fits.  Strips are at least two rows high with 16 paths, so that a (+-1,+-2) path's
 // predecessor always lies in the previous strip.
 static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
                        size_t resident, ViewPlan* plan) {
+  if (ctx.sgm_mode == CSGM_SGM_COMPACT) return compact_plan(ctx, p, w, h, fixed, plan);
   const size_t budget = ctx.ws->budget;
   if (ctx.sgm_mode != CSGM_SGM_STREAMED && resident <= budget) {
     plan->streamed = false;
@@ -107,6 +140,8 @@ static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, s
 
 int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_inputs,
               ViewPlan* plan, bool color) {
+  if (color && ctx.sgm_mode == CSGM_SGM_COMPACT)
+    return fail(CSGM_E_INVALID, "compact SGM needs grayscale Census with 16-bit aggregates");
   return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs, color),
                      pair_workspace_bytes(p, w, h, host_inputs, color, ctx.tuning), plan);
 }
@@ -161,6 +196,100 @@ static int run_view_general(Context& ctx, const csgm_params& p, const uint64_t* 
   ctx.prof->kernel_begin();
   CK(launch_winners(s, sum, p.aggregate_bytes, ctx.sm_count, ctx.stream), "winners kernel launch");
   ctx.prof->kernel_end("winners");
+  return CSGM_OK;
+}
+
+// One view through compact SGM (GpuCandidateStereo.execute, GpuCandidateStereo.java:53-167):
+// every direction's proposals, then every direction's compact aggregates and lower bounds, then
+// the selection of the certified pixels and the list of the others.  The listed pixels are then
+// aggregated exactly, every path walked again with only their rows kept, in chunks that fit the
+// budget, and selected from their full aggregates.
+static int run_view_compact(Context& ctx, const csgm_params& p, int pool, const uint64_t* desc_a,
+                            const uint64_t* desc_b, const uint8_t* tex_a, const uint8_t* tex_b,
+                            const uint8_t* gray_a, const uint8_t* gray_b, int w, int h,
+                            int reverse, float* out, int32_t* summary, uint8_t* reasons,
+                            uint8_t* boundary, DeviceStats* dstats) {
+  int status = CSGM_OK;
+  const size_t n = (size_t)w * h, D = (size_t)p.disparities;
+  const int C = p.directions * pool;
+  WS(cand, uint16_t, kEsgmCand, n * C * 2);
+  WS(compact, uint16_t, kEsgmCompact, n * C * 6);
+  WS(outside, uint16_t, kEsgmOutside, n * 2);
+  WS(slots, int32_t, kEsgmSlots, n * 4);
+  WS(pixels, int32_t, kEsgmPixels, n * 4);
+  WS(count, int32_t, kEsgmCount, 16);
+  CostArgs c{desc_a, desc_b, tex_a, tex_b, gray_a, gray_b, nullptr, w, h, p.disparities,
+             p.min_disparity, reverse, p.window_x, p.window_y, words_of(p), p.cost_mode,
+             p.census_weight_milli, p.ad_truncation, p.gradient_truncation,
+             p.window_x * p.window_y - 1};
+  CK(cudaMemsetAsync(compact, 0, n * C * 6, ctx.stream), "compact clear");
+  CK(cudaMemsetAsync(outside, 0, n * 2, ctx.stream), "bound clear");
+  CK(cudaMemsetAsync(count, 0, 16, ctx.stream), "count clear");
+  EsgmArgs e{c, 0, 0, p.p1, p.p2, p.edge_scale, cand, compact, outside, C, 0, pool, slots,
+             nullptr};
+  for (int phase = 0; phase < 2; phase++)
+    for (int d = 0; d < p.directions; d++) {
+      direction(d, e.dx, e.dy);
+      e.direction = d;
+      ctx.prof->kernel_begin();
+      CK(launch_esgm_paths(e, phase, ctx.sm_count, ctx.stream), "compact path kernel launch");
+      ctx.prof->kernel_end(phase == 0 ? "esgm_proposals" : "esgm_compact");
+    }
+  SelectArgs s{nullptr, out, summary, reasons, boundary, dstats, w, h, p.disparities,
+               p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+  EsgmSelectArgs sel{c, cand, compact, outside, s, C, slots, pixels, count};
+  ctx.prof->kernel_begin();
+  CK(launch_esgm_select(sel, ctx.sm_count, ctx.stream), "compact select kernel launch");
+  ctx.prof->kernel_end("esgm_select");
+  int32_t unresolved = 0;
+  CK(cudaMemcpyAsync(&unresolved, count, 4, cudaMemcpyDeviceToHost, ctx.stream),
+     "unresolved count readback");
+  CK(cudaStreamSynchronize(ctx.stream), "compact SGM proposals");
+  if (ctx.compact_report) {
+    ctx.compact_report[2 * reverse] = (int64_t)n - unresolved;
+    ctx.compact_report[2 * reverse + 1] = unresolved;
+  }
+  if (unresolved == 0) return CSGM_OK;
+  // Exact pass in chunks of listed pixels: each chunk's aggregates and cost rows (4 bytes per
+  // disparity and pixel) within what the budget leaves.
+  const Workspace& ws = *ctx.ws;
+  const size_t held = ws.buffers[kEsgmSum].bytes + ws.buffers[kEsgmCost].bytes;
+  const size_t room = ws.budget > ws.allocated - held ? ws.budget - (ws.allocated - held) : 0;
+  const int64_t chunk = std::min<int64_t>(unresolved, (int64_t)(room / (4 * D)));
+  if (chunk < 1)
+    return fail(CSGM_E_NOMEM, "compact SGM's exact pass exceeds the device budget");
+  WS(sum, uint16_t, kEsgmSum, (size_t)chunk * D * 2);
+  WS(cost, uint16_t, kEsgmCost, (size_t)chunk * D * 2);
+  for (int64_t lo = 0; lo < unresolved; lo += chunk) {
+    const int64_t rows = std::min<int64_t>(chunk, unresolved - lo);
+    CK(cudaMemsetAsync(sum, 0, (size_t)rows * D * 2, ctx.stream), "exact aggregate clear");
+    EsgmArgs x = e;
+    x.slots = slots;
+    x.sum = sum;
+    x.slot_lo = (int32_t)lo;
+    x.slot_hi = (int32_t)(lo + rows);
+    for (int d = 0; d < p.directions; d++) {
+      direction(d, x.dx, x.dy);
+      x.direction = d;
+      ctx.prof->kernel_begin();
+      CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
+      ctx.prof->kernel_end("esgm_exact");
+    }
+    CostArgs cr = c;
+    cr.out = cost;
+    cr.pixels = pixels + lo;
+    cr.npixels = (int)rows;
+    ctx.prof->kernel_begin();
+    CK(launch_cost_volume(cr, ctx.sm_count, ctx.stream), "cost kernel launch");
+    ctx.prof->kernel_end("cost_volume");
+    SelectArgs sw = s;
+    sw.cost = cost;
+    sw.pixels = pixels + lo;
+    sw.npixels = (int)rows;
+    ctx.prof->kernel_begin();
+    CK(launch_winners(sw, sum, 2, ctx.sm_count, ctx.stream), "winners kernel launch");
+    ctx.prof->kernel_end("winners");
+  }
   return CSGM_OK;
 }
 
@@ -339,6 +468,13 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
     status = run_view_streamed(ctx, p, desc_r, desc_l, tex_r, tex_l, right, left, w, h, 1, disp_r,
                                nullptr, nullptr, nullptr, nullptr, plan.rows);
     if (status) return status;
+  } else if (plan.compact) {
+    status = run_view_compact(ctx, p, plan.pool, desc_l, desc_r, tex_l, tex_r, left, right, w, h,
+                              0, disp_l, nullptr, reasons, boundary, dstats);
+    if (status) return status;
+    status = run_view_compact(ctx, p, plan.pool, desc_r, desc_l, tex_r, tex_l, right, left, w, h,
+                              1, disp_r, nullptr, nullptr, nullptr, nullptr);
+    if (status) return status;
   } else if (use_fused(p, h)) {
     // Both views in one pass structure (stereo_fused.cu).
     FusedViews v{desc_l,           desc_r,           tex_l,          tex_r,
@@ -390,6 +526,8 @@ int run_pair_device(Context& ctx, const csgm_params& p, const uint8_t* left, con
   if (status) return status;
   if (plan.streamed && !sync)
     return fail(CSGM_E_INVALID, "a streamed pair needs sync != 0 (its strips use host memory)");
+  if (plan.compact && !sync)
+    return fail(CSGM_E_INVALID, "a compact SGM pair needs sync != 0 (it reads back its count)");
   return pair_on_device(ctx, p, plan, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
                         disp_r, reasons, boundary, stats, sync, true);
 }
@@ -408,7 +546,7 @@ int run_pair_device_graph(Context& ctx, GraphCache& cache, const csgm_params& p,
   ViewPlan plan;
   int status = plan_pair(ctx, p, w, h, false, &plan);
   if (status) return status;
-  if (plan.streamed)  // strips copy through host memory: not captured
+  if (plan.streamed || plan.compact)  // host copies and a count readback: not captured
     return run_pair_device(ctx, p, left, right, valid_l, valid_r, w, h, lr_checked, disp_l,
                            disp_r, reasons, boundary, stats, sync);
   // The key: everything the captured work depends on.
@@ -834,6 +972,9 @@ static int run_match_general(Context& ctx, const csgm_params& p, const ViewPlan&
   if (plan.streamed)
     status = run_view_streamed(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
                                d_summary, d_reasons, d_boundary, dstats, plan.rows);
+  else if (plan.compact)
+    status = run_view_compact(ctx, p, plan.pool, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse,
+                              d_out, d_summary, d_reasons, d_boundary, dstats);
   else
     status = run_view_general(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
                               d_summary, d_reasons, d_boundary, dstats);
@@ -861,7 +1002,8 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
   // Resident on the fused kernels when they apply and their workspace fits the budget, else
   // resident on the general ones, else streamed (as the session's mode allows).
   const bool summary = out_summary != nullptr;
-  if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && use_fused(p, h) &&
+  if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && ctx.sgm_mode != CSGM_SGM_COMPACT &&
+      use_fused(p, h) &&
       match_fused_bytes(p, w, h, summary, ctx.tuning) <= ctx.ws->budget)
     return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                            out_disp, out_summary, reasons, boundary, stats);

@@ -26,7 +26,11 @@ enum Slot {
   // l/r in the pair's order), per-view outputs, the comparison flag.
   kMatchIn0, kMatchIn1 = kMatchIn0 + 6, kMatchDisp = kMatchIn1 + 6, kMatchReasons = kMatchDisp + 2,
   kMatchBoundary = kMatchReasons + 2, kMatchSummary = kMatchBoundary + 2,
-  kMatchStats = kMatchSummary + 2, kMatchEqual, kSlotCount
+  kMatchStats = kMatchSummary + 2, kMatchEqual,
+  // Compact SGM: proposals, compact aggregates, lower bounds, the unresolved pixels and their
+  // exact aggregates and cost rows.
+  kEsgmCand, kEsgmCompact, kEsgmOutside, kEsgmSlots, kEsgmPixels, kEsgmCount, kEsgmSum, kEsgmCost,
+  kSlotCount
 };
 
 // Pinned host memory that a session grows on demand (the streamed down pass parks its partial
@@ -81,6 +85,8 @@ struct TuningTable {
 // they apply, else the general ones) or streamed through strips of `rows` rows (general kernels).
 struct ViewPlan {
   bool streamed = false;
+  bool compact = false;       // compact SGM (CSGM_SGM_COMPACT)
+  int pool = 0;               // its proposals per path
   int rows = 0;               // strip height (the image height when resident)
   size_t device_bytes = 0;    // device memory of the plan
   size_t host_bytes = 0;      // pinned host memory of the plan
@@ -167,6 +173,9 @@ struct Context {
   // Options.gpuSgm (CSGM_SGM_*) and Options.gpuStripRows: resident or streamed views.
   int sgm_mode = CSGM_SGM_AUTO;
   int strip_rows = 64;
+  int candidates = 2;  // Options.esgmCandidates
+  // Compact SGM's last outcome per view (reverse 0/1): certified pixels, pixels verified exactly.
+  int64_t* compact_report = nullptr;
   HostBuffer* host_partial = nullptr;  // null: streaming unavailable (batch slots)
   // Launch shape of the fused sweep for this call (from the session's tuning table).
   SweepTuning tuning;
@@ -253,6 +262,8 @@ struct csgm_session {
   csgm::MatchTwin twin;    // csgm_match's held view
   int sgm_mode = CSGM_SGM_AUTO;  // csgm_session_set_streaming
   int strip_rows = 64;
+  int candidates = 2;             // csgm_session_set_candidates
+  int64_t compact_report[4] = {0, 0, 0, 0};
   csgm::HostBuffer host_partial;
   csgm::TuningTable tuning;  // csgm_autotune / csgm_session_load_tuning
   bool graphs = false;       // csgm_session_set_graphs

@@ -72,31 +72,32 @@ __global__ void __launch_bounds__(kCensusBx * kCensusBy) census_texture_kernel(C
 }
 
 // One cost cell per thread-lane: a warp covers one pixel's disparities (coalesced uint16 stores).
+// The cost of pixel (x, y) at disparity index k: 512 when the pixel or its target lies within the
+// census window's half-size of the border or is untextured, else StereoCost.value.
+__device__ __forceinline__ int cost_at(const CostArgs& a, int x, int y, int k, int64_t n) {
+  const int rx = a.wx / 2, ry = a.wy / 2, w = a.w;
+  const int64_t p = (int64_t)y * w + x;
+  if (!(x >= rx && x < w - rx && y >= ry && y < a.h - ry && a.tex_a[p])) return kInvalidCost;
+  const long long disparity = (long long)a.min_disparity + k;
+  const long long target = (long long)x + (a.reverse ? disparity : -disparity);
+  if (target < rx || target >= w - rx) return kInvalidCost;
+  const int64_t q = (int64_t)y * w + target;
+  return a.tex_b[q] ? cell_cost(a, p, q, n) : kInvalidCost;
+}
+
 __global__ void cost_volume_kernel(CostArgs a) {
   int w = a.w, h = a.h, D = a.D;
   int64_t n = (int64_t)w * h;
-  int rx = a.wx / 2, ry = a.wy / 2;
   int lane = threadIdx.x & 31;
   int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t first = (int64_t)a.y0 * w, count = a.rows ? (int64_t)a.rows * w : n;
+  const int64_t first = (int64_t)a.y0 * w;
+  const int64_t count = a.pixels ? a.npixels : a.rows ? (int64_t)a.rows * w : n;
   for (int64_t local = warp; local < count; local += warps) {
-    const int64_t p = first + local;
-    int x = (int)(p % w), y = (int)(p / w);
-    bool inside = x >= rx && x < w - rx && y >= ry && y < h - ry && a.tex_a[p];
+    const int64_t p = a.pixels ? a.pixels[local] : first + local;
+    const int x = (int)(p % w), y = (int)(p / w);
     uint16_t* out = a.out + local * D;
-    for (int k = lane; k < D; k += 32) {
-      int value = kInvalidCost;
-      if (inside) {
-        long long disparity = (long long)a.min_disparity + k;
-        long long target = (long long)x + (a.reverse ? disparity : -disparity);
-        if (target >= rx && target < w - rx) {
-          int64_t q = (int64_t)y * w + target;
-          if (a.tex_b[q]) value = cell_cost(a, p, q, n);
-        }
-      }
-      out[k] = (uint16_t)value;
-    }
+    for (int k = lane; k < D; k += 32) out[k] = (uint16_t)cost_at(a, x, y, k, n);
   }
 }
 
@@ -177,6 +178,112 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Compact SGM (GpuCandidateStereo.java:53-167, the path kernel hooks :401-479).  One warp per line
+// as in paths_line_kernel, each pixel's costs computed from the descriptors (no cost volume); at
+// every pixel, after the path state L:
+//  PHASE 0: `pool` separated proposals of the path: the valid disparity of least L (ties: the
+//   smaller), then the least among those more than one away from every proposal so far;
+//  PHASE 1 (all directions' proposals known): L at every proposal - 1, proposal, proposal + 1 is
+//   added to the pixel's compact aggregates, and the least L over the valid disparities no
+//   proposal covers (within one) to the pixel's lower bound of the aggregate there;
+//  PHASE 2 (exact pass): L is added to the full aggregate row of each listed pixel.
+// The directions run one after another, so every read-modify-write of a pixel is ordered.
+template <int PHASE>
+__global__ void esgm_paths_kernel(EsgmArgs a) {
+  extern __shared__ int smem[];
+  const CostArgs& ca = a.cost;
+  const int D = ca.D, w = ca.w, h = ca.h, C = a.C;
+  const int64_t n = (int64_t)w * h;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  int* prev = smem + (size_t)warp * 3 * D;
+  int* cur = prev + D;
+  int* cost = cur + D;
+  int* props = smem + (size_t)warps * 3 * D + (size_t)warp * C;  // PHASE 1: the proposals
+  const int64_t lines = line_count(w, h, a.dx, a.dy);
+  for (int64_t line = (int64_t)blockIdx.x * warps + warp; line < lines;
+       line += (int64_t)gridDim.x * warps) {
+    int x, y;
+    line_start(line, w, h, a.dx, a.dy, x, y);
+    int64_t prev_p = -1;
+    while (x >= 0 && x < w && y >= 0 && y < h) {
+      const int64_t p = (int64_t)y * w + x;
+      const bool has = prev_p >= 0 && ca.tex_a[prev_p];
+      int minimum = 0, local_p2 = a.p2;
+      if (has) {
+        int m = INT_MAX;
+        for (int k = lane; k < D; k += 32) m = min(m, prev[k]);
+        minimum = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
+        local_p2 = path_p2(a.p1, a.p2, a.edge_scale, ca.gray_a[p], ca.gray_a[prev_p]);
+      }
+      for (int k = lane; k < D; k += 32) {
+        const int c = cost_at(ca, x, y, k, n);
+        int v = c;
+        if (has) {
+          int t = min(prev[k], minimum + local_p2);
+          if (k > 0) t = min(t, prev[k - 1] + a.p1);
+          if (k + 1 < D) t = min(t, prev[k + 1] + a.p1);
+          v += t - minimum;
+        }
+        cur[k] = v;
+        cost[k] = c;
+      }
+      __syncwarp();
+      if constexpr (PHASE == 0) {
+        int chosen[4] = {65535, 65535, 65535, 65535};
+        for (int choice = 0; choice < a.pool; choice++) {
+          unsigned key = 0x7fffffffu;
+          for (int k = lane; k < D; k += 32)
+            if (cost[k] != kInvalidCost) {
+              bool eligible = true;
+              for (int j = 0; j < choice; j++) eligible &= abs(k - chosen[j]) > 1;
+              if (eligible) key = min(key, (unsigned)(cur[k] * (D + 1) + k));
+            }
+          key = __reduce_min_sync(0xffffffffu, key);
+          chosen[choice] = key == 0x7fffffffu ? 65535 : (int)(key % (unsigned)(D + 1));
+          if (lane == 0) a.cand[p * C + a.direction * a.pool + choice] = (uint16_t)chosen[choice];
+        }
+      } else if constexpr (PHASE == 1) {
+        for (int j = lane; j < C; j += 32) props[j] = a.cand[p * C + j];
+        __syncwarp();
+        for (int j = lane; j < 3 * C; j += 32) {
+          const int k = props[j / 3] + j % 3 - 1;
+          if (k >= 0 && k < D) {
+            uint16_t* at = a.compact + p * C * 3 + j;
+            *at = (uint16_t)(*at + cur[k]);
+          }
+        }
+        unsigned lower = 0x7fffffffu;
+        for (int k = lane; k < D; k += 32)
+          if (cost[k] != kInvalidCost) {
+            bool covered = false;
+            for (int j = 0; j < C; j++) covered |= abs(k - props[j]) <= 1;
+            if (!covered) lower = min(lower, (unsigned)cur[k]);
+          }
+        lower = __reduce_min_sync(0xffffffffu, lower);
+        if (lane == 0)
+          a.outside[p] = lower == 0x7fffffffu
+                             ? (uint16_t)65535
+                             : (uint16_t)min(65535u, (unsigned)a.outside[p] + lower);
+      } else {
+        const int slot = a.slots[p];
+        if (slot >= a.slot_lo && slot < a.slot_hi) {
+          uint16_t* s = a.sum + (int64_t)(slot - a.slot_lo) * D;
+          for (int k = lane; k < D; k += 32) s[k] = (uint16_t)(s[k] + cur[k]);
+        }
+      }
+      __syncwarp();
+      int* swap = prev;
+      prev = cur;
+      cur = swap;
+      prev_p = p;
+      x += a.dx;
+      y += a.dy;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Winner selection (CensusSgm.java:460-515) with the winners record of GpuStereo.java:758-769
 // and the arithmetic of the host select (GpuStereo.java:644-686).  One warp per pixel.
 __device__ void select_pixel(const SelectArgs& a, int64_t p, int best, int value, int second,
@@ -230,9 +337,11 @@ __global__ void winners_kernel(SelectArgs a, const SumT* __restrict__ sum) {
   int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long counts[6] = {0, 0, 0, 0, 0, 0};
-  const int64_t first = (int64_t)a.y0 * w, count = a.rows ? (int64_t)a.rows * w : n;
+  const int64_t first = (int64_t)a.y0 * w;
+  const int64_t count = a.pixels ? a.npixels : a.rows ? (int64_t)a.rows * w : n;
   for (int64_t local = warp; local < count; local += warps) {
-    const int64_t p = first + local;
+    // A listed pixel (compact SGM's exact pass) has its cost and sum in row `local`.
+    const int64_t p = a.pixels ? a.pixels[local] : first + local;
     int x = (int)(p % w), y = (int)(p / w);
     const uint16_t* c = a.cost + local * D;
     const SumT* s = sum + local * D;
@@ -279,6 +388,89 @@ __global__ void winners_kernel(SelectArgs a, const SumT* __restrict__ sum) {
     if (counts[3]) atomicAdd(&a.stats->upper_boundary_rejected, counts[3]);
     if (counts[4]) atomicAdd(&a.stats->ambiguity_rejected, counts[4]);
     if (counts[5]) atomicAdd(&a.stats->selected, counts[5]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Compact SGM selection (the esgm_select kernel, GpuCandidateStereo.java:448-478, and the
+// certification of execute, :78-100).  A thread per pixel: the winners record from the compact
+// aggregates (best = least aggregate over the proposals, ties to the smaller disparity; before /
+// after its neighbours; second the least over the compact cells more than one away), then the
+// outcome is certified when the lower bound elsewhere exceeds the best and every known other
+// aggregate does, and the uniqueness test is decided either way by the known values.  A certified
+// pixel is selected at once; the others are listed for the exact pass.
+__global__ void esgm_select_kernel(EsgmSelectArgs a) {
+  const SelectArgs& s = a.sel;
+  const int w = s.w, h = s.h, D = s.D, C = a.C, rx = s.wx / 2, ry = s.wy / 2;
+  const int64_t n = (int64_t)w * h;
+  unsigned long long counts[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(p % w), y = (int)(p / w);
+    auto valid = [&](int k) {
+      return k >= 0 && k < D && cost_at(a.cost, x, y, k, n) != kInvalidCost;
+    };
+    const uint16_t* cand = a.cand + p * C;
+    const uint16_t* compact = a.compact + p * C * 3;
+    int best = -1, value = INT_MAX, second = INT_MAX, before = -1, after = -1, owner = -1;
+    for (int j = 0; j < C; j++) {
+      const int k = cand[j], v = compact[3 * j + 1];
+      if (k < D && (v < value || (v == value && (best < 0 || k < best)))) {
+        best = k;
+        value = v;
+        owner = j;
+      }
+    }
+    if (owner >= 0) {
+      if (valid(best - 1)) before = compact[3 * owner];
+      if (valid(best + 1)) after = compact[3 * owner + 2];
+      for (int j = 0; j < 3 * C; j++) {
+        const int k = (int)cand[j / 3] + j % 3 - 1;
+        if (abs(k - best) > 1 && valid(k)) second = min(second, (int)compact[j]);
+      }
+    }
+    const int flags = (valid(0) ? 1 : 0) | (valid(D - 1) ? 2 : 0);
+    bool trusted = true;
+    if (best >= 0) {
+      const long long lower = a.outside[p];
+      const bool winner = lower > value && (before < 0 || before > value) &&
+                          (after < 0 || after > value) && second > value;
+      const double margin = fmax(1.0, value * s.uniqueness);
+      trusted = winner && (best == 0 || best == D - 1 || (double)second - (double)value <= margin ||
+                           (double)(lower - value) > margin);
+    }
+    s.out[p] = __int_as_float(0x7fc00000);
+    if (trusted) {
+      a.slots[p] = -1;
+      if (s.summary) {
+        int32_t* r = s.summary + 6 * p;
+        r[0] = best;
+        r[1] = value;
+        r[2] = second;
+        r[3] = before;
+        r[4] = after;
+        r[5] = flags;
+      }
+      if (x >= rx && x < w - rx && y >= ry && y < h - ry)
+        select_pixel(s, p, best, value, second, before, after, flags, counts);
+    } else {
+      const int slot = atomicAdd(a.count, 1);
+      a.slots[p] = slot;
+      a.pixels[slot] = (int32_t)p;
+    }
+  }
+  if (s.stats) {
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+      for (int o = 16; o > 0; o /= 2) counts[i] += __shfl_down_sync(0xffffffffu, counts[i], o);
+    if ((threadIdx.x & 31) == 0) {
+      if (counts[0]) atomicAdd(&s.stats->lower_boundary_rejected, counts[0]);
+      if (counts[1]) atomicAdd(&s.stats->full_interval_pixels, counts[1]);
+      if (counts[2]) atomicAdd(&s.stats->boundary_rejected, counts[2]);
+      if (counts[3]) atomicAdd(&s.stats->upper_boundary_rejected, counts[3]);
+      if (counts[4]) atomicAdd(&s.stats->ambiguity_rejected, counts[4]);
+      if (counts[5]) atomicAdd(&s.stats->selected, counts[5]);
+    }
   }
 }
 
@@ -349,7 +541,7 @@ cudaError_t launch_census_texture(const CensusArgs& a, int images, cudaStream_t 
 }
 
 cudaError_t launch_cost_volume(const CostArgs& a, int sm_count, cudaStream_t stream) {
-  int64_t n = (int64_t)a.w * (a.rows ? a.rows : a.h);
+  int64_t n = a.pixels ? a.npixels : (int64_t)a.w * (a.rows ? a.rows : a.h);
   cost_volume_kernel<<<grid_for(n * 32, 256, sm_count * 32), 256, 0, stream>>>(a);
   return cudaGetLastError();
 }
@@ -374,9 +566,30 @@ cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int s
   return cudaGetLastError();
 }
 
+cudaError_t launch_esgm_paths(const EsgmArgs& a, int phase, int sm_count, cudaStream_t stream) {
+  const int warps = 4;
+  const size_t shared = ((size_t)warps * 3 * a.cost.D + (size_t)warps * a.C) * sizeof(int);
+  const int64_t lines = line_count(a.cost.w, a.cost.h, a.dx, a.dy);
+  const int grid = grid_for(lines, warps, sm_count * 64);
+  auto kernel = phase == 0 ? esgm_paths_kernel<0>
+                : phase == 1 ? esgm_paths_kernel<1>
+                             : esgm_paths_kernel<2>;
+  if (shared > 48 * 1024)
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared);
+  kernel<<<grid, warps * 32, shared, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_esgm_select(const EsgmSelectArgs& a, int sm_count, cudaStream_t stream) {
+  const int64_t n = (int64_t)a.sel.w * a.sel.h;
+  const int grid = grid_for(n, 256, sm_count * 16);
+  esgm_select_kernel<<<grid, 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, int sm_count,
                            cudaStream_t stream) {
-  int64_t n = (int64_t)a.w * (a.rows ? a.rows : a.h);
+  int64_t n = a.pixels ? a.npixels : (int64_t)a.w * (a.rows ? a.rows : a.h);
   int grid = grid_for(n * 32, 256, sm_count * 16);
   if (sum_bytes == 2)
     winners_kernel<uint16_t><<<grid, 256, 0, stream>>>(a, (const uint16_t*)sum);

@@ -31,6 +31,9 @@ struct CostArgs {
   int w, h, D, min_disparity, reverse, wx, wy, words, mode, weight, ad_cap, grad_cap, bits;
   // Strip of rows y0 .. y0+rows-1 (rows 0 = the whole image); out is indexed strip-locally.
   int y0 = 0, rows = 0;
+  // The listed pixels pixels[i] (i < npixels) only, cost row i (compact SGM's exact pass).
+  const int32_t* pixels = nullptr;
+  int npixels = 0;
 };
 
 struct PathArgs {
@@ -59,6 +62,41 @@ struct SelectArgs {
   // Strip of rows y0 .. y0+rows-1 (rows 0 = the whole image): cost and sum are strip-local, the
   // outputs are indexed by image pixel.
   int y0 = 0, rows = 0;
+  // Compact SGM's exact pass: the listed pixels pixels[i] (i < npixels) only, their cost and sum
+  // in row i.
+  const int32_t* pixels = nullptr;
+  int npixels = 0;
+};
+
+// Compact SGM (GpuCandidateStereo.java:53-167, kernel hooks :401-479): per path, a few separated
+// proposals per pixel; then the exact aggregate at every proposal and its neighbours and a lower
+// bound of the aggregate elsewhere; pixels whose outcome these certify are selected from them, the
+// others are aggregated and selected exactly.
+// No cost volume is kept: the path walks compute each pixel's costs from the descriptors.
+struct EsgmArgs {
+  CostArgs cost;  // the view's cost inputs (out unused)
+  int dx, dy, p1, p2, edge_scale;
+  uint16_t* cand;     // [n][C] proposals (65535: none), C = directions x pool
+  uint16_t* compact;  // [n][C][3] aggregates at proposal - 1, proposal, proposal + 1
+  uint16_t* outside;  // [n] lower bound of the aggregate away from every proposal (65535: none)
+  int C, direction, pool;
+  // Exact pass: the full path cost of a pixel whose slot lies in [slot_lo, slot_hi) is added to
+  // row slot - slot_lo of sum ([slot_hi - slot_lo][D]).
+  const int32_t* slots;
+  uint16_t* sum;
+  int32_t slot_lo = 0, slot_hi = 0;
+};
+
+struct EsgmSelectArgs {
+  CostArgs cost;  // validity of the disparities
+  const uint16_t* cand;
+  const uint16_t* compact;
+  const uint16_t* outside;
+  SelectArgs sel;     // outputs, counters and the selection parameters
+  int C;
+  int32_t* slots;     // [n] index among the unresolved pixels, -1 when certified
+  int32_t* pixels;    // [n] the unresolved pixels, in slot order
+  int32_t* count;     // unresolved pixels so far
 };
 
 struct LrArgs {
@@ -124,6 +162,8 @@ cudaError_t launch_color_census(const uint8_t* bgr, const uint8_t* valid, int w,
 cudaError_t launch_cost_volume(const CostArgs& a, int sm_count, cudaStream_t stream);
 cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int sm_count,
                               cudaStream_t stream);
+cudaError_t launch_esgm_paths(const EsgmArgs& a, int phase, int sm_count, cudaStream_t stream);
+cudaError_t launch_esgm_select(const EsgmSelectArgs& a, int sm_count, cudaStream_t stream);
 cudaError_t launch_winners(const SelectArgs& a, const void* sum, int sum_bytes, int sm_count,
                            cudaStream_t stream);
 cudaError_t launch_lr_check(const LrArgs& a, int sm_count, cudaStream_t stream);

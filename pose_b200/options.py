@@ -45,8 +45,10 @@ class Options:
     compute: str = "gpu"
     gpuDevice: int = 0
     gpuMemoryMb: int = 0
-    # resident or streamed views (Options.java:32,39; --gpu-sgm, --gpu-strip-rows)
+    # resident, streamed or compact views (Options.java:32,35,39; --gpu-sgm, --esgm-candidates,
+    # --gpu-strip-rows)
     gpuSgm: str = "auto"
+    esgmCandidates: int = 2
     gpuStripRows: int = 64
     # pyramid matcher (Options.java:28,85-86; DenseMatcher.java)
     pyramidLevels: int = 1  # 0 = automatic
@@ -102,8 +104,10 @@ class Options:
             raise ValueError("Require 0 <= p1 < p2, 0 <= uniqueness < 1")
         if self.directions not in (4, 8, 16):
             raise ValueError("Directions must be 4 or 8 (16 is this matcher's extension)")
-        if self.gpuSgm not in ("auto", "resident", "streamed"):
-            raise ValueError("--gpu-sgm must be auto, resident or streamed")
+        if self.gpuSgm not in ("auto", "resident", "streamed", "esgm"):
+            raise ValueError("--gpu-sgm must be auto, resident, streamed or esgm")
+        if self.esgmCandidates < 1 or self.esgmCandidates > 4:
+            raise ValueError("--esgm-candidates must be 1..4")
         if self.gpuStripRows < 1:
             raise ValueError("--gpu-strip-rows must be positive")
         if (self.tileSize < 32 or self.tileOverlap < 2 or self.tileOverlap > self.tileSize

@@ -140,9 +140,20 @@ class GpuSgm:
         check(self.lib.csgm_session_set_budget(self.handle, int(nbytes)))
 
     def set_streaming(self, mode: str = "auto", strip_rows: int = 64) -> None:
-        """Options.gpuSgm ("auto", "resident", "streamed") and Options.gpuStripRows."""
+        """Options.gpuSgm ("auto", "resident", "streamed", "esgm") and Options.gpuStripRows."""
         check(self.lib.csgm_session_set_streaming(self.handle, _abi.SGM_MODES[mode],
                                                   int(strip_rows)))
+
+    def set_candidates(self, per_path: int = 2) -> None:
+        """Options.esgmCandidates: compact SGM's separated proposals per path (1..4)."""
+        check(self.lib.csgm_session_set_candidates(self.handle, int(per_path)))
+
+    def compact_report(self, reverse: int = 0) -> tuple:
+        """(certified, verified exactly) pixels of compact SGM's last view of that side."""
+        cert, exact = ctypes.c_int64(), ctypes.c_int64()
+        check(self.lib.csgm_session_compact_report(self.handle, int(reverse), ctypes.byref(cert),
+                                                   ctypes.byref(exact)))
+        return cert.value, exact.value
 
     def plan(self, params: CsgmParams, w: int, h: int) -> int:
         out = ctypes.c_int64()
@@ -366,6 +377,7 @@ class CensusSgm:
         self._own = session is None
         self.session = session or GpuSgm(options.gpuDevice, options.gpuMemoryMb)
         self.session.set_streaming(options.gpuSgm, options.gpuStripRows)
+        self.session.set_candidates(options.esgmCandidates)
 
     def params(self) -> CsgmParams:
         return params_from_options(self.options)

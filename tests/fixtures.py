@@ -113,3 +113,20 @@ def plane_metrics(disp: np.ndarray, w: int, h: int, truth: float):
     e = d[np.isfinite(d)] - truth
     e.sort()
     return len(e), math.sqrt(float(np.sum(e * e)) / len(e)), e[len(e) * 9 // 10] - e[len(e) // 10]
+
+
+def esgm_production_pair(fixture: int):
+    """src/test/java/sgm/EsgmProductionRegression.java:15-29: 160x47, Random(174) (fixture 0 and
+    2) or a periodic pattern (fixture 1), right = left shifted by 11 (-11 for fixture 2) with the
+    column clamped to the image, a 7x5 hole in the left mask."""
+    w, h = 160, 47
+    a = JavaRandom(174).nextBytes(w * h)
+    if fixture == 1:
+        y, x = np.mgrid[0:h, 0:w]
+        a = ((x % 12) * 19 + (y % 3) * 7).astype(np.uint8).reshape(-1)
+    shift = -11 if fixture == 2 else 11
+    cols = np.clip(np.arange(w) + shift, 0, w - 1)
+    b = np.ascontiguousarray(a.reshape(h, w)[:, cols]).reshape(-1)
+    ma = np.full((h, w), 255, np.uint8)
+    ma[8:13, 29:36] = 0
+    return w, h, a, b, ma.reshape(-1), np.full(w * h, 255, np.uint8)

@@ -25,6 +25,9 @@ class OracleSession:
     def set_streaming(self, mode="auto", strip_rows=64):
         self.streaming = (mode, strip_rows)
 
+    def set_candidates(self, per_path=2):
+        self.candidates = per_path
+
     def pair(self, params, left, right, w, h, validLeft=None, validRight=None, want_views=False,
              want_reasons=False, leftBgr=None, rightBgr=None):
         r = orc.pair(params, left, right, w, h, validLeft, validRight, want_reasons=True,

@@ -156,7 +156,7 @@ def test_streamed_match_equals_oracle(session, reverse):
 
 
 def test_streaming_settings_are_checked(session):
-    assert session.lib.csgm_session_set_streaming(session.handle, 3, 0) == _abi.CSGM_E_INVALID
+    assert session.lib.csgm_session_set_streaming(session.handle, 4, 0) == _abi.CSGM_E_INVALID
     assert session.lib.csgm_session_set_streaming(session.handle, 0, -1) == _abi.CSGM_E_INVALID
-    with pytest.raises(KeyError):  # ESGM (compact candidates) is not built
-        session.set_streaming("esgm")
+    with pytest.raises(KeyError):
+        session.set_streaming("disk")
