@@ -39,6 +39,10 @@ WORKLOADS = {
                            p2=None, directions=16, aggregate="32", ad_truncation=10),
     "cfg2-zncc": dict(spec="cfg2", census=(7, 7), D=256, cost="zncc", p1=None, p2=None,
                       directions=16, aggregate="32"),
+    # the cfg1 pair through compact SGM (--gpu-sgm esgm, 2 proposals per path): no cost or
+    # aggregate volume
+    "cfg1-esgm": dict(spec="cfg1", census=(9, 7), D=128, cost="census", p1=10, p2=120,
+                      sgm="esgm", candidates=2),
 }
 
 
@@ -89,9 +93,11 @@ def workload_desc(name: str, prm) -> str:
     from pose_b200.synthetic import spec_for
 
     s = spec_for(wl["spec"])
+    mode = (f"compact SGM ({wl['candidates']} proposals per path, exact pass over the rest), "
+            if wl.get("sgm") == "esgm" else "")
     return (f"{s.width}x{s.height} D{prm.disparities} {wl['cost']} {prm.window_x}x{prm.window_y} "
             f"{prm.directions}-path P1={prm.p1} P2={prm.p2} uint{8 * prm.aggregate_bytes} "
-            "aggregate, WTA+subpixel, LR check; both views per pair")
+            f"aggregate, {mode}WTA+subpixel, LR check; both views per pair")
 
 
 # ---------------------------------------------------------------------------------------------
@@ -201,7 +207,7 @@ def pair_model_bytes_per_cell(prm) -> int:
 
 
 def model_bytes_per_launch(kernel: str, prm, w: int, h: int):
-    """A kernel's share of the pair model's 5 + 4 Sb bytes per cell (SURVEY 8(d) accounting):
+    """A kernel's share of the pair model's 5 + 4 Sb bytes per cell:
     the sweeps read both views' cost volumes (2 streams x 2 views x 1 B) and one stream's partial
     aggregate is written and read by the other (2 views x 2 Sb); the cost kernel writes the volume
     once (1 B).  None for kernels the model does not count."""
@@ -243,6 +249,21 @@ def algorithmic_bytes_per_launch(kernel: str, prm, w: int, h: int, lines_in_swee
     if kernel == "sweep" and lines_in_sweep:
         return (table["sweep"] + lines) * cells
     return table[kernel] * cells
+
+
+def compact_bytes_per_launch(kernel: str, prm, w: int, h: int, proposals: int):
+    """Algorithmic HBM bytes of one compact SGM launch (one view, every direction): both images'
+    descriptors and textures and the view's grays once, plus the phase's own arrays (C =
+    directions x proposals: 2-byte proposals, three 2-byte compact aggregates each, a 4-byte lower
+    bound and slot per pixel).  The exact pass's listed rows are left out (a few % of pixels)."""
+    n = w * h
+    c = prm.directions * proposals
+    words = (prm.window_x * prm.window_y - 1 + 63) // 64
+    inputs = n * (2 * 8 * words + 2 + 1)
+    table = {"esgm_proposals": inputs + 2 * n * c,
+             "esgm_compact": inputs + 2 * n * c + 2 * 6 * n * c + 2 * 4 * n,
+             "esgm_exact": inputs + 4 * n}
+    return table.get(kernel)
 
 
 def read_traffic(workload: str, kernel: str):
@@ -381,6 +402,10 @@ def run_ours(args):
     cells = n * prm.disparities
     lib = _abi.load()
     session = GpuSgm(local)
+    compact = WORKLOADS[args.workload].get("sgm") == "esgm"
+    if compact:
+        session.set_streaming("esgm")
+        session.set_candidates(WORKLOADS[args.workload]["candidates"])
 
     # Device-resident inputs/outputs (torch is only the allocator here).
     d_left = torch.from_numpy(left).to(f"cuda:{local}")
@@ -470,6 +495,9 @@ def run_ours(args):
         name, (count, total_ns) = max(kernels.items(), key=lambda kv: kv[1][1])
         per_launch = model_bytes_per_launch(name, prm, w, h)
         impl = algorithmic_bytes_per_launch(name, prm, w, h, "lines_rest" in kernels)
+        if compact:
+            per_launch = impl = compact_bytes_per_launch(
+                name, prm, w, h, WORKLOADS[args.workload]["candidates"])
         peak, peak_kind = measured_peak_gbs()
         if per_launch and count:
             launch_s = total_ns / count / 1e9

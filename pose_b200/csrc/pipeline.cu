@@ -75,7 +75,7 @@ static size_t strip_bytes(const csgm_params& p, int w, int rows) {
 // aggregates and cost rows (the least chunk of the exact pass).
 static size_t compact_bytes(const csgm_params& p, int w, int h, int pool) {
   const size_t n = (size_t)w * h, C = (size_t)p.directions * pool;
-  return n * (C * 8 + 2 + 8) + 16 + (size_t)w * p.disparities * 4;
+  return n * (C * 8 + 4 + 8) + 16 + (size_t)w * p.disparities * 4;
 }
 
 // GpuCandidateStereo.plan (GpuCandidateStereo.java:20-47): grayscale Census with 16-bit
@@ -214,7 +214,7 @@ static int run_view_compact(Context& ctx, const csgm_params& p, int pool, const 
   const int C = p.directions * pool;
   WS(cand, uint16_t, kEsgmCand, n * C * 2);
   WS(compact, uint16_t, kEsgmCompact, n * C * 6);
-  WS(outside, uint16_t, kEsgmOutside, n * 2);
+  WS(outside, uint32_t, kEsgmOutside, n * 4);
   WS(slots, int32_t, kEsgmSlots, n * 4);
   WS(pixels, int32_t, kEsgmPixels, n * 4);
   WS(count, int32_t, kEsgmCount, 16);
@@ -223,18 +223,15 @@ static int run_view_compact(Context& ctx, const csgm_params& p, int pool, const 
              p.census_weight_milli, p.ad_truncation, p.gradient_truncation,
              p.window_x * p.window_y - 1};
   CK(cudaMemsetAsync(compact, 0, n * C * 6, ctx.stream), "compact clear");
-  CK(cudaMemsetAsync(outside, 0, n * 2, ctx.stream), "bound clear");
+  CK(cudaMemsetAsync(outside, 0, n * 4, ctx.stream), "bound clear");
   CK(cudaMemsetAsync(count, 0, 16, ctx.stream), "count clear");
-  EsgmArgs e{c, 0, 0, p.p1, p.p2, p.edge_scale, cand, compact, outside, C, 0, pool, slots,
+  EsgmArgs e{c, p.directions, p.p1, p.p2, p.edge_scale, cand, compact, outside, C, pool, slots,
              nullptr};
-  for (int phase = 0; phase < 2; phase++)
-    for (int d = 0; d < p.directions; d++) {
-      direction(d, e.dx, e.dy);
-      e.direction = d;
-      ctx.prof->kernel_begin();
-      CK(launch_esgm_paths(e, phase, ctx.sm_count, ctx.stream), "compact path kernel launch");
-      ctx.prof->kernel_end(phase == 0 ? "esgm_proposals" : "esgm_compact");
-    }
+  for (int phase = 0; phase < 2; phase++) {
+    ctx.prof->kernel_begin();
+    CK(launch_esgm_paths(e, phase, ctx.sm_count, ctx.stream), "compact path kernel launch");
+    ctx.prof->kernel_end(phase == 0 ? "esgm_proposals" : "esgm_compact");
+  }
   SelectArgs s{nullptr, out, summary, reasons, boundary, dstats, w, h, p.disparities,
                p.window_x, p.window_y, p.min_disparity, p.uniqueness};
   EsgmSelectArgs sel{c, cand, compact, outside, s, C, slots, pixels, count};
@@ -268,13 +265,9 @@ static int run_view_compact(Context& ctx, const csgm_params& p, int pool, const 
     x.sum = sum;
     x.slot_lo = (int32_t)lo;
     x.slot_hi = (int32_t)(lo + rows);
-    for (int d = 0; d < p.directions; d++) {
-      direction(d, x.dx, x.dy);
-      x.direction = d;
-      ctx.prof->kernel_begin();
-      CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
-      ctx.prof->kernel_end("esgm_exact");
-    }
+    ctx.prof->kernel_begin();
+    CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
+    ctx.prof->kernel_end("esgm_exact");
     CostArgs cr = c;
     cr.out = cost;
     cr.pixels = pixels + lo;

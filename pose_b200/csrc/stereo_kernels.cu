@@ -179,15 +179,52 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
 
 // ---------------------------------------------------------------------------------------------
 // Compact SGM (GpuCandidateStereo.java:53-167, the path kernel hooks :401-479).  One warp per line
-// as in paths_line_kernel, each pixel's costs computed from the descriptors (no cost volume); at
-// every pixel, after the path state L:
+// as in paths_line_kernel, each pixel's costs computed from the descriptors (no cost volume), and
+// every direction of a phase in one launch (blockIdx.y = direction); at every pixel, after the
+// path state L:
 //  PHASE 0: `pool` separated proposals of the path: the valid disparity of least L (ties: the
 //   smaller), then the least among those more than one away from every proposal so far;
 //  PHASE 1 (all directions' proposals known): L at every proposal - 1, proposal, proposal + 1 is
 //   added to the pixel's compact aggregates, and the least L over the valid disparities no
-//   proposal covers (within one) to the pixel's lower bound of the aggregate there;
+//   proposal covers (within one) to the pixel's lower bound of the aggregate there (or the bound
+//   is marked empty when every valid disparity is covered, which no direction changes);
 //  PHASE 2 (exact pass): L is added to the full aggregate row of each listed pixel.
-// The directions run one after another, so every read-modify-write of a pixel is ordered.
+// The directions' additions to a pixel are atomic 32-bit adds of a 16-bit value shifted into its
+// half of the word.  They are exact in any order: the plan allows 16-bit aggregates only while
+// directions x (512 + P2) <= 65535, and one path's L never exceeds 512 + P2, so no 16-bit sum
+// carries into its neighbour (the reference adds the directions one after another with the same
+// wrap-free values, GpuCandidateStereo.java:437-444).
+// cost_at for the Census cost (the only one compact SGM plans for), with the pixel's own terms
+// (border, texture, descriptor words) taken once per pixel instead of once per disparity.
+struct CensusPixel {
+  bool inside;
+  uint64_t w0, w1;
+  __device__ __forceinline__ CensusPixel(const CostArgs& a, int x, int y, int64_t n) {
+    const int rx = a.wx / 2, ry = a.wy / 2;
+    const int64_t p = (int64_t)y * a.w + x;
+    inside = x >= rx && x < a.w - rx && y >= ry && y < a.h - ry && a.tex_a[p];
+    w0 = inside ? a.desc_a[p] : 0;
+    w1 = inside && a.words > 1 ? a.desc_a[n + p] : 0;
+  }
+  __device__ __forceinline__ int at(const CostArgs& a, int x, int y, int k, int64_t n) const {
+    if (!inside) return kInvalidCost;
+    const int rx = a.wx / 2;
+    const long long disparity = (long long)a.min_disparity + k;
+    const long long target = (long long)x + (a.reverse ? disparity : -disparity);
+    if (target < rx || target >= a.w - rx) return kInvalidCost;
+    const int64_t q = (int64_t)y * a.w + target;
+    if (!a.tex_b[q]) return kInvalidCost;
+    int hamming = __popcll(w0 ^ a.desc_b[q]);
+    if (a.words > 1) hamming += __popcll(w1 ^ a.desc_b[n + q]);
+    return hamming;
+  }
+};
+
+__device__ __forceinline__ void add_u16(uint16_t* at, unsigned v) {
+  const uintptr_t address = (uintptr_t)at;
+  atomicAdd((unsigned*)(address & ~(uintptr_t)3), v << ((address & 2) ? 16 : 0));
+}
+
 template <int PHASE>
 __global__ void esgm_paths_kernel(EsgmArgs a) {
   extern __shared__ int smem[];
@@ -195,15 +232,21 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
   const int D = ca.D, w = ca.w, h = ca.h, C = a.C;
   const int64_t n = (int64_t)w * h;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  int* prev = smem + (size_t)warp * 3 * D;
+  const int dir = blockIdx.y;
+  int dx, dy;
+  direction(dir, dx, dy);
+  int* prev = smem + (size_t)warp * 4 * D;
   int* cur = prev + D;
   int* cost = cur + D;
-  int* props = smem + (size_t)warps * 3 * D + (size_t)warp * C;  // PHASE 1: the proposals
-  const int64_t lines = line_count(w, h, a.dx, a.dy);
+  int* covered = cost + D;  // PHASE 1: proposals within one of k (cleared after each pixel)
+  const int64_t lines = line_count(w, h, dx, dy);
+  if (PHASE == 1)
+    for (int k = lane; k < D; k += 32) covered[k] = 0;
+  __syncwarp();
   for (int64_t line = (int64_t)blockIdx.x * warps + warp; line < lines;
        line += (int64_t)gridDim.x * warps) {
     int x, y;
-    line_start(line, w, h, a.dx, a.dy, x, y);
+    line_start(line, w, h, dx, dy, x, y);
     int64_t prev_p = -1;
     while (x >= 0 && x < w && y >= 0 && y < h) {
       const int64_t p = (int64_t)y * w + x;
@@ -215,8 +258,18 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
         minimum = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
         local_p2 = path_p2(a.p1, a.p2, a.edge_scale, ca.gray_a[p], ca.gray_a[prev_p]);
       }
+      // PHASE 1: proposal lane + 32 r of the pixel in prop[r] (C <= 64).
+      int prop[2] = {65535, 65535};
+      if (PHASE == 1)
+        for (int r = 0; r < 2; r++)
+          if (lane + 32 * r < C) {
+            prop[r] = a.cand[p * C + lane + 32 * r];
+            for (int k = max(prop[r] - 1, 0); k <= prop[r] + 1 && k < D; k++)
+              atomicAdd(&covered[k], 1);
+          }
+      const CensusPixel pixel(ca, x, y, n);
       for (int k = lane; k < D; k += 32) {
-        const int c = cost_at(ca, x, y, k, n);
+        const int c = pixel.at(ca, x, y, k, n);
         int v = c;
         if (has) {
           int t = min(prev[k], minimum + local_p2);
@@ -240,35 +293,36 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
             }
           key = __reduce_min_sync(0xffffffffu, key);
           chosen[choice] = key == 0x7fffffffu ? 65535 : (int)(key % (unsigned)(D + 1));
-          if (lane == 0) a.cand[p * C + a.direction * a.pool + choice] = (uint16_t)chosen[choice];
+          if (lane == 0) a.cand[p * C + dir * a.pool + choice] = (uint16_t)chosen[choice];
         }
       } else if constexpr (PHASE == 1) {
-        for (int j = lane; j < C; j += 32) props[j] = a.cand[p * C + j];
-        __syncwarp();
-        for (int j = lane; j < 3 * C; j += 32) {
-          const int k = props[j / 3] + j % 3 - 1;
-          if (k >= 0 && k < D) {
-            uint16_t* at = a.compact + p * C * 3 + j;
-            *at = (uint16_t)(*at + cur[k]);
-          }
+        for (int base = 0; base < 3 * C; base += 32) {  // uniform trip count: shuffles below
+          const int j = base + lane, source = min(j, 3 * C - 1) / 3;
+          const int low = __shfl_sync(0xffffffffu, prop[0], source & 31);
+          const int high = __shfl_sync(0xffffffffu, prop[1], source & 31);
+          const int k = (source < 32 ? low : high) + j % 3 - 1;
+          if (j < 3 * C && k >= 0 && k < D) add_u16(a.compact + p * C * 3 + j, (unsigned)cur[k]);
         }
         unsigned lower = 0x7fffffffu;
         for (int k = lane; k < D; k += 32)
-          if (cost[k] != kInvalidCost) {
-            bool covered = false;
-            for (int j = 0; j < C; j++) covered |= abs(k - props[j]) <= 1;
-            if (!covered) lower = min(lower, (unsigned)cur[k]);
-          }
+          if (cost[k] != kInvalidCost && covered[k] == 0) lower = min(lower, (unsigned)cur[k]);
         lower = __reduce_min_sync(0xffffffffu, lower);
-        if (lane == 0)
-          a.outside[p] = lower == 0x7fffffffu
-                             ? (uint16_t)65535
-                             : (uint16_t)min(65535u, (unsigned)a.outside[p] + lower);
+        if (lane == 0) {
+          if (lower == 0x7fffffffu)
+            atomicOr(a.outside + p, 0x80000000u);
+          else
+            atomicAdd(a.outside + p, lower);
+        }
+        __syncwarp();
+        for (int r = 0; r < 2; r++)
+          if (lane + 32 * r < C)
+            for (int k = max(prop[r] - 1, 0); k <= prop[r] + 1 && k < D; k++)
+              atomicSub(&covered[k], 1);
       } else {
         const int slot = a.slots[p];
         if (slot >= a.slot_lo && slot < a.slot_hi) {
-          uint16_t* s = a.sum + (int64_t)(slot - a.slot_lo) * D;
-          for (int k = lane; k < D; k += 32) s[k] = (uint16_t)(s[k] + cur[k]);
+          uint16_t* row = a.sum + (int64_t)(slot - a.slot_lo) * D;
+          for (int k = lane; k < D; k += 32) add_u16(row + k, (unsigned)cur[k]);
         }
       }
       __syncwarp();
@@ -276,8 +330,8 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
       prev = cur;
       cur = swap;
       prev_p = p;
-      x += a.dx;
-      y += a.dy;
+      x += dx;
+      y += dy;
     }
     __syncwarp();
   }
@@ -432,7 +486,8 @@ __global__ void esgm_select_kernel(EsgmSelectArgs a) {
     const int flags = (valid(0) ? 1 : 0) | (valid(D - 1) ? 2 : 0);
     bool trusted = true;
     if (best >= 0) {
-      const long long lower = a.outside[p];
+      const unsigned bound = a.outside[p];
+      const long long lower = (bound & 0x80000000u) ? 65535 : min(bound, 65535u);
       const bool winner = lower > value && (before < 0 || before > value) &&
                           (after < 0 || after > value) && second > value;
       const double margin = fmax(1.0, value * s.uniqueness);
@@ -567,10 +622,15 @@ cudaError_t launch_paths_line(const PathArgs& a, void* sum, int sum_bytes, int s
 }
 
 cudaError_t launch_esgm_paths(const EsgmArgs& a, int phase, int sm_count, cudaStream_t stream) {
-  const int warps = 4;
-  const size_t shared = ((size_t)warps * 3 * a.cost.D + (size_t)warps * a.C) * sizeof(int);
-  const int64_t lines = line_count(a.cost.w, a.cost.h, a.dx, a.dy);
-  const int grid = grid_for(lines, warps, sm_count * 64);
+  const int warps = a.cost.D > 2048 ? 2 : 4;  // 4 D-int rows per warp within 227 KB
+  const size_t shared = (size_t)warps * 4 * a.cost.D * sizeof(int);
+  int64_t lines = 0;
+  for (int d = 0; d < a.directions; d++) {
+    int dx, dy;
+    direction(d, dx, dy);
+    lines = std::max(lines, line_count(a.cost.w, a.cost.h, dx, dy));
+  }
+  const dim3 grid(grid_for(lines, warps, sm_count * 64), a.directions);
   auto kernel = phase == 0 ? esgm_paths_kernel<0>
                 : phase == 1 ? esgm_paths_kernel<1>
                              : esgm_paths_kernel<2>;

@@ -75,11 +75,12 @@ struct SelectArgs {
 // No cost volume is kept: the path walks compute each pixel's costs from the descriptors.
 struct EsgmArgs {
   CostArgs cost;  // the view's cost inputs (out unused)
-  int dx, dy, p1, p2, edge_scale;
+  int directions, p1, p2, edge_scale;
   uint16_t* cand;     // [n][C] proposals (65535: none), C = directions x pool
   uint16_t* compact;  // [n][C][3] aggregates at proposal - 1, proposal, proposal + 1
-  uint16_t* outside;  // [n] lower bound of the aggregate away from every proposal (65535: none)
-  int C, direction, pool;
+  // [n] lower bound of the aggregate away from every proposal; bit 31: no such disparity
+  uint32_t* outside;
+  int C, pool;
   // Exact pass: the full path cost of a pixel whose slot lies in [slot_lo, slot_hi) is added to
   // row slot - slot_lo of sum ([slot_hi - slot_lo][D]).
   const int32_t* slots;
@@ -91,7 +92,7 @@ struct EsgmSelectArgs {
   CostArgs cost;  // validity of the disparities
   const uint16_t* cand;
   const uint16_t* compact;
-  const uint16_t* outside;
+  const uint32_t* outside;
   SelectArgs sel;     // outputs, counters and the selection parameters
   int C;
   int32_t* slots;     // [n] index among the unresolved pixels, -1 when certified

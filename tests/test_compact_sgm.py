@@ -96,6 +96,22 @@ def test_production_fixtures(session, fixture, directions):
         assert_same(got, want, f"fixture {fixture}, {directions} paths, {pool} proposals")
 
 
+def test_wide_disparity_range(session):
+    """D = 2100 (the path kernels then run two warps a block to fit four D-rows each in shared
+    memory) on a 2304x9 noise pair shifted by 1500."""
+    from fixtures import shifted
+
+    w, h = 2304, 9
+    a = np.random.default_rng(31).integers(0, 256, w * h, dtype=np.uint8)
+    b = shifted(a, w, h, 1500)
+    o = Options()
+    o.disparities, o.directions, o.census = 2100, 4, 3
+    prm = params_from_options(o)
+    want = orc.pair(prm, a, b, w, h, want_reasons=True)
+    got, _ = compact_pair(session, prm, a, b, w, h, pool=1)
+    assert_same(got, want, "compact, D2100")
+
+
 def test_compact_crop_equals_oracle(session):
     """A 1600x200 crop of the synthetic 1600x1067 scene (D128, census 9x7): one proposal per path
     leaves pixels to the exact pass, which must then give the full SGM's outcome."""
