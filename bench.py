@@ -633,6 +633,9 @@ def run_profile_pairs(args):
         left = np.ascontiguousarray(left.reshape(-1, w)[:h]).reshape(-1)
         right = np.ascontiguousarray(right.reshape(-1, w)[:h]).reshape(-1)
     session = GpuSgm(0)
+    if WORKLOADS[args.workload].get("sgm") == "esgm":
+        session.set_streaming("esgm")
+        session.set_candidates(WORKLOADS[args.workload]["candidates"])
     for _ in range(args.profile_pairs):
         r = session.pair(prm, left, right, w, h)
     session.close()

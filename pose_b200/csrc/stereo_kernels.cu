@@ -196,26 +196,33 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
 // wrap-free values, GpuCandidateStereo.java:437-444).
 // cost_at for the Census cost (the only one compact SGM plans for), with the pixel's own terms
 // (border, texture, descriptor words) taken once per pixel instead of once per disparity.
+// The target of disparity k is x0 + step * k (step = +1 for the right view, -1 for the left).
 struct CensusPixel {
   bool inside;
   uint64_t w0, w1;
+  const uint64_t *b0, *b1;  // the target row's descriptor words
+  const uint8_t* tb;        // the target row's texture flags
+  long long x0;
+  int step, lo, hi;  // valid targets lo <= t < hi
   __device__ __forceinline__ CensusPixel(const CostArgs& a, int x, int y, int64_t n) {
     const int rx = a.wx / 2, ry = a.wy / 2;
-    const int64_t p = (int64_t)y * a.w + x;
+    const int64_t row = (int64_t)y * a.w, p = row + x;
     inside = x >= rx && x < a.w - rx && y >= ry && y < a.h - ry && a.tex_a[p];
     w0 = inside ? a.desc_a[p] : 0;
     w1 = inside && a.words > 1 ? a.desc_a[n + p] : 0;
+    b0 = a.desc_b + row;
+    b1 = a.desc_b + n + row;
+    tb = a.tex_b + row;
+    step = a.reverse ? 1 : -1;
+    x0 = (long long)x + (long long)step * a.min_disparity;
+    lo = rx;
+    hi = a.w - rx;
   }
-  __device__ __forceinline__ int at(const CostArgs& a, int x, int y, int k, int64_t n) const {
-    if (!inside) return kInvalidCost;
-    const int rx = a.wx / 2;
-    const long long disparity = (long long)a.min_disparity + k;
-    const long long target = (long long)x + (a.reverse ? disparity : -disparity);
-    if (target < rx || target >= a.w - rx) return kInvalidCost;
-    const int64_t q = (int64_t)y * a.w + target;
-    if (!a.tex_b[q]) return kInvalidCost;
-    int hamming = __popcll(w0 ^ a.desc_b[q]);
-    if (a.words > 1) hamming += __popcll(w1 ^ a.desc_b[n + q]);
+  __device__ __forceinline__ int at(const CostArgs& a, int k) const {
+    const long long t = x0 + (long long)step * k;
+    if (!inside || t < lo || t >= hi || !tb[t]) return kInvalidCost;
+    int hamming = __popcll(w0 ^ b0[t]);
+    if (a.words > 1) hamming += __popcll(w1 ^ b1[t]);
     return hamming;
   }
 };
@@ -235,6 +242,10 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
   const int dir = blockIdx.y;
   int dx, dy;
   direction(dir, dx, dy);
+  // StereoCost.pathP2 by the gray difference of a pixel and its predecessor.
+  __shared__ int p2_of[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) p2_of[i] = path_p2(a.p1, a.p2, a.edge_scale, i, 0);
+  __syncthreads();
   int* prev = smem + (size_t)warp * 4 * D;
   int* cur = prev + D;
   int* cost = cur + D;
@@ -256,7 +267,7 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
         int m = INT_MAX;
         for (int k = lane; k < D; k += 32) m = min(m, prev[k]);
         minimum = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
-        local_p2 = path_p2(a.p1, a.p2, a.edge_scale, ca.gray_a[p], ca.gray_a[prev_p]);
+        local_p2 = p2_of[abs((int)ca.gray_a[p] - (int)ca.gray_a[prev_p])];
       }
       // PHASE 1: proposal lane + 32 r of the pixel in prop[r] (C <= 64).
       int prop[2] = {65535, 65535};
@@ -269,7 +280,7 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
           }
       const CensusPixel pixel(ca, x, y, n);
       for (int k = lane; k < D; k += 32) {
-        const int c = pixel.at(ca, x, y, k, n);
+        const int c = pixel.at(ca, k);
         int v = c;
         if (has) {
           int t = min(prev[k], minimum + local_p2);
@@ -282,17 +293,22 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
       }
       __syncwarp();
       if constexpr (PHASE == 0) {
+        // Keys (L << 12) | k order as the reference's L * (D + 1) + k (k < D <= 4096, and
+        // L <= 512 + P2 <= 65535 within the 16-bit bound).
         int chosen[4] = {65535, 65535, 65535, 65535};
-        for (int choice = 0; choice < a.pool; choice++) {
-          unsigned key = 0x7fffffffu;
+#pragma unroll
+        for (int choice = 0; choice < 4; choice++) {
+          if (choice >= a.pool) break;
+          unsigned key = 0xffffffffu;
           for (int k = lane; k < D; k += 32)
             if (cost[k] != kInvalidCost) {
               bool eligible = true;
+#pragma unroll
               for (int j = 0; j < choice; j++) eligible &= abs(k - chosen[j]) > 1;
-              if (eligible) key = min(key, (unsigned)(cur[k] * (D + 1) + k));
+              if (eligible) key = min(key, ((unsigned)cur[k] << 12) | (unsigned)k);
             }
           key = __reduce_min_sync(0xffffffffu, key);
-          chosen[choice] = key == 0x7fffffffu ? 65535 : (int)(key % (unsigned)(D + 1));
+          chosen[choice] = key == 0xffffffffu ? 65535 : (int)(key & 4095u);
           if (lane == 0) a.cand[p * C + dir * a.pool + choice] = (uint16_t)chosen[choice];
         }
       } else if constexpr (PHASE == 1) {
