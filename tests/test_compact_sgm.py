@@ -246,3 +246,26 @@ def test_compact_settings_are_checked(session):
             assert e.value.status == _abi.CSGM_E_INVALID
     finally:
         session.set_streaming("auto")
+
+
+def test_census_sgm_compute_in_compact_mode(session):
+    """CensusSgm.compute with Options.gpuSgm = "esgm" (the matcher, the LR check and every
+    post-filter on its outputs) equals the resident run: the map, reasons and the Stats CSV."""
+    from pose_b200.sgm import CensusSgm
+
+    w, h, a, b, ma, mb = esgm_production_pair(0)
+    results = {}
+    for mode, pool in (("resident", 2), ("esgm", 1), ("esgm", 4)):
+        o = Options()
+        o.minDisparity, o.disparities, o.directions = -15, 129, 8
+        o.gpuSgm, o.esgmCandidates = mode, pool
+        results[(mode, pool)] = CensusSgm(o, session=session).compute(a, b, w, h, ma, mb,
+                                                                     want_reasons=True)
+    session.set_streaming("auto")
+    session.set_candidates(2)
+    want = results[("resident", 2)]
+    for key in (("esgm", 1), ("esgm", 4)):
+        got = results[key]
+        assert np.array_equal(bits(got.disparity), bits(want.disparity)), key
+        assert np.array_equal(got.reasons, want.reasons), key
+        assert got.stats.csv() == want.stats.csv(), key
