@@ -183,6 +183,13 @@ int csgm_session_set_streaming(csgm_session* session, int32_t mode, int32_t stri
  * path keeps per pixel in compact SGM, 1..4 (default 2); the plan lowers it until it fits. */
 int csgm_session_set_candidates(csgm_session* session, int32_t per_path);
 
+/* Host memory a streamed plan may use for its parked aggregate, GpuCandidateStereo.hostBudget
+ * (src/main/java/sgm/GpuCandidateStereo.java:15-16: --memory-mb); 0 = no limit (the default).
+ * Over it, AUTO runs compact SGM where it applies (grayscale Census, 16-bit aggregates;
+ * GpuStereo.execute, src/main/java/sgm/GpuStereo.java:184-193) and otherwise, like STREAMED,
+ * fails with CSGM_E_NOMEM. */
+int csgm_session_set_host_budget(csgm_session* session, int64_t bytes);
+
 /* Compact SGM's outcome for the session's last view of each side (reverse 0 = left, 1 = right):
  * the pixels its proposals certified and those it aggregated exactly (the reference's
  * esgm_left/right report, GpuCandidateStereo.java:106-131). */

@@ -173,6 +173,7 @@ SIGNATURES = {
     "csgm_session_set_budget": (ctypes.c_int, [_P, _I64]),
     "csgm_session_set_streaming": (ctypes.c_int, [_P, _I32, _I32]),
     "csgm_session_set_candidates": (ctypes.c_int, [_P, _I32]),
+    "csgm_session_set_host_budget": (ctypes.c_int, [_P, _I64]),
     "csgm_session_compact_report": (
         ctypes.c_int, [_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "csgm_plan_detail": (

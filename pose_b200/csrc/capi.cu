@@ -156,6 +156,7 @@ void session_settings(Context& ctx, csgm_session* s, const csgm_params& p, int w
   ctx.sgm_mode = s->sgm_mode;
   ctx.strip_rows = s->strip_rows;
   ctx.candidates = s->candidates;
+  ctx.host_budget = s->host_budget;
   ctx.compact_report = s->compact_report;
   ctx.host_partial = &s->host_partial;
   if (s->tuning_forced)
@@ -334,6 +335,13 @@ int csgm_session_set_candidates(csgm_session* s, int32_t per_path) {
   if (per_path < 1 || per_path > 4) return fail(CSGM_E_INVALID, "--esgm-candidates must be 1..4");
   std::lock_guard<std::mutex> guard(s->lock);
   s->candidates = per_path;
+  return CSGM_OK;
+}
+
+int csgm_session_set_host_budget(csgm_session* s, int64_t bytes) {
+  if (!s || bytes < 0) return fail(CSGM_E_INVALID, "invalid session or host budget");
+  std::lock_guard<std::mutex> guard(s->lock);
+  s->host_budget = (size_t)bytes;
   return CSGM_OK;
 }
 

@@ -107,7 +107,7 @@ static int compact_plan(const Context& ctx, const csgm_params& p, int w, int h, 
 // until one fits.  Strips are at least two rows high with 16 paths, so that a (+-1,+-2) path's
 // predecessor always lies in the previous strip.
 static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
-                       size_t resident, ViewPlan* plan) {
+                       size_t resident, ViewPlan* plan, bool gray = true) {
   if (ctx.sgm_mode == CSGM_SGM_COMPACT) return compact_plan(ctx, p, w, h, fixed, plan);
   const size_t budget = ctx.ws->budget;
   if (ctx.sgm_mode != CSGM_SGM_STREAMED && resident <= budget) {
@@ -125,6 +125,18 @@ static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, s
   for (int rows = std::min(h, std::max(ctx.strip_rows, min_rows)); rows >= min_rows; rows /= 2) {
     const size_t bytes = fixed + strip_bytes(p, w, rows);
     if (bytes <= budget) {
+      const size_t host = (size_t)w * h * p.disparities * p.aggregate_bytes;
+      if (ctx.host_budget && host > ctx.host_budget) {
+        // GpuStereo.execute (GpuStereo.java:184-193): under auto, a view whose aggregate does
+        // not fit host memory runs compact SGM where it applies.
+        if (ctx.sgm_mode == CSGM_SGM_AUTO && gray && p.cost_mode == CSGM_COST_CENSUS &&
+            p.aggregate_bytes == 2)
+          return compact_plan(ctx, p, w, h, fixed, plan);
+        return fail(CSGM_E_NOMEM,
+                    "streamed SGM parks a %.1f MiB aggregate in host memory, over the host "
+                    "budget of %.1f MiB",
+                    host / 1048576.0, ctx.host_budget / 1048576.0);
+      }
       plan->streamed = true;
       plan->rows = rows;
       plan->device_bytes = bytes;
@@ -143,7 +155,7 @@ int plan_pair(const Context& ctx, const csgm_params& p, int w, int h, bool host_
   if (color && ctx.sgm_mode == CSGM_SGM_COMPACT)
     return fail(CSGM_E_INVALID, "compact SGM needs grayscale Census with 16-bit aggregates");
   return choose_plan(ctx, p, w, h, pair_fixed_bytes(p, w, h, host_inputs, color),
-                     pair_workspace_bytes(p, w, h, host_inputs, color, ctx.tuning), plan);
+                     pair_workspace_bytes(p, w, h, host_inputs, color, ctx.tuning), plan, !color);
 }
 
 void* HostBuffer::get(size_t want, int* status) {

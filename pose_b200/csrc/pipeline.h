@@ -174,6 +174,8 @@ struct Context {
   int sgm_mode = CSGM_SGM_AUTO;
   int strip_rows = 64;
   int candidates = 2;  // Options.esgmCandidates
+  // Host memory a streamed plan may park its aggregate in (0: no limit; csgm_session_set_host_budget).
+  size_t host_budget = 0;
   // Compact SGM's last outcome per view (reverse 0/1): certified pixels, pixels verified exactly.
   int64_t* compact_report = nullptr;
   HostBuffer* host_partial = nullptr;  // null: streaming unavailable (batch slots)
@@ -263,6 +265,7 @@ struct csgm_session {
   int sgm_mode = CSGM_SGM_AUTO;  // csgm_session_set_streaming
   int strip_rows = 64;
   int candidates = 2;             // csgm_session_set_candidates
+  size_t host_budget = 0;         // csgm_session_set_host_budget
   int64_t compact_report[4] = {0, 0, 0, 0};
   csgm::HostBuffer host_partial;
   csgm::TuningTable tuning;  // csgm_autotune / csgm_session_load_tuning

@@ -148,6 +148,11 @@ class GpuSgm:
         """Options.esgmCandidates: compact SGM's separated proposals per path (1..4)."""
         check(self.lib.csgm_session_set_candidates(self.handle, int(per_path)))
 
+    def set_host_budget(self, nbytes: int) -> None:
+        """Host memory for a streamed plan's parked aggregate (0: no limit); over it, auto mode
+        runs compact SGM where it applies (GpuCandidateStereo.hostBudget, --memory-mb)."""
+        check(self.lib.csgm_session_set_host_budget(self.handle, int(nbytes)))
+
     def compact_report(self, reverse: int = 0) -> tuple:
         """(certified, verified exactly) pixels of compact SGM's last view of that side."""
         cert, exact = ctypes.c_int64(), ctypes.c_int64()
@@ -378,6 +383,7 @@ class CensusSgm:
         self.session = session or GpuSgm(options.gpuDevice, options.gpuMemoryMb)
         self.session.set_streaming(options.gpuSgm, options.gpuStripRows)
         self.session.set_candidates(options.esgmCandidates)
+        self.session.set_host_budget(options.memoryMb << 20)  # GpuCandidateStereo.hostBudget
 
     def params(self) -> CsgmParams:
         return params_from_options(self.options)

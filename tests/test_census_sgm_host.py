@@ -28,6 +28,9 @@ class OracleSession:
     def set_candidates(self, per_path=2):
         self.candidates = per_path
 
+    def set_host_budget(self, nbytes=0):
+        self.host_budget = nbytes
+
     def pair(self, params, left, right, w, h, validLeft=None, validRight=None, want_views=False,
              want_reasons=False, leftBgr=None, rightBgr=None):
         r = orc.pair(params, left, right, w, h, validLeft, validRight, want_reasons=True,

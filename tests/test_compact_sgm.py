@@ -269,3 +269,41 @@ def test_census_sgm_compute_in_compact_mode(session):
         assert np.array_equal(bits(got.disparity), bits(want.disparity)), key
         assert np.array_equal(got.reasons, want.reasons), key
         assert got.stats.csv() == want.stats.csv(), key
+
+
+def test_auto_runs_compact_over_the_host_budget():
+    """GpuStereo.execute (GpuStereo.java:184-193) under --gpu-sgm auto: a pair over the device
+    budget streams while its aggregate fits the host budget, and runs compact SGM (no host bytes,
+    the same results) once it does not; streamed mode refuses instead."""
+    from pose_b200.sgm import GpuSgm
+
+    w, h, _, a, b, ma, mb = upgrade_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 41, -3
+    prm = params_from_options(o)
+    want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
+    with GpuSgm(0) as s:
+        full = s.plan_detail(prm, w, h)
+        s.set_budget(full["device_bytes"] // 3)
+        streamed = s.plan_detail(prm, w, h)
+        assert streamed["streamed"] and streamed["host_bytes"] > 0
+        s.set_host_budget(streamed["host_bytes"])
+        assert s.plan_detail(prm, w, h) == streamed
+        s.set_host_budget(streamed["host_bytes"] - 1)
+        compact = s.plan_detail(prm, w, h)
+        assert not compact["streamed"] and compact["host_bytes"] == 0
+        got = s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+        assert_same(got, want, "auto over the host budget")
+        assert all(c + v == w * h and c > 0 for c, v in (s.compact_report(r) for r in (0, 1)))
+        s.set_streaming("streamed", 16)
+        with pytest.raises(_abi.CsgmError) as e:
+            s.pair(prm, a, b, w, h, ma, mb)
+        assert e.value.status == _abi.CSGM_E_NOMEM
+        s.set_streaming("auto")
+        zncc = params_from_options(Options(disparities=41, minDisparity=-3, matchingCost="zncc"))
+        with pytest.raises(_abi.CsgmError) as e:  # compact SGM is Census only
+            s.pair(zncc, a, b, w, h, ma, mb)
+        assert e.value.status == _abi.CSGM_E_NOMEM
+        s.set_host_budget(0)
+        again = s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+        assert_same(again, want, "streamed again without a host budget")
