@@ -85,6 +85,8 @@ static int compact_plan(const Context& ctx, const csgm_params& p, int w, int h, 
                         ViewPlan* plan) {
   if (p.cost_mode != CSGM_COST_CENSUS || p.aggregate_bytes != 2)
     return fail(CSGM_E_INVALID, "compact SGM needs grayscale Census with 16-bit aggregates");
+  if ((int64_t)w * h > INT32_MAX)  // the unresolved pixels' slots and list are int32
+    return fail(CSGM_E_UNSUPPORTED, "compact SGM supports at most %d pixels", INT32_MAX);
   for (int pool = ctx.candidates; pool >= 1; pool--) {
     const size_t bytes = fixed + compact_bytes(p, w, h, pool);
     if (bytes <= ctx.ws->budget) {
