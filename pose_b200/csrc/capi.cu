@@ -75,6 +75,19 @@ void* Workspace::get(int slot, size_t bytes, int* status) {
   return b.ptr;
 }
 
+void Workspace::release(int slot) {
+  Buffer& b = buffers[slot];
+  if (!b.ptr) return;
+  generation++;
+  if (async_stream)
+    cudaFreeAsync(b.ptr, async_stream);
+  else
+    cudaFree(b.ptr);
+  allocated -= b.bytes;
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
 void Workspace::release_all() {
   generation++;
   for (auto& b : buffers)

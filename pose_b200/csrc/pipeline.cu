@@ -73,35 +73,39 @@ static size_t strip_bytes(const csgm_params& p, int w, int rows) {
 // Device bytes of compact SGM besides `fixed`: proposals and compact aggregates (8 bytes per
 // proposal and pixel), the lower bounds, the unresolved slots and list, and one image row of exact
 // aggregates and cost rows (the least chunk of the exact pass).
-static size_t compact_bytes(const csgm_params& p, int w, int h, int pool) {
+static size_t compact_bytes(const csgm_params& p, int w, int h, int pool, int views) {
   const size_t n = (size_t)w * h, C = (size_t)p.directions * pool;
-  return n * (C * 8 + 4 + 8) + 16 + (size_t)w * p.disparities * 4;
+  return views * n * (C * 8 + 4 + 8) + 16 + (size_t)w * p.disparities * 4;
 }
 
 // GpuCandidateStereo.plan (GpuCandidateStereo.java:20-47): grayscale Census with 16-bit
 // aggregates only; the proposals per path start at the session's count and drop until the
-// compact buffers fit the budget.
+// compact buffers fit the budget.  A pair first tries both views at once (`views` = 2: twice the
+// arrays, the path launches shared), then one view after the other.
 static int compact_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
-                        ViewPlan* plan) {
+                        ViewPlan* plan, int views) {
   if (p.cost_mode != CSGM_COST_CENSUS || p.aggregate_bytes != 2)
     return fail(CSGM_E_INVALID, "compact SGM needs grayscale Census with 16-bit aggregates");
   if ((int64_t)w * h > INT32_MAX)  // the unresolved pixels' slots and list are int32
     return fail(CSGM_E_UNSUPPORTED, "compact SGM supports at most %d pixels", INT32_MAX);
-  for (int pool = ctx.candidates; pool >= 1; pool--) {
-    const size_t bytes = fixed + compact_bytes(p, w, h, pool);
-    if (bytes <= ctx.ws->budget) {
-      plan->streamed = false;
-      plan->compact = true;
-      plan->pool = pool;
-      plan->rows = h;
-      plan->device_bytes = bytes;
-      plan->host_bytes = 0;
-      return CSGM_OK;
+  for (int at_once = views; at_once >= 1; at_once--) {
+    for (int pool = ctx.candidates; pool >= 1; pool--) {
+      const size_t bytes = fixed + compact_bytes(p, w, h, pool, at_once);
+      if (bytes <= ctx.ws->budget) {
+        plan->streamed = false;
+        plan->compact = true;
+        plan->views = at_once;
+        plan->pool = pool;
+        plan->rows = h;
+        plan->device_bytes = bytes;
+        plan->host_bytes = 0;
+        return CSGM_OK;
+      }
     }
   }
   return fail(CSGM_E_NOMEM,
               "No compact Census/16-bit GPU plan fits: needs %.1f MiB, budget %.1f MiB",
-              (fixed + compact_bytes(p, w, h, 1)) / 1048576.0, ctx.ws->budget / 1048576.0);
+              (fixed + compact_bytes(p, w, h, 1, 1)) / 1048576.0, ctx.ws->budget / 1048576.0);
 }
 
 // GpuStereo.plan (GpuStereo.java:33-84): resident when the whole volume fits the budget (unless
@@ -109,8 +113,8 @@ static int compact_plan(const Context& ctx, const csgm_params& p, int w, int h, 
 // until one fits.  Strips are at least two rows high with 16 paths, so that a (+-1,+-2) path's
 // predecessor always lies in the previous strip.
 static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, size_t fixed,
-                       size_t resident, ViewPlan* plan, bool gray = true) {
-  if (ctx.sgm_mode == CSGM_SGM_COMPACT) return compact_plan(ctx, p, w, h, fixed, plan);
+                       size_t resident, ViewPlan* plan, bool gray = true, int views = 2) {
+  if (ctx.sgm_mode == CSGM_SGM_COMPACT) return compact_plan(ctx, p, w, h, fixed, plan, views);
   const size_t budget = ctx.ws->budget;
   if (ctx.sgm_mode != CSGM_SGM_STREAMED && resident <= budget) {
     plan->streamed = false;
@@ -133,7 +137,7 @@ static int choose_plan(const Context& ctx, const csgm_params& p, int w, int h, s
         // not fit host memory runs compact SGM where it applies.
         if (ctx.sgm_mode == CSGM_SGM_AUTO && gray && p.cost_mode == CSGM_COST_CENSUS &&
             p.aggregate_bytes == 2)
-          return compact_plan(ctx, p, w, h, fixed, plan);
+          return compact_plan(ctx, p, w, h, fixed, plan, views);
         return fail(CSGM_E_NOMEM,
                     "streamed SGM parks a %.1f MiB aggregate in host memory, over the host "
                     "budget of %.1f MiB",
@@ -213,89 +217,131 @@ static int run_view_general(Context& ctx, const csgm_params& p, const uint64_t* 
   return CSGM_OK;
 }
 
-// One view through compact SGM (GpuCandidateStereo.execute, GpuCandidateStereo.java:53-167):
-// every direction's proposals, then every direction's compact aggregates and lower bounds, then
-// the selection of the certified pixels and the list of the others.  The listed pixels are then
+// The outputs of one compact SGM view.
+struct CompactOut {
+  float* out;
+  int32_t* summary;
+  uint8_t* reasons;
+  uint8_t* boundary;
+  DeviceStats* dstats;
+};
+
+// One view, or both views of a pair, through compact SGM (GpuCandidateStereo.execute,
+// GpuCandidateStereo.java:53-167): every direction's proposals, then every direction's compact
+// aggregates and lower bounds (both views in the same launches), then each view's selection of
+// the certified pixels and list of the others.  The listed pixels of each view are then
 // aggregated exactly, every path walked again with only their rows kept, in chunks that fit the
-// budget, and selected from their full aggregates.
-static int run_view_compact(Context& ctx, const csgm_params& p, int pool, const uint64_t* desc_a,
-                            const uint64_t* desc_b, const uint8_t* tex_a, const uint8_t* tex_b,
-                            const uint8_t* gray_a, const uint8_t* gray_b, int w, int h,
-                            int reverse, float* out, int32_t* summary, uint8_t* reasons,
-                            uint8_t* boundary, DeviceStats* dstats) {
+// budget, and selected from their full aggregates.  With two views, the second is the mirrored
+// view of the first (a and b swapped, reverse flipped).
+static int run_views_compact(Context& ctx, const csgm_params& p, int pool, int views,
+                             const uint64_t* desc_a, const uint64_t* desc_b,
+                             const uint8_t* tex_a, const uint8_t* tex_b, const uint8_t* gray_a,
+                             const uint8_t* gray_b, int w, int h, int reverse,
+                             const CompactOut* outs) {
   int status = CSGM_OK;
   const size_t n = (size_t)w * h, D = (size_t)p.disparities;
   const int C = p.directions * pool;
-  WS(cand, uint16_t, kEsgmCand, n * C * 2);
-  WS(compact, uint16_t, kEsgmCompact, n * C * 6);
-  WS(outside, uint32_t, kEsgmOutside, n * 4);
-  WS(slots, int32_t, kEsgmSlots, n * 4);
-  WS(pixels, int32_t, kEsgmPixels, n * 4);
+  WS(cand, uint16_t, kEsgmCand, views * n * C * 2);
+  WS(compact, uint16_t, kEsgmCompact, views * n * C * 6);
+  WS(outside, uint32_t, kEsgmOutside, views * n * 4);
+  WS(slots, int32_t, kEsgmSlots, views * n * 4);
+  WS(pixels, int32_t, kEsgmPixels, views * n * 4);
   WS(count, int32_t, kEsgmCount, 16);
   CostArgs c{desc_a, desc_b, tex_a, tex_b, gray_a, gray_b, nullptr, w, h, p.disparities,
              p.min_disparity, reverse, p.window_x, p.window_y, words_of(p), p.cost_mode,
              p.census_weight_milli, p.ad_truncation, p.gradient_truncation,
              p.window_x * p.window_y - 1};
-  CK(cudaMemsetAsync(compact, 0, n * C * 6, ctx.stream), "compact clear");
-  CK(cudaMemsetAsync(outside, 0, n * 4, ctx.stream), "bound clear");
+  CK(cudaMemsetAsync(compact, 0, views * n * C * 6, ctx.stream), "compact clear");
+  CK(cudaMemsetAsync(outside, 0, views * n * 4, ctx.stream), "bound clear");
   CK(cudaMemsetAsync(count, 0, 16, ctx.stream), "count clear");
   EsgmArgs e{c, p.directions, p.p1, p.p2, p.edge_scale, cand, compact, outside, C, pool, slots,
              nullptr};
+  e.views = views;
   for (int phase = 0; phase < 2; phase++) {
     ctx.prof->kernel_begin();
     CK(launch_esgm_paths(e, phase, ctx.sm_count, ctx.stream), "compact path kernel launch");
     ctx.prof->kernel_end(phase == 0 ? "esgm_proposals" : "esgm_compact");
   }
-  SelectArgs s{nullptr, out, summary, reasons, boundary, dstats, w, h, p.disparities,
-               p.window_x, p.window_y, p.min_disparity, p.uniqueness};
-  EsgmSelectArgs sel{c, cand, compact, outside, s, C, slots, pixels, count};
-  ctx.prof->kernel_begin();
-  CK(launch_esgm_select(sel, ctx.sm_count, ctx.stream), "compact select kernel launch");
-  ctx.prof->kernel_end("esgm_select");
-  int32_t unresolved = 0;
-  CK(cudaMemcpyAsync(&unresolved, count, 4, cudaMemcpyDeviceToHost, ctx.stream),
+  // View v's inputs and arrays.
+  auto view_args = [&](int v) {
+    EsgmArgs x = e;
+    x.views = 1;
+    if (v) {
+      std::swap(x.cost.desc_a, x.cost.desc_b);
+      std::swap(x.cost.tex_a, x.cost.tex_b);
+      std::swap(x.cost.gray_a, x.cost.gray_b);
+      x.cost.reverse = !x.cost.reverse;
+    }
+    x.cand = cand + v * n * C;
+    x.compact = compact + v * 3 * n * C;
+    x.outside = outside + v * n;
+    x.slots = slots + v * n;
+    return x;
+  };
+  for (int v = 0; v < views; v++) {
+    const EsgmArgs x = view_args(v);
+    const CompactOut& o = outs[v];
+    SelectArgs s{nullptr, o.out, o.summary, o.reasons, o.boundary, o.dstats, w, h,
+                 p.disparities, p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+    EsgmSelectArgs sel{x.cost, x.cand, x.compact, x.outside, s, C, slots + v * n,
+                       pixels + v * n, count + v};
+    ctx.prof->kernel_begin();
+    CK(launch_esgm_select(sel, ctx.sm_count, ctx.stream), "compact select kernel launch");
+    ctx.prof->kernel_end("esgm_select");
+  }
+  int32_t unresolved[2] = {0, 0};
+  CK(cudaMemcpyAsync(unresolved, count, 8, cudaMemcpyDeviceToHost, ctx.stream),
      "unresolved count readback");
   CK(cudaStreamSynchronize(ctx.stream), "compact SGM proposals");
-  if (ctx.compact_report) {
-    ctx.compact_report[2 * reverse] = (int64_t)n - unresolved;
-    ctx.compact_report[2 * reverse + 1] = unresolved;
+  for (int v = 0; v < views; v++) {
+    const int side = views == 2 ? v : reverse;
+    if (ctx.compact_report) {
+      ctx.compact_report[2 * side] = (int64_t)n - unresolved[v];
+      ctx.compact_report[2 * side + 1] = unresolved[v];
+    }
   }
-  if (unresolved == 0) return CSGM_OK;
-  // Exact pass in chunks of listed pixels: each chunk's aggregates and cost rows (4 bytes per
-  // disparity and pixel) within what the budget leaves.
-  const Workspace& ws = *ctx.ws;
-  const size_t held = ws.buffers[kEsgmSum].bytes + ws.buffers[kEsgmCost].bytes;
-  const size_t room = ws.budget > ws.allocated - held ? ws.budget - (ws.allocated - held) : 0;
-  const int64_t chunk = std::min<int64_t>(unresolved, (int64_t)(room / (4 * D)));
-  if (chunk < 1)
-    return fail(CSGM_E_NOMEM, "compact SGM's exact pass exceeds the device budget");
-  WS(sum, uint16_t, kEsgmSum, (size_t)chunk * D * 2);
-  WS(cost, uint16_t, kEsgmCost, (size_t)chunk * D * 2);
-  for (int64_t lo = 0; lo < unresolved; lo += chunk) {
-    const int64_t rows = std::min<int64_t>(chunk, unresolved - lo);
-    CK(cudaMemsetAsync(sum, 0, (size_t)rows * D * 2, ctx.stream), "exact aggregate clear");
-    EsgmArgs x = e;
-    x.slots = slots;
-    x.sum = sum;
-    x.slot_lo = (int32_t)lo;
-    x.slot_hi = (int32_t)(lo + rows);
-    ctx.prof->kernel_begin();
-    CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
-    ctx.prof->kernel_end("esgm_exact");
-    CostArgs cr = c;
-    cr.out = cost;
-    cr.pixels = pixels + lo;
-    cr.npixels = (int)rows;
-    ctx.prof->kernel_begin();
-    CK(launch_cost_volume(cr, ctx.sm_count, ctx.stream), "cost kernel launch");
-    ctx.prof->kernel_end("cost_volume");
-    SelectArgs sw = s;
-    sw.cost = cost;
-    sw.pixels = pixels + lo;
-    sw.npixels = (int)rows;
-    ctx.prof->kernel_begin();
-    CK(launch_winners(sw, sum, 2, ctx.sm_count, ctx.stream), "winners kernel launch");
-    ctx.prof->kernel_end("winners");
+  for (int v = 0; v < views; v++) {
+    if (unresolved[v] == 0) continue;
+    const EsgmArgs x0 = view_args(v);
+    const CompactOut& o = outs[v];
+    // Exact pass in chunks of listed pixels: each chunk's aggregates and cost rows (4 bytes per
+    // disparity and pixel) within what the budget leaves.
+    const Workspace& ws = *ctx.ws;
+    const size_t held = ws.buffers[kEsgmSum].bytes + ws.buffers[kEsgmCost].bytes;
+    const size_t room = ws.budget > ws.allocated - held ? ws.budget - (ws.allocated - held) : 0;
+    const int64_t chunk = std::min<int64_t>(unresolved[v], (int64_t)(room / (4 * D)));
+    if (chunk < 1)
+      return fail(CSGM_E_NOMEM, "compact SGM's exact pass exceeds the device budget");
+    WS(sum, uint16_t, kEsgmSum, (size_t)chunk * D * 2);
+    WS(cost, uint16_t, kEsgmCost, (size_t)chunk * D * 2);
+    const int32_t* list = pixels + v * n;
+    SelectArgs s{nullptr, o.out, o.summary, o.reasons, o.boundary, o.dstats, w, h,
+                 p.disparities, p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+    for (int64_t lo = 0; lo < unresolved[v]; lo += chunk) {
+      const int64_t rows = std::min<int64_t>(chunk, unresolved[v] - lo);
+      CK(cudaMemsetAsync(sum, 0, (size_t)rows * D * 2, ctx.stream), "exact aggregate clear");
+      EsgmArgs x = x0;
+      x.sum = sum;
+      x.slot_lo = (int32_t)lo;
+      x.slot_hi = (int32_t)(lo + rows);
+      ctx.prof->kernel_begin();
+      CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
+      ctx.prof->kernel_end("esgm_exact");
+      CostArgs cr = x0.cost;
+      cr.out = cost;
+      cr.pixels = list + lo;
+      cr.npixels = (int)rows;
+      ctx.prof->kernel_begin();
+      CK(launch_cost_volume(cr, ctx.sm_count, ctx.stream), "cost kernel launch");
+      ctx.prof->kernel_end("cost_volume");
+      SelectArgs sw = s;
+      sw.cost = cost;
+      sw.pixels = list + lo;
+      sw.npixels = (int)rows;
+      ctx.prof->kernel_begin();
+      CK(launch_winners(sw, sum, 2, ctx.sm_count, ctx.stream), "winners kernel launch");
+      ctx.prof->kernel_end("winners");
+    }
   }
   return CSGM_OK;
 }
@@ -408,6 +454,20 @@ static float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// A session's workspace keeps its buffers from call to call.  A call on a compact plan frees the
+// volumes of the other plans first, and any other call frees compact SGM's arrays, so that the
+// buffers the call's own plan counts fit the budget (nothing is freed when the plan repeats).
+static void release_other_plans(Workspace& ws, bool compact) {
+  static const int volumes[] = {kCostL, kCostR,    kSum,       kSumUp,     kSumLines,
+                                kPen,   kCarry,    kFlags,     kPixelInfo, kStripCarry};
+  static const int arrays[] = {kEsgmCand,   kEsgmCompact, kEsgmOutside, kEsgmSlots,
+                               kEsgmPixels, kEsgmCount,   kEsgmSum,     kEsgmCost};
+  if (compact)
+    for (int slot : volumes) ws.release(slot);
+  else
+    for (int slot : arrays) ws.release(slot);
+}
+
 // The device part of a pair.  `own_call` = this is the whole call (csgm_pair_device), so it owns
 // the call-level timing; csgm_pair times its own copies around it.
 static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& plan,
@@ -419,6 +479,7 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
   int words = words_of(p);
+  release_other_plans(*ctx.ws, plan.compact);
   if (own_call) ctx.prof->begin_call(ctx.stream);
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (own_call && ctx.prof->level >= 1) {
@@ -476,11 +537,19 @@ static int pair_on_device(Context& ctx, const csgm_params& p, const ViewPlan& pl
                                nullptr, nullptr, nullptr, nullptr, plan.rows);
     if (status) return status;
   } else if (plan.compact) {
-    status = run_view_compact(ctx, p, plan.pool, desc_l, desc_r, tex_l, tex_r, left, right, w, h,
-                              0, disp_l, nullptr, reasons, boundary, dstats);
-    if (status) return status;
-    status = run_view_compact(ctx, p, plan.pool, desc_r, desc_l, tex_r, tex_l, right, left, w, h,
-                              1, disp_r, nullptr, nullptr, nullptr, nullptr);
+    // Both views; the right view's counters are discarded.
+    const CompactOut outs[2] = {{disp_l, nullptr, reasons, boundary, dstats},
+                                {disp_r, nullptr, nullptr, nullptr, nullptr}};
+    if (plan.views == 2) {
+      status = run_views_compact(ctx, p, plan.pool, 2, desc_l, desc_r, tex_l, tex_r, left, right,
+                                 w, h, 0, outs);
+    } else {
+      status = run_views_compact(ctx, p, plan.pool, 1, desc_l, desc_r, tex_l, tex_r, left, right,
+                                 w, h, 0, &outs[0]);
+      if (status) return status;
+      status = run_views_compact(ctx, p, plan.pool, 1, desc_r, desc_l, tex_r, tex_l, right, left,
+                                 w, h, 1, &outs[1]);
+    }
     if (status) return status;
   } else if (use_fused(p, h)) {
     // Both views in one pass structure (stereo_fused.cu).
@@ -942,6 +1011,7 @@ static int run_match_general(Context& ctx, const csgm_params& p, const ViewPlan&
   int status = CSGM_OK;
   size_t n = (size_t)w * h;
   int words = words_of(p);
+  release_other_plans(*ctx.ws, plan.compact);
   WS(d_a, uint64_t, kDescL, n * words * 8);
   WS(d_b, uint64_t, kDescR, n * words * 8);
   WS(d_ga, uint8_t, kImgL, n);
@@ -979,10 +1049,11 @@ static int run_match_general(Context& ctx, const csgm_params& p, const ViewPlan&
   if (plan.streamed)
     status = run_view_streamed(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
                                d_summary, d_reasons, d_boundary, dstats, plan.rows);
-  else if (plan.compact)
-    status = run_view_compact(ctx, p, plan.pool, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse,
-                              d_out, d_summary, d_reasons, d_boundary, dstats);
-  else
+  else if (plan.compact) {
+    const CompactOut out{d_out, d_summary, d_reasons, d_boundary, dstats};
+    status = run_views_compact(ctx, p, plan.pool, 1, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h,
+                               reverse, &out);
+  } else
     status = run_view_general(ctx, p, d_a, d_b, d_ta, d_tb, d_ga, d_gb, w, h, reverse, d_out,
                               d_summary, d_reasons, d_boundary, dstats);
   if (status) return status;
@@ -1011,14 +1082,17 @@ int run_match_host(Context& ctx, const csgm_params& p, const uint64_t* desc_a,
   const bool summary = out_summary != nullptr;
   if (ctx.twin && ctx.sgm_mode != CSGM_SGM_STREAMED && ctx.sgm_mode != CSGM_SGM_COMPACT &&
       use_fused(p, h) &&
-      match_fused_bytes(p, w, h, summary, ctx.tuning) <= ctx.ws->budget)
+      match_fused_bytes(p, w, h, summary, ctx.tuning) <= ctx.ws->budget) {
+    release_other_plans(*ctx.ws, false);
     return run_match_fused(ctx, p, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h, reverse,
                            out_disp, out_summary, reasons, boundary, stats);
+  }
   if (ctx.twin) ctx.twin->valid = false;
   const size_t fixed = match_fixed_bytes(p, w, h, summary);
   const size_t cells = (size_t)w * h * p.disparities;
   ViewPlan plan;
-  int status = choose_plan(ctx, p, w, h, fixed, fixed + cells * (2 + p.aggregate_bytes), &plan);
+  int status = choose_plan(ctx, p, w, h, fixed, fixed + cells * (2 + p.aggregate_bytes), &plan,
+                           true, 1);
   if (status) return status;
   return run_match_general(ctx, p, plan, desc_a, desc_b, gray_a, gray_b, tex_a, tex_b, w, h,
                            reverse, out_disp, out_summary, reasons, boundary, stats);

@@ -87,6 +87,7 @@ struct ViewPlan {
   bool streamed = false;
   bool compact = false;       // compact SGM (CSGM_SGM_COMPACT)
   int pool = 0;               // its proposals per path
+  int views = 1;              // its views at once (2: a pair's views share the path launches)
   int rows = 0;               // strip height (the image height when resident)
   size_t device_bytes = 0;    // device memory of the plan
   size_t host_bytes = 0;      // pinned host memory of the plan
@@ -123,6 +124,8 @@ struct Workspace {
   cudaStream_t async_stream = nullptr;
   void* get(int slot, size_t bytes, int* status);
   void release_all();
+  // Frees one buffer (nothing when it holds none).
+  void release(int slot);
 };
 
 struct Profiler {

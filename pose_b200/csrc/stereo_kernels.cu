@@ -235,11 +235,26 @@ __device__ __forceinline__ void add_u16(uint16_t* at, unsigned v) {
 template <int PHASE>
 __global__ void esgm_paths_kernel(EsgmArgs a) {
   extern __shared__ int smem[];
-  const CostArgs& ca = a.cost;
+  CostArgs ca = a.cost;
   const int D = ca.D, w = ca.w, h = ca.h, C = a.C;
   const int64_t n = (int64_t)w * h;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  const int dir = blockIdx.y;
+  const int dir = blockIdx.y % a.directions;
+  if (blockIdx.y >= a.directions) {  // the mirrored view
+    const uint64_t* d = ca.desc_a;
+    ca.desc_a = ca.desc_b;
+    ca.desc_b = d;
+    const uint8_t* t = ca.tex_a;
+    ca.tex_a = ca.tex_b;
+    ca.tex_b = t;
+    t = ca.gray_a;
+    ca.gray_a = ca.gray_b;
+    ca.gray_b = t;
+    ca.reverse = !ca.reverse;
+    a.cand += n * C;
+    a.compact += 3 * n * C;
+    a.outside += n;
+  }
   int dx, dy;
   direction(dir, dx, dy);
   // StereoCost.pathP2 by the gray difference of a pixel and its predecessor.
@@ -646,7 +661,7 @@ cudaError_t launch_esgm_paths(const EsgmArgs& a, int phase, int sm_count, cudaSt
     direction(d, dx, dy);
     lines = std::max(lines, line_count(a.cost.w, a.cost.h, dx, dy));
   }
-  const dim3 grid(grid_for(lines, warps, sm_count * 64), a.directions);
+  const dim3 grid(grid_for(lines, warps, sm_count * 64), a.directions * (phase == 2 ? 1 : a.views));
   auto kernel = phase == 0 ? esgm_paths_kernel<0>
                 : phase == 1 ? esgm_paths_kernel<1>
                              : esgm_paths_kernel<2>;

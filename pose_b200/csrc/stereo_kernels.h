@@ -86,6 +86,10 @@ struct EsgmArgs {
   const int32_t* slots;
   uint16_t* sum;
   int32_t slot_lo = 0, slot_hi = 0;
+  // 2: blocks with blockIdx.y >= directions walk the mirrored view (images, masks and grays
+  // swapped, reverse flipped) into the arrays that follow the first view's (cand + n C,
+  // compact + 3 n C, outside + n); the exact pass runs one view at a time.
+  int views = 1;
 };
 
 struct EsgmSelectArgs {

@@ -135,7 +135,8 @@ def test_compact_crop_equals_oracle(session):
 
 def test_exact_pass_in_chunks():
     """A budget of exactly the compact plan leaves one image row of exact aggregates: the exact
-    pass runs in many chunks and still equals the oracle; a budget below the plan is refused."""
+    pass runs in many chunks and still equals the oracle; a budget below the smallest plan is
+    refused."""
     from pose_b200.sgm import GpuSgm
 
     # Two unrelated noise images: few outcomes are certain, so most pixels go to the exact pass.
@@ -156,10 +157,14 @@ def test_exact_pass_in_chunks():
         got, reports = compact_pair(s, prm, a, b, w, h, pool=1)
         assert_same(got, want, "compact with one row of exact aggregates")
         assert max(v for _, v in reports) > w, "the exact pass should take several chunks"
+    # The smallest plan holds one view's arrays at a time (8 bytes per path and pixel + 12).
+    smallest = plan["device_bytes"] - w * h * (prm.directions * 8 + 12)
     with GpuSgm(0) as s:
-        s.set_budget(plan["device_bytes"] - 1)
         s.set_streaming("esgm")
         s.set_candidates(1)
+        s.set_budget(smallest)
+        assert s.plan_detail(prm, w, h)["device_bytes"] == smallest
+        s.set_budget(smallest - 1)
         with pytest.raises(_abi.CsgmError) as e:
             s.pair(prm, a, b, w, h)
         assert e.value.status == _abi.CSGM_E_NOMEM
@@ -167,26 +172,36 @@ def test_exact_pass_in_chunks():
 
 def test_plan_lowers_the_proposals_to_fit():
     """GpuCandidateStereo.plan tries pool = esgmCandidates .. 1: a budget between the 1- and
-    2-proposal plans gives the 1-proposal plan."""
+    2-proposal plans gives the 1-proposal plan.  A pair's plan first holds both views' arrays;
+    below the smallest such plan it runs one view after the other."""
     from pose_b200.sgm import GpuSgm
 
     w, h, _, a, b, ma, mb = upgrade_pair()
+    n = w * h
     o = Options()
     o.disparities, o.minDisparity = 41, -3
     prm = params_from_options(o)
+    want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
+    per_view = {pool: n * (prm.directions * pool * 8 + 12) for pool in (1, 2)}
     with GpuSgm(0) as s:
         s.set_streaming("esgm")
         sizes = {}
         for pool in (1, 2):
             s.set_candidates(pool)
             sizes[pool] = s.plan_detail(prm, w, h)["device_bytes"]
-        assert sizes[2] - sizes[1] == w * h * prm.directions * 8
+        assert sizes[2] - sizes[1] == 2 * (per_view[2] - per_view[1])  # both views' arrays
         s.set_budget(sizes[2] - 1)
         s.set_candidates(2)
         assert s.plan_detail(prm, w, h)["device_bytes"] == sizes[1]
-        want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
         got = s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
         assert_same(got, want, "compact with the lowered proposal count")
+        one_view = sizes[2] - per_view[2]  # 2 proposals, one view's arrays
+        assert one_view < sizes[1]
+        s.set_budget(sizes[1] - 1)
+        assert s.plan_detail(prm, w, h)["device_bytes"] == one_view
+        got = s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+        assert_same(got, want, "compact one view after the other")
+        assert all(c + v == n for c, v in (s.compact_report(r) for r in (0, 1)))
 
 
 @pytest.mark.parametrize("reverse", [0, 1])
@@ -307,3 +322,28 @@ def test_auto_runs_compact_over_the_host_budget():
         s.set_host_budget(0)
         again = s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
         assert_same(again, want, "streamed again without a host budget")
+
+
+def test_plan_switch_frees_the_other_plans_buffers():
+    """A session's workspace keeps its buffers from call to call. A compact call after a resident
+    one frees the resident volumes, so it fits a budget of exactly its own plan; the resident call
+    after it frees the compact arrays again."""
+    from pose_b200.sgm import GpuSgm
+
+    w, h, _, a, b, ma, mb = upgrade_pair()
+    o = Options()
+    o.disparities, o.minDisparity = 41, -3
+    prm = params_from_options(o)
+    want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
+    with GpuSgm(0) as s:
+        assert_same(s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True), want,
+                    "resident")
+        resident_bytes = s.plan_detail(prm, w, h)["device_bytes"]
+        s.set_streaming("esgm")
+        s.set_budget(s.plan_detail(prm, w, h)["device_bytes"])
+        assert_same(s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True), want,
+                    "compact after resident")
+        s.set_streaming("auto")
+        s.set_budget(resident_bytes)
+        assert_same(s.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True), want,
+                    "resident after compact")
