@@ -1,7 +1,8 @@
-"""Edge cases against the oracle, bit for bit on both kernel paths: the smallest image the
-reference accepts (CensusSgm.java:56-60), the smallest and largest disparity counts, ranges at
-the fused kernels' edge, odd sizes, everything masked out, large negative ranges, and an image
-taller than the fused sweep's row limit (65535 rows: the general kernels run it)."""
+"""Edge cases against the oracle, bit for bit on both kernel paths and, where it applies
+(Census, 16-bit aggregates), through compact SGM: the smallest image the reference accepts
+(CensusSgm.java:56-60), the smallest and largest disparity counts, ranges at the fused kernels'
+edge, odd sizes, everything masked out, large negative ranges, and an image taller than the fused
+sweep's row limit (65535 rows: the general kernels run it)."""
 from __future__ import annotations
 
 import numpy as np
@@ -31,14 +32,22 @@ def bits(a):
 def check(session, o, a, b, w, h, ma=None, mb=None, paths=(0, 1)):
     prm = params_from_options(o)
     want = orc.pair(prm, a, b, w, h, ma, mb, want_reasons=True)
-    for flags in paths:
+    runs = [(flags, "auto") for flags in paths]
+    if prm.cost_mode == 0 and prm.aggregate_bytes == 2:  # compact SGM: Census, 16-bit
+        runs.append((0, "esgm"))
+    for flags, mode in runs:
         prm.flags = flags
-        got = session.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
-        assert np.array_equal(bits(got.left), bits(want["dl"])), flags
-        assert np.array_equal(bits(got.right), bits(want["dr"])), flags
-        assert np.array_equal(bits(got.disparity), bits(want["checked"])), flags
-        assert np.array_equal(got.reasons, want["reasons"]), flags
-        assert np.array_equal(got.searchBoundary, want["boundary"]), flags
+        session.set_streaming(mode)
+        try:
+            got = session.pair(prm, a, b, w, h, ma, mb, want_views=True, want_reasons=True)
+        finally:
+            session.set_streaming("auto")
+        what = (flags, mode)
+        assert np.array_equal(bits(got.left), bits(want["dl"])), what
+        assert np.array_equal(bits(got.right), bits(want["dr"])), what
+        assert np.array_equal(bits(got.disparity), bits(want["checked"])), what
+        assert np.array_equal(got.reasons, want["reasons"]), what
+        assert np.array_equal(got.searchBoundary, want["boundary"]), what
     return want
 
 
