@@ -429,33 +429,34 @@ __global__ void penalty_kernel(const PenaltyArgs a) {
   for (int d = threadIdx.x; d < 256; d += blockDim.x)
     step_p2[d] = path_p2(a.p1, a.p2, a.edge_scale, d, 0);
   __syncthreads();
-  const int xs = blockIdx.x * blockDim.x + threadIdx.x;
   const int yp = blockIdx.y, s = blockIdx.z;
   const int W = a.W, H = a.H;
-  if (xs >= W) return;
-  const int step = s ? -1 : 1;  // image offset of one stream step, in x and in y
-  const int x = s ? W - 1 - xs : xs, y = s ? H - 1 - yp : yp;
-  const int px[4] = {x - step, x, x - step, x + step};
-  const int py[4] = {y, y - step, y - step, y - step};
-  uint32_t word[4] = {0, 0, 0, 0};
+  // Several pixels of the row per thread, so that the table above is filled once per 1024 pixels.
+  for (int xs = blockIdx.x * blockDim.x + threadIdx.x; xs < W; xs += gridDim.x * blockDim.x) {
+    const int step = s ? -1 : 1;  // image offset of one stream step, in x and in y
+    const int x = s ? W - 1 - xs : xs, y = s ? H - 1 - yp : yp;
+    const int px[4] = {x - step, x, x - step, x + step};
+    const int py[4] = {y, y - step, y - step, y - step};
+    uint32_t word[4] = {0, 0, 0, 0};
 #pragma unroll
-  for (int v = 0; v < 2; v++) {
-    const uint8_t* g = a.gray[v];
-    const int center = g[(int64_t)y * W + x];
+    for (int v = 0; v < 2; v++) {
+      const uint8_t* g = a.gray[v];
+      const int center = g[(int64_t)y * W + x];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      int value = a.p2;
-      if (px[i] >= 0 && px[i] < W && py[i] >= 0 && py[i] < H)
-        value = step_p2[abs(center - (int)g[(int64_t)py[i] * W + px[i]])];
-      word[i] |= (uint32_t)(value - a.p1) << (16 * v);
+      for (int i = 0; i < 4; i++) {
+        int value = a.p2;
+        if (px[i] >= 0 && px[i] < W && py[i] >= 0 && py[i] < H)
+          value = step_p2[abs(center - (int)g[(int64_t)py[i] * W + px[i]])];
+        word[i] |= (uint32_t)(value - a.p1) << (16 * v);
+      }
+      if (a.tex[v][(int64_t)y * W + x]) word[0] |= 0x8000u << (16 * v);
     }
-    if (a.tex[v][(int64_t)y * W + x]) word[0] |= 0x8000u << (16 * v);
-  }
-  a.out[((int64_t)s * H + yp) * W + xs] = make_uint4(word[0], word[1], word[2], word[3]);
-  if (a.info && s == 0) {
-    const int64_t p = (int64_t)y * W + x;
-    a.info[p] = (uint32_t)a.gray[0][p] | (uint32_t)a.gray[1][p] << 8 |
-                (a.tex[0][p] ? 1u : 0u) << 16 | (a.tex[1][p] ? 1u : 0u) << 24;
+    a.out[((int64_t)s * H + yp) * W + xs] = make_uint4(word[0], word[1], word[2], word[3]);
+    if (a.info && s == 0) {
+      const int64_t p = (int64_t)y * W + x;
+      a.info[p] = (uint32_t)a.gray[0][p] | (uint32_t)a.gray[1][p] << 8 |
+                  (a.tex[0][p] ? 1u : 0u) << 16 | (a.tex[1][p] ? 1u : 0u) << 24;
+    }
   }
 }
 
@@ -2035,7 +2036,7 @@ int run_views_fused(Context& ctx, const csgm_params& p, const FusedViews& v, int
     PenaltyArgs pa{{v.gray_l, v.gray_r}, {v.tex_l, v.tex_r}, pen, info, w, h, p.p1, p.p2,
                    p.edge_scale};
     ctx.prof->kernel_begin();
-    penalty_kernel<<<dim3((w + 127) / 128, h, 2), 128, 0, ctx.stream>>>(pa);
+    penalty_kernel<<<dim3((w + 1023) / 1024, h, 2), 128, 0, ctx.stream>>>(pa);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return cuda_fail(le, "penalty kernel launch");
     ctx.prof->kernel_end("penalty");
