@@ -178,22 +178,6 @@ __global__ void paths_line_kernel(PathArgs a, SumT* __restrict__ sum) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Compact SGM (GpuCandidateStereo.java:53-167, the path kernel hooks :401-479).  One warp per line
-// as in paths_line_kernel, each pixel's costs computed from the descriptors (no cost volume), and
-// every direction of a phase in one launch (blockIdx.y = direction); at every pixel, after the
-// path state L:
-//  PHASE 0: `pool` separated proposals of the path: the valid disparity of least L (ties: the
-//   smaller), then the least among those more than one away from every proposal so far;
-//  PHASE 1 (all directions' proposals known): L at every proposal - 1, proposal, proposal + 1 is
-//   added to the pixel's compact aggregates, and the least L over the valid disparities no
-//   proposal covers (within one) to the pixel's lower bound of the aggregate there (or the bound
-//   is marked empty when every valid disparity is covered, which no direction changes);
-//  PHASE 2 (exact pass): L is added to the full aggregate row of each listed pixel.
-// The directions' additions to a pixel are atomic 32-bit adds of a 16-bit value shifted into its
-// half of the word.  They are exact in any order: the plan allows 16-bit aggregates only while
-// directions x (512 + P2) <= 65535, and one path's L never exceeds 512 + P2, so no 16-bit sum
-// carries into its neighbour (the reference adds the directions one after another with the same
-// wrap-free values, GpuCandidateStereo.java:437-444).
 // cost_at for the Census cost (the only one compact SGM plans for), with the pixel's own terms
 // (border, texture, descriptor words) taken once per pixel instead of once per disparity.
 // The target of disparity k is x0 + step * k (step = +1 for the right view, -1 for the left).
@@ -227,11 +211,28 @@ struct CensusPixel {
   }
 };
 
+// *at += v as a 32-bit atomic add on the word that holds *at (exact while no 16-bit sum wraps).
 __device__ __forceinline__ void add_u16(uint16_t* at, unsigned v) {
   const uintptr_t address = (uintptr_t)at;
   atomicAdd((unsigned*)(address & ~(uintptr_t)3), v << ((address & 2) ? 16 : 0));
 }
 
+// Compact SGM (GpuCandidateStereo.java:53-167, the path kernel hooks :401-479).  One warp per line
+// as in paths_line_kernel, each pixel's costs computed from the descriptors (no cost volume), and
+// every direction of a phase in one launch (blockIdx.y = direction, plus the direction count for
+// a pair's mirrored view); at every pixel, after the path state L:
+//  PHASE 0: `pool` separated proposals of the path: the valid disparity of least L (ties: the
+//   smaller), then the least among those more than one away from every proposal so far;
+//  PHASE 1 (all directions' proposals known): L at every proposal - 1, proposal, proposal + 1 is
+//   added to the pixel's compact aggregates, and the least L over the valid disparities no
+//   proposal covers (within one) to the pixel's lower bound of the aggregate there (or the bound
+//   is marked empty when every valid disparity is covered, which no direction changes);
+//  PHASE 2 (exact pass): L is added to the full aggregate row of each listed pixel.
+// The directions' additions to a pixel are atomic 32-bit adds of a 16-bit value shifted into its
+// half of the word.  They are exact in any order: the plan allows 16-bit aggregates only while
+// directions x (512 + P2) <= 65535, and one path's L never exceeds 512 + P2, so no 16-bit sum
+// carries into its neighbour (the reference adds the directions one after another with the same
+// wrap-free values, GpuCandidateStereo.java:437-444).
 template <int PHASE>
 __global__ void esgm_paths_kernel(EsgmArgs a) {
   extern __shared__ int smem[];
