@@ -300,6 +300,48 @@ static int run_views_compact(Context& ctx, const csgm_params& p, int pool, int v
       ctx.compact_report[2 * side + 1] = unresolved[v];
     }
   }
+  // Both views' listed pixels in one exact pass when their rows fit the budget together.
+  if (views == 2 && unresolved[0] > 0 && unresolved[1] > 0) {
+    const Workspace& ws = *ctx.ws;
+    const size_t held = ws.buffers[kEsgmSum].bytes + ws.buffers[kEsgmCost].bytes;
+    const size_t room = ws.budget > ws.allocated - held ? ws.budget - (ws.allocated - held) : 0;
+    const int64_t rows = (int64_t)unresolved[0] + unresolved[1];
+    if ((size_t)rows * 4 * D <= room) {
+      WS(sum, uint16_t, kEsgmSum, (size_t)rows * D * 2);
+      WS(cost, uint16_t, kEsgmCost, (size_t)rows * D * 2);
+      CK(cudaMemsetAsync(sum, 0, (size_t)rows * D * 2, ctx.stream), "exact aggregate clear");
+      EsgmArgs x = e;  // view 0's arrays; the kernel finds view 1's after them
+      x.sum = sum;
+      x.slot_lo = 0;
+      x.slot_hi = unresolved[0];
+      x.sum2 = sum + (size_t)unresolved[0] * D;
+      x.slot_lo2 = 0;
+      x.slot_hi2 = unresolved[1];
+      ctx.prof->kernel_begin();
+      CK(launch_esgm_paths(x, 2, ctx.sm_count, ctx.stream), "exact path kernel launch");
+      ctx.prof->kernel_end("esgm_exact");
+      for (int v = 0; v < 2; v++) {
+        const CompactOut& o = outs[v];
+        const size_t first = v ? (size_t)unresolved[0] : 0;
+        CostArgs cr = view_args(v).cost;
+        cr.out = cost + first * D;
+        cr.pixels = pixels + v * n;
+        cr.npixels = unresolved[v];
+        ctx.prof->kernel_begin();
+        CK(launch_cost_volume(cr, ctx.sm_count, ctx.stream), "cost kernel launch");
+        ctx.prof->kernel_end("cost_volume");
+        SelectArgs sw{cost + first * D, o.out, o.summary, o.reasons, o.boundary, o.dstats, w, h,
+                      p.disparities, p.window_x, p.window_y, p.min_disparity, p.uniqueness};
+        sw.pixels = pixels + v * n;
+        sw.npixels = unresolved[v];
+        ctx.prof->kernel_begin();
+        CK(launch_winners(sw, sum + first * D, 2, ctx.sm_count, ctx.stream),
+           "winners kernel launch");
+        ctx.prof->kernel_end("winners");
+      }
+      return CSGM_OK;
+    }
+  }
   for (int v = 0; v < views; v++) {
     if (unresolved[v] == 0) continue;
     const EsgmArgs x0 = view_args(v);

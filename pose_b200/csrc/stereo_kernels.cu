@@ -255,6 +255,10 @@ __global__ void esgm_paths_kernel(EsgmArgs a) {
     a.cand += n * C;
     a.compact += 3 * n * C;
     a.outside += n;
+    a.slots += n;
+    a.sum = a.sum2;
+    a.slot_lo = a.slot_lo2;
+    a.slot_hi = a.slot_hi2;
   }
   int dx, dy;
   direction(dir, dx, dy);
@@ -662,7 +666,7 @@ cudaError_t launch_esgm_paths(const EsgmArgs& a, int phase, int sm_count, cudaSt
     direction(d, dx, dy);
     lines = std::max(lines, line_count(a.cost.w, a.cost.h, dx, dy));
   }
-  const dim3 grid(grid_for(lines, warps, sm_count * 64), a.directions * (phase == 2 ? 1 : a.views));
+  const dim3 grid(grid_for(lines, warps, sm_count * 64), a.directions * a.views);
   auto kernel = phase == 0 ? esgm_paths_kernel<0>
                 : phase == 1 ? esgm_paths_kernel<1>
                              : esgm_paths_kernel<2>;

@@ -88,8 +88,11 @@ struct EsgmArgs {
   int32_t slot_lo = 0, slot_hi = 0;
   // 2: blocks with blockIdx.y >= directions walk the mirrored view (images, masks and grays
   // swapped, reverse flipped) into the arrays that follow the first view's (cand + n C,
-  // compact + 3 n C, outside + n); the exact pass runs one view at a time.
+  // compact + 3 n C, outside + n, slots + n); in the exact pass that view's listed pixels in
+  // [slot_lo2, slot_hi2) go to sum2.
   int views = 1;
+  uint16_t* sum2 = nullptr;
+  int32_t slot_lo2 = 0, slot_hi2 = 0;
 };
 
 struct EsgmSelectArgs {
